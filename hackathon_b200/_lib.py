@@ -1,0 +1,69 @@
+"""Loads the in-tree CUDA library and declares the C ABI (include/ddm_b200.h).
+
+There is no fallback: if the library is missing or cannot load, importing the
+engine fails with the reason.
+"""
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "libddm_b200.so")
+
+DDM_OK, DDM_ERR_ARG, DDM_ERR_CUDA, DDM_ERR_STATE, DDM_ERR_NOMEM, DDM_ERR_NODEV = range(6)
+DTYPES = {"u8": 0, "u16": 1, "f32": 2}
+
+
+class Geometry(C.Structure):
+    _fields_ = [("N", C.c_int32), ("T", C.c_int32), ("TPAD", C.c_int32), ("L", C.c_int32),
+                ("NB", C.c_int32), ("kmin", C.c_double), ("kmax", C.c_double),
+                ("knodes", C.c_int32), ("reserved", C.c_int32)]
+
+
+_vp = C.c_void_p
+_i32 = C.c_int32
+_SIGS = {
+    "ddm_create": (C.c_int, [C.POINTER(Geometry), C.POINTER(_vp)]),
+    "ddm_destroy": (None, [_vp]),
+    "ddm_last_error": (C.c_char_p, [_vp]),
+    "ddm_create_error": (C.c_char_p, []),
+    "ddm_get_geometry": (C.c_int, [_vp, C.POINTER(Geometry)]),
+    "ddm_bins_count": (C.c_int, [_vp]),
+    "ddm_get_bins": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
+    "ddm_ingest_luma": (C.c_int, [_vp, _vp, _i32, C.POINTER(_i32)]),
+    "ddm_ingest_frames": (C.c_int, [_vp, _vp, _i32, _i32, _vp, C.c_float]),
+    "ddm_ingest_frames_device": (C.c_int, [_vp, _vp, _i32, _i32, _vp, C.c_float]),
+    "ddm_set_spatial_mask": (C.c_int, [_vp, _vp]),
+    "ddm_compute_temporal": (C.c_int, [_vp, _vp, _vp, _i32]),
+    "ddm_compute_temporal_async": (C.c_int, [_vp, _vp, _vp, _i32]),
+    "ddm_read_radial": (C.c_int, [_vp, _vp, _vp, _vp]),
+    "ddm_read_history": (C.c_int, [_vp, _vp]),
+    "ddm_read_temporal_full": (C.c_int, [_vp, _vp, _vp, _vp]),
+    "ddm_read_mean": (C.c_int, [_vp, C.POINTER(C.c_double)]),
+    "ddm_idle": (C.c_int, [_vp]),
+    "ddm_pending": (C.c_int, [_vp]),
+    "ddm_wait_for_capacity": (C.c_int, [_vp]),
+    "ddm_throttled": (C.c_int64, [_vp]),
+    "ddm_set_stream": (C.c_int, [_vp, _vp]),
+    "ddm_kernel_launches": (C.c_int64, [_vp]),
+}
+
+_lib = None
+
+
+def load():
+    """The loaded library with every C-ABI signature declared."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with `python -m hackathon_b200.build`")
+        lib = C.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGS.items():
+            f = getattr(lib, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = lib
+    return _lib
+
+
+def exported_symbols():
+    return list(_SIGS)

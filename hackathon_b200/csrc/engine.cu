@@ -1,0 +1,727 @@
+// The engine behind the C ABI (include/ddm_b200.h): device buffers, host
+// tables, ingest chunking with copy/compute overlap, temporal + radial
+// launches and readback. Mirrors the lifetime and call rules of the
+// reference's WebGPU engine (motility-ddm/src/ddm-engine.ts).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/ddm_b200.h"
+#include "kernels.cuh"
+#include "tables.h"
+
+using namespace ddm;
+
+namespace {
+
+constexpr int MAX_PENDING = 2;  // ddm-engine.ts:46
+constexpr int NSTAGE = 2;       // host->device staging buffers (double buffer)
+
+thread_local std::string g_create_error;
+
+}  // namespace
+
+struct ddm_engine {
+  ddm_geometry g{};
+  int NH = 0, NHB = 0, modes = 0, chunk = 0;
+  int device = 0;
+  std::string err;
+  int64_t launches = 0, throttled = 0;
+
+  cudaStream_t own_stream = nullptr, stream = nullptr, copy_stream = nullptr;
+  cudaEvent_t ready_ev[NSTAGE]{}, free_ev[NSTAGE]{}, meta_ev = nullptr;
+  std::vector<cudaEvent_t> inflight;  // completion events of recent ingests
+
+  // geometry tables
+  BinTable bins;
+  float2 *d_hist = nullptr;            // [modes][T]
+  float2 *d_rows = nullptr;            // [chunk][NHB][N][KB]
+  double *d_rowsum = nullptr;          // [chunk][N]
+  double *d_means = nullptr;           // [chunk]
+  float *d_win = nullptr, *d_wys = nullptr;
+  double *d_ninv = nullptr, *d_invtot = nullptr;
+  float2 *d_tw_s = nullptr, *d_tw_t = nullptr;
+  float2 *d_wcorr4 = nullptr, *d_wcorr_full = nullptr;
+  uint8_t *d_smask = nullptr;
+  void *d_stage[NSTAGE]{};             // device staging for host frames
+  size_t stage_bytes = 0;
+  int *d_slots = nullptr;              // [NSTAGE][chunk] (device copy of slots)
+  int *h_slots = nullptr;              // pinned [NSTAGE][chunk]
+  double scale_last = 1.0;
+  int last_mean_index = -1;
+  bool have_frames = false;
+
+  // temporal
+  uint32_t *d_order = nullptr;
+  float *d_mask = nullptr, *d_npairs = nullptr;
+  float2 *d_mspec = nullptr;
+  char *h_meta = nullptr;              // pinned staging for order/mask/npairs/mspec
+  size_t meta_bytes = 0;
+  int4 *d_items = nullptr;             // bin-sorted (mode, kx, ky, bin)
+  int4 *d_units = nullptr;             // fused-path units
+  int nunits = 0;
+  int *d_bin_units = nullptr;          // [NB+1]
+  uint32_t *d_offsets = nullptr, *d_nmodes = nullptr;
+  int4 *d_units_full = nullptr;
+  int nunits_full = 0;
+  int *d_counter = nullptr;
+  double *d_partials = nullptr;
+  double *d_radD = nullptr, *d_radP = nullptr, *d_radDrift = nullptr;
+  float *d_fullD = nullptr, *d_fullP = nullptr;
+  float2 *d_fullC = nullptr;
+  bool full_valid = false, radial_valid = false;
+};
+
+static int fail(ddm_engine *h, int code, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  if (h) h->err = buf;
+  return code;
+}
+
+#define CK(call)                                                                     \
+  do {                                                                               \
+    cudaError_t e_ = (call);                                                         \
+    if (e_ != cudaSuccess)                                                           \
+      return fail(h, DDM_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_));  \
+  } while (0)
+
+#define CKL(call)                                                                    \
+  do {                                                                               \
+    cudaError_t e_ = (call);                                                         \
+    h->launches++;                                                                   \
+    if (e_ != cudaSuccess)                                                           \
+      return fail(h, DDM_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_));  \
+  } while (0)
+
+template <typename T>
+static int dalloc(ddm_engine *h, T **p, size_t count) {
+  if (count == 0) count = 1;
+  cudaError_t e = cudaMalloc((void **)p, sizeof(T) * count);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(h, DDM_ERR_NOMEM, "cudaMalloc of %zu bytes failed: %s", sizeof(T) * count,
+                cudaGetErrorString(e));
+  }
+  return DDM_OK;
+}
+
+static bool is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
+
+static void release(ddm_engine *h) {
+  if (!h) return;
+  cudaSetDevice(h->device);
+  if (h->own_stream) cudaStreamSynchronize(h->own_stream);
+  if (h->copy_stream) cudaStreamSynchronize(h->copy_stream);
+  void *dev[] = {h->d_hist, h->d_rows, h->d_rowsum, h->d_means, h->d_win, h->d_wys, h->d_ninv,
+                 h->d_invtot, h->d_tw_s, h->d_tw_t, h->d_wcorr4, h->d_wcorr_full, h->d_smask,
+                 h->d_stage[0], h->d_stage[1], h->d_slots, h->d_order, h->d_mask, h->d_npairs,
+                 h->d_mspec, h->d_items, h->d_units, h->d_bin_units, h->d_offsets, h->d_nmodes,
+                 h->d_units_full, h->d_counter, h->d_partials, h->d_radD, h->d_radP,
+                 h->d_radDrift, h->d_fullD, h->d_fullP, h->d_fullC};
+  for (void *p : dev)
+    if (p) cudaFree(p);
+  if (h->h_slots) cudaFreeHost(h->h_slots);
+  if (h->h_meta) cudaFreeHost(h->h_meta);
+  for (int i = 0; i < NSTAGE; i++) {
+    if (h->ready_ev[i]) cudaEventDestroy(h->ready_ev[i]);
+    if (h->free_ev[i]) cudaEventDestroy(h->free_ev[i]);
+  }
+  for (cudaEvent_t e : h->inflight) cudaEventDestroy(e);
+  if (h->meta_ev) cudaEventDestroy(h->meta_ev);
+  if (h->own_stream) cudaStreamDestroy(h->own_stream);
+  if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
+  delete h;
+}
+
+static int build_units(ddm_engine *h) {
+  // fused path: runs of up to U modes inside one bin, bins in order
+  const int NB = h->g.NB;
+  const int total = (int)h->bins.offsets[NB];
+  const int grid = std::max(1, temporal_max_grid(h->g.TPAD, h->g.L, false));
+  int U = total / (3 * grid);
+  U = std::max(16, std::min(256, U + (U & 1)));
+  std::vector<int4> units;
+  std::vector<int> bin_units(NB + 1, 0);
+  for (int b = 0; b < NB; b++) {
+    bin_units[b] = (int)units.size();
+    const int i0 = (int)h->bins.offsets[b], i1 = (int)h->bins.offsets[b + 1];
+    for (int i = i0; i < i1; i += U) units.push_back(make_int4(i, std::min(U, i1 - i), b, 0));
+  }
+  bin_units[NB] = (int)units.size();
+  h->nunits = (int)units.size();
+  std::vector<int4> items(std::max(total, 1));
+  for (int i = 0; i < total; i++) {
+    const int32_t *m = &h->bins.modes[4 * (size_t)i];
+    items[i] = make_int4(m[0], m[1], m[2], 0);
+  }
+  for (int b = 0; b < NB; b++)
+    for (uint32_t i = h->bins.offsets[b]; i < h->bins.offsets[b + 1]; i++) items[i].w = b;
+  // full path: all modes in runs of 64
+  std::vector<int4> uf;
+  for (int m = 0; m < h->modes; m += 64) uf.push_back(make_int4(m, std::min(64, h->modes - m), -1, 0));
+  h->nunits_full = (int)uf.size();
+  int rc;
+  if ((rc = dalloc(h, &h->d_items, items.size())) || (rc = dalloc(h, &h->d_units, units.size())) ||
+      (rc = dalloc(h, &h->d_bin_units, NB + 1)) || (rc = dalloc(h, &h->d_offsets, NB + 1)) ||
+      (rc = dalloc(h, &h->d_nmodes, NB)) || (rc = dalloc(h, &h->d_units_full, uf.size())) ||
+      (rc = dalloc(h, &h->d_counter, 1)) ||
+      (rc = dalloc(h, &h->d_partials, (size_t)h->nunits * PFIELDS * h->g.L + h->nunits)))
+    return rc;
+  CK(cudaMemcpy(h->d_items, items.data(), sizeof(int4) * items.size(), cudaMemcpyHostToDevice));
+  if (!units.empty())
+    CK(cudaMemcpy(h->d_units, units.data(), sizeof(int4) * units.size(), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(h->d_bin_units, bin_units.data(), sizeof(int) * (NB + 1), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(h->d_offsets, h->bins.offsets.data(), sizeof(uint32_t) * (NB + 1), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(h->d_nmodes, h->bins.nModes.data(), sizeof(uint32_t) * NB, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(h->d_units_full, uf.data(), sizeof(int4) * uf.size(), cudaMemcpyHostToDevice));
+  return DDM_OK;
+}
+
+// Uploads the spatial weighting: window, w(y)*scale is per call (scale), row
+// normalisers and the window-spectrum correction for the current mask.
+static int upload_mask_tables(ddm_engine *h, const uint8_t *mask) {
+  const int N = h->g.N, NH = h->NH;
+  const std::vector<double> w = blackman_harris(N);
+  std::vector<double> ninv(N);
+  double total = 0;
+  for (int y = 0; y < N; y++) {
+    double c = 0;
+    for (int x = 0; x < N; x++) c += mask ? (mask[(size_t)y * N + x] ? 1 : 0) : 1;
+    ninv[y] = c > 0 ? 1.0 / c : 0.0;
+    total += c;
+  }
+  const double invtot = total > 0 ? 1.0 / total : 0.0;
+  CK(cudaMemcpy(h->d_ninv, ninv.data(), sizeof(double) * N, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(h->d_invtot, &invtot, sizeof(double), cudaMemcpyHostToDevice));
+  if (!mask) {
+    if (h->d_smask) {
+      cudaFree(h->d_smask);
+      h->d_smask = nullptr;
+    }
+    if (h->d_wcorr_full) {
+      cudaFree(h->d_wcorr_full);
+      h->d_wcorr_full = nullptr;
+    }
+    return DDM_OK;
+  }
+  int rc;
+  if (!h->d_smask && (rc = dalloc(h, &h->d_smask, (size_t)N * N))) return rc;
+  if (!h->d_wcorr_full && (rc = dalloc(h, &h->d_wcorr_full, (size_t)N * NH))) return rc;
+  std::vector<uint8_t> m01((size_t)N * N);
+  for (size_t i = 0; i < m01.size(); i++) m01[i] = mask[i] ? 1 : 0;
+  CK(cudaMemcpy(h->d_smask, m01.data(), m01.size(), cudaMemcpyHostToDevice));
+  // per-row window spectrum W_y(kx) = sum_x w(x) S(x,y) exp(-2 pi i kx x/N)
+  std::vector<float> wc(2 * (size_t)N * NH);
+  std::vector<cd> row(N);
+  for (int y = 0; y < N; y++) {
+    for (int x = 0; x < N; x++) row[x] = cd(w[x] * m01[(size_t)y * N + x], 0);
+    host_fft(row, false);
+    for (int kx = 0; kx < NH; kx++) {
+      wc[2 * ((size_t)y * NH + kx)] = (float)row[kx].real();
+      wc[2 * ((size_t)y * NH + kx) + 1] = (float)row[kx].imag();
+    }
+  }
+  CK(cudaMemcpy(h->d_wcorr_full, wc.data(), sizeof(float) * wc.size(), cudaMemcpyHostToDevice));
+  return DDM_OK;
+}
+
+extern "C" const char *ddm_create_error(void) { return g_create_error.c_str(); }
+
+extern "C" int ddm_create(const ddm_geometry *geometry, ddm_engine **out) {
+  g_create_error.clear();
+  if (!geometry || !out) {
+    g_create_error = "ddm_create: null argument";
+    return DDM_ERR_ARG;
+  }
+  *out = nullptr;
+  ddm_geometry g = *geometry;
+  if (g.TPAD == 0) {
+    g.TPAD = 1;
+    while (g.TPAD < 2 * g.T) g.TPAD <<= 1;
+  }
+  char msg[256] = {0};
+  if (!is_pow2(g.N) || g.N < 64 || g.N > 2048)
+    snprintf(msg, sizeof msg, "N = %d: must be a power of two in [64, 2048]", g.N);
+  else if (g.T < 2 || !is_pow2(g.TPAD) || g.TPAD < 128 || g.TPAD > 8192 || 2 * g.T > g.TPAD)
+    snprintf(msg, sizeof msg, "T = %d, TPAD = %d: need TPAD a power of two in [128, 8192] and TPAD >= 2T",
+             g.T, g.TPAD);
+  else if (g.L < 2 || g.L > g.T)
+    snprintf(msg, sizeof msg, "L = %d: need 2 <= L <= T", g.L);
+  else if (g.NB < 1 || !(g.kmax > g.kmin) || g.kmin < 0)
+    snprintf(msg, sizeof msg, "bins: need NB >= 1 and 0 <= kmin < kmax");
+  else if (g.knodes < 1 || g.knodes > 16)
+    snprintf(msg, sizeof msg, "knodes = %d: need 1..16", g.knodes);
+  if (msg[0]) {
+    g_create_error = msg;
+    return DDM_ERR_ARG;
+  }
+  int dev = 0, ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    g_create_error = "no CUDA device";
+    return DDM_ERR_NODEV;
+  }
+  cudaGetDevice(&dev);
+  cudaDeviceProp prop;
+  cudaGetDeviceProperties(&prop, dev);
+  if (prop.major != 10) {
+    snprintf(msg, sizeof msg, "device %d is sm_%d%d; this library is built for sm_100a", dev,
+             prop.major, prop.minor);
+    g_create_error = msg;
+    return DDM_ERR_NODEV;
+  }
+
+  ddm_engine *h = new ddm_engine();
+  h->g = g;
+  h->device = dev;
+  h->NH = g.N / 2 + 1;
+  h->NHB = (h->NH + KB - 1) / KB;
+  h->modes = g.N * h->NH;
+  {
+    const size_t per = (size_t)h->NHB * g.N * KB * sizeof(float2);
+    const size_t target = 32u << 20;  // rows scratch stays L2-resident
+    h->chunk = (int)std::max<size_t>(4, std::min<size_t>(64, target / per));
+  }
+  h->bins = make_bins(g.N, g.NB, g.kmin, g.kmax, g.knodes);
+  int rc = DDM_OK;
+  auto bail = [&](int code) {
+    g_create_error = h->err;
+    release(h);
+    return code;
+  };
+  if (cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking) != cudaSuccess) {
+    h->err = "stream creation failed";
+    return bail(DDM_ERR_CUDA);
+  }
+  h->stream = h->own_stream;
+  for (int i = 0; i < NSTAGE; i++) {
+    cudaEventCreateWithFlags(&h->ready_ev[i], cudaEventDisableTiming);
+    cudaEventCreateWithFlags(&h->free_ev[i], cudaEventDisableTiming);
+  }
+  cudaEventCreateWithFlags(&h->meta_ev, cudaEventDisableTiming);
+  const int N = g.N;
+  h->stage_bytes = (size_t)h->chunk * N * N * sizeof(float);
+  if ((rc = dalloc(h, &h->d_hist, (size_t)h->modes * g.T)) ||
+      (rc = dalloc(h, &h->d_rows, (size_t)h->chunk * h->NHB * N * KB)) ||
+      (rc = dalloc(h, &h->d_rowsum, (size_t)h->chunk * N)) ||
+      (rc = dalloc(h, &h->d_means, (size_t)h->chunk)) || (rc = dalloc(h, &h->d_win, N)) ||
+      (rc = dalloc(h, &h->d_wys, N)) || (rc = dalloc(h, &h->d_ninv, N)) ||
+      (rc = dalloc(h, &h->d_invtot, 1)) || (rc = dalloc(h, &h->d_tw_s, N)) ||
+      (rc = dalloc(h, &h->d_tw_t, g.TPAD)) || (rc = dalloc(h, &h->d_wcorr4, 4)) ||
+      (rc = dalloc(h, &h->d_slots, (size_t)NSTAGE * h->chunk)) ||
+      (rc = dalloc(h, (char **)&h->d_stage[0], h->stage_bytes)) ||
+      (rc = dalloc(h, (char **)&h->d_stage[1], h->stage_bytes)) ||
+      (rc = dalloc(h, &h->d_order, g.T)) || (rc = dalloc(h, &h->d_mask, g.T)) ||
+      (rc = dalloc(h, &h->d_npairs, g.L)) || (rc = dalloc(h, &h->d_mspec, g.TPAD)) ||
+      (rc = dalloc(h, &h->d_radD, (size_t)g.NB * g.L)) || (rc = dalloc(h, &h->d_radP, g.NB)) ||
+      (rc = dalloc(h, &h->d_radDrift, (size_t)g.NB * g.L * DRIFT)))
+    return bail(rc);
+  h->meta_bytes = sizeof(uint32_t) * g.T + sizeof(float) * g.T + sizeof(float) * g.L +
+                  sizeof(float2) * g.TPAD;
+  if (cudaHostAlloc((void **)&h->h_meta, h->meta_bytes, cudaHostAllocDefault) != cudaSuccess ||
+      cudaHostAlloc((void **)&h->h_slots, sizeof(int) * NSTAGE * h->chunk, cudaHostAllocDefault) !=
+          cudaSuccess) {
+    h->err = "pinned host allocation failed";
+    return bail(DDM_ERR_NOMEM);
+  }
+  // tables
+  const std::vector<double> w = blackman_harris(N);
+  std::vector<float> wf(N);
+  for (int i = 0; i < N; i++) wf[i] = (float)w[i];
+  std::vector<float> tws = twiddle_table(N), twt = twiddle_table(g.TPAD);
+  // DFT of the window at kx = 0..3 (zero beyond for the 4-term window)
+  float wc4[8];
+  for (int kx = 0; kx < 4; kx++) {
+    double re = 0, im = 0;
+    for (int x = 0; x < N; x++) {
+      const double a = -2.0 * M_PI * kx * x / N;
+      re += w[x] * std::cos(a);
+      im += w[x] * std::sin(a);
+    }
+    wc4[2 * kx] = (float)re;
+    wc4[2 * kx + 1] = (float)im;
+  }
+  if (cudaMemcpy(h->d_win, wf.data(), sizeof(float) * N, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(h->d_tw_s, tws.data(), sizeof(float) * tws.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(h->d_tw_t, twt.data(), sizeof(float) * twt.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(h->d_wcorr4, wc4, sizeof wc4, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemset(h->d_hist, 0, sizeof(float2) * (size_t)h->modes * g.T) != cudaSuccess) {
+    h->err = "table upload failed";
+    return bail(DDM_ERR_CUDA);
+  }
+  if ((rc = upload_mask_tables(h, nullptr)) || (rc = build_units(h))) return bail(rc);
+  *out = h;
+  return DDM_OK;
+}
+
+extern "C" void ddm_destroy(ddm_engine *h) { release(h); }
+
+extern "C" const char *ddm_last_error(const ddm_engine *h) { return h ? h->err.c_str() : ""; }
+
+extern "C" int ddm_get_geometry(const ddm_engine *h, ddm_geometry *out) {
+  if (!h || !out) return DDM_ERR_ARG;
+  *out = h->g;
+  return DDM_OK;
+}
+
+extern "C" int ddm_bins_count(const ddm_engine *h) {
+  return h ? (int)h->bins.offsets[h->g.NB] : -1;
+}
+
+extern "C" int ddm_get_bins(const ddm_engine *h, uint32_t *binOffsets, int32_t *binModes,
+                            double *kCenter, uint32_t *nModes, double *kNodes) {
+  if (!h) return DDM_ERR_ARG;
+  const BinTable &b = h->bins;
+  if (binOffsets) memcpy(binOffsets, b.offsets.data(), sizeof(uint32_t) * b.offsets.size());
+  if (binModes) memcpy(binModes, b.modes.data(), sizeof(int32_t) * b.modes.size());
+  if (kCenter) memcpy(kCenter, b.kCenter.data(), sizeof(double) * b.kCenter.size());
+  if (nModes) memcpy(nModes, b.nModes.data(), sizeof(uint32_t) * b.nModes.size());
+  if (kNodes) memcpy(kNodes, b.kNodes.data(), sizeof(double) * b.kNodes.size());
+  return DDM_OK;
+}
+
+extern "C" int ddm_set_stream(ddm_engine *h, void *stream) {
+  if (!h) return DDM_ERR_ARG;
+  cudaSetDevice(h->device);
+  cudaStreamSynchronize(h->stream);
+  h->stream = stream ? (cudaStream_t)stream : h->own_stream;
+  return DDM_OK;
+}
+
+extern "C" int64_t ddm_kernel_launches(const ddm_engine *h) { return h ? h->launches : 0; }
+
+// Rows + columns for one chunk of frames already in device memory.
+static int launch_chunk(ddm_engine *h, const void *dframes, int dtype, int n, const int *d_slots,
+                        float scale) {
+  const int N = h->g.N;
+  // w(y) * scale for this call's scale
+  RowParams rp{};
+  rp.frames = dframes;
+  rp.frame_stride = (long long)N * N;
+  rp.nframes = n;
+  rp.win = h->d_win;
+  rp.wys = h->d_wys;
+  rp.ninv = h->d_ninv;
+  rp.smask = h->d_smask;
+  rp.tw = h->d_tw_s;
+  rp.rows = h->d_rows;
+  rp.rowsum = h->d_rowsum;
+  CKL(launch_rows(N, dtype, rp, h->stream));
+  ColParams cp{};
+  cp.rows = h->d_rows;
+  cp.rowsum = h->d_rowsum;
+  cp.ninv = h->d_ninv;
+  cp.inv_total = h->d_invtot;
+  cp.wys = h->d_wys;
+  cp.wcorr = h->d_smask ? h->d_wcorr_full : h->d_wcorr4;
+  cp.wcorr_full = h->d_smask ? 1 : 0;
+  cp.slots = d_slots;
+  cp.tw = h->d_tw_s;
+  cp.hist = h->d_hist;
+  cp.means = h->d_means;
+  cp.scale = scale;
+  cp.nframes = n;
+  cp.T = h->g.T;
+  cp.NH = h->NH;
+  cp.NHB = h->NHB;
+  CKL(launch_cols(N, cp, h->stream));
+  h->last_mean_index = n - 1;
+  h->have_frames = true;
+  return DDM_OK;
+}
+
+static int set_scale(ddm_engine *h, float scale) {
+  if (!(scale > 0) || !std::isfinite(scale)) return fail(h, DDM_ERR_ARG, "scale must be finite and > 0");
+  if ((double)scale == h->scale_last && h->have_frames) return DDM_OK;
+  const int N = h->g.N;
+  const std::vector<double> w = blackman_harris(N);
+  std::vector<float> wys(N);
+  for (int y = 0; y < N; y++) wys[y] = (float)(w[y] * (double)scale);
+  // ordered on the engine stream behind earlier chunks that read d_wys
+  CK(cudaStreamSynchronize(h->stream));
+  CK(cudaMemcpy(h->d_wys, wys.data(), sizeof(float) * N, cudaMemcpyHostToDevice));
+  h->scale_last = scale;
+  return DDM_OK;
+}
+
+static int check_frames_args(ddm_engine *h, const void *frames, int dtype, int n, const int32_t *slots) {
+  if (!frames && n > 0) return fail(h, DDM_ERR_ARG, "frames is NULL");
+  if (dtype < 0 || dtype > 2) return fail(h, DDM_ERR_ARG, "dtype %d: expected 0 (u8), 1 (u16), 2 (f32)", dtype);
+  if (n < 0) return fail(h, DDM_ERR_ARG, "n = %d < 0", n);
+  if (n > 0 && !slots) return fail(h, DDM_ERR_ARG, "slots is NULL");
+  for (int i = 0; i < n; i++)
+    if (slots[i] < 0) return fail(h, DDM_ERR_ARG, "slot %d < 0", slots[i]);
+  return DDM_OK;
+}
+
+static void note_inflight(ddm_engine *h) {
+  cudaEvent_t e;
+  if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) == cudaSuccess) {
+    cudaEventRecord(e, h->stream);
+    h->inflight.push_back(e);
+  }
+}
+
+static int dtype_size(int dtype) { return dtype == 0 ? 1 : dtype == 1 ? 2 : 4; }
+
+static int ingest_impl(ddm_engine *h, const void *frames, int dtype, int n, const int32_t *slots,
+                       float scale, bool device) {
+  cudaSetDevice(h->device);
+  int rc = check_frames_args(h, frames, dtype, n, slots);
+  if (rc) return rc;
+  if ((rc = set_scale(h, scale))) return rc;
+  const int N = h->g.N;
+  const size_t fbytes = (size_t)N * N * dtype_size(dtype);
+  for (int c0 = 0, ci = 0; c0 < n; c0 += h->chunk, ci++) {
+    const int m = std::min(h->chunk, n - c0);
+    const int s = ci % NSTAGE;
+    // slots of this chunk: pinned host -> device on the copy stream
+    CK(cudaEventSynchronize(h->free_ev[s]));
+    int *hs = h->h_slots + (size_t)s * h->chunk;
+    for (int i = 0; i < m; i++) hs[i] = slots[c0 + i] % h->g.T;
+    int *ds = h->d_slots + (size_t)s * h->chunk;
+    CK(cudaMemcpyAsync(ds, hs, sizeof(int) * m, cudaMemcpyHostToDevice, h->copy_stream));
+    const void *src;
+    if (device) {
+      src = (const char *)frames + (size_t)c0 * fbytes;
+    } else {
+      CK(cudaMemcpyAsync(h->d_stage[s], (const char *)frames + (size_t)c0 * fbytes, m * fbytes,
+                         cudaMemcpyHostToDevice, h->copy_stream));
+      src = h->d_stage[s];
+    }
+    CK(cudaEventRecord(h->ready_ev[s], h->copy_stream));
+    CK(cudaStreamWaitEvent(h->stream, h->ready_ev[s], 0));
+    if ((rc = launch_chunk(h, src, dtype, m, ds, scale))) return rc;
+    CK(cudaEventRecord(h->free_ev[s], h->stream));
+  }
+  // the caller's host buffer is free once the copies have run
+  CK(cudaStreamSynchronize(h->copy_stream));
+  note_inflight(h);
+  h->radial_valid = false;
+  return DDM_OK;
+}
+
+extern "C" int ddm_ingest_frames(ddm_engine *h, const void *frames, int32_t dtype, int32_t n,
+                                 const int32_t *slots, float scale) {
+  if (!h) return DDM_ERR_ARG;
+  return ingest_impl(h, frames, dtype, n, slots, scale, false);
+}
+
+extern "C" int ddm_ingest_frames_device(ddm_engine *h, const void *frames, int32_t dtype, int32_t n,
+                                        const int32_t *slots, float scale) {
+  if (!h) return DDM_ERR_ARG;
+  return ingest_impl(h, frames, dtype, n, slots, scale, true);
+}
+
+static int prune_inflight(ddm_engine *h) {
+  std::vector<cudaEvent_t> keep;
+  for (cudaEvent_t e : h->inflight) {
+    if (cudaEventQuery(e) == cudaSuccess)
+      cudaEventDestroy(e);
+    else
+      keep.push_back(e);
+  }
+  cudaGetLastError();  // cudaErrorNotReady is not an error here
+  h->inflight.swap(keep);
+  return (int)h->inflight.size();
+}
+
+extern "C" int ddm_pending(ddm_engine *h) { return h ? prune_inflight(h) : 0; }
+
+extern "C" int ddm_wait_for_capacity(ddm_engine *h) {
+  if (!h) return DDM_ERR_ARG;
+  while (prune_inflight(h) > MAX_PENDING) CK(cudaEventSynchronize(h->inflight.front()));
+  return DDM_OK;
+}
+
+extern "C" int64_t ddm_throttled(const ddm_engine *h) { return h ? h->throttled : 0; }
+
+extern "C" int ddm_ingest_luma(ddm_engine *h, const float *luma, int32_t slot, int32_t *accepted) {
+  if (!h) return DDM_ERR_ARG;
+  if (accepted) *accepted = 0;
+  if (!luma) return fail(h, DDM_ERR_ARG, "ingestLuma expects %d values", h->g.N * h->g.N);
+  if (prune_inflight(h) > MAX_PENDING) {
+    h->throttled++;
+    return DDM_OK;
+  }
+  const int32_t s = slot;
+  int rc = ingest_impl(h, luma, DDM_F32, 1, &s, 1.0f, false);
+  if (rc == DDM_OK && accepted) *accepted = 1;
+  return rc;
+}
+
+extern "C" int ddm_set_spatial_mask(ddm_engine *h, const uint8_t *mask) {
+  if (!h) return DDM_ERR_ARG;
+  cudaSetDevice(h->device);
+  CK(cudaStreamSynchronize(h->stream));
+  return upload_mask_tables(h, mask);
+}
+
+static int temporal_impl(ddm_engine *h, const uint32_t *order, const float *mask, int full) {
+  cudaSetDevice(h->device);
+  const int T = h->g.T, L = h->g.L, TPAD = h->g.TPAD;
+  if (!order || !mask) return fail(h, DDM_ERR_ARG, "computeTemporal: order/mask must have length %d", T);
+  for (int j = 0; j < T; j++)
+    if (order[j] >= (uint32_t)T) return fail(h, DDM_ERR_ARG, "order[%d] = %u is not a slot < %d", j, order[j], T);
+  std::vector<float> npairs, mspec;
+  temporal_meta(mask, T, TPAD, L, npairs, mspec);
+  // the pinned staging may still be read by the previous analysis' copies
+  CK(cudaEventSynchronize(h->meta_ev));
+  char *p = h->h_meta;
+  uint32_t *ho = (uint32_t *)p;
+  float *hm = (float *)(ho + T);
+  float *hn = hm + T;
+  float *hs = hn + L;
+  memcpy(ho, order, sizeof(uint32_t) * T);
+  for (int j = 0; j < T; j++) hm[j] = mask[j] != 0.f ? 1.f : 0.f;
+  memcpy(hn, npairs.data(), sizeof(float) * L);
+  memcpy(hs, mspec.data(), sizeof(float) * 2 * TPAD);
+  CK(cudaMemcpyAsync(h->d_order, ho, sizeof(uint32_t) * T, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->d_mask, hm, sizeof(float) * T, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->d_npairs, hn, sizeof(float) * L, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->d_mspec, hs, sizeof(float2) * TPAD, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaEventRecord(h->meta_ev, h->stream));
+
+  TemporalParams tp{};
+  tp.hist = h->d_hist;
+  tp.order = h->d_order;
+  tp.mask = h->d_mask;
+  tp.npairs = h->d_npairs;
+  tp.mspec = h->d_mspec;
+  tp.tw = h->d_tw_t;
+  tp.unit_counter = h->d_counter;
+  tp.T = T;
+  tp.L = L;
+  int rc;
+  if (full) {
+    if (!h->d_fullD) {
+      if ((rc = dalloc(h, &h->d_fullD, (size_t)h->modes * L)) ||
+          (rc = dalloc(h, &h->d_fullC, (size_t)h->modes * L)) || (rc = dalloc(h, &h->d_fullP, h->modes)))
+        return rc;
+    }
+    tp.items = nullptr;
+    tp.units = h->d_units_full;
+    tp.nunits = h->nunits_full;
+    tp.outD = h->d_fullD;
+    tp.outC = h->d_fullC;
+    tp.outP = h->d_fullP;
+    const int grid = std::min(temporal_max_grid(TPAD, L, true), h->nunits_full);
+    CK(cudaMemsetAsync(h->d_counter, 0, sizeof(int), h->stream));
+    CKL(launch_temporal(TPAD, L, true, tp, std::max(grid, 1), h->stream));
+    RadialFullParams rp{};
+    rp.D = h->d_fullD;
+    rp.C = h->d_fullC;
+    rp.P = h->d_fullP;
+    rp.items = h->d_items;
+    rp.offsets = h->d_offsets;
+    rp.NB = h->g.NB;
+    rp.L = L;
+    rp.oD = h->d_radD;
+    rp.oP = h->d_radP;
+    rp.odrift = h->d_radDrift;
+    CKL(launch_radial_full(rp, h->stream));
+    h->full_valid = true;
+  } else {
+    tp.items = h->d_items;
+    tp.units = h->d_units;
+    tp.nunits = h->nunits;
+    tp.partials = h->d_partials;
+    const int grid = std::min(temporal_max_grid(TPAD, L, false), h->nunits);
+    CK(cudaMemsetAsync(h->d_counter, 0, sizeof(int), h->stream));
+    if (h->nunits > 0) CKL(launch_temporal(TPAD, L, false, tp, std::max(grid, 1), h->stream));
+    ReduceParams rp{};
+    rp.partials = h->d_partials;
+    rp.bin_units = h->d_bin_units;
+    rp.nmodes = h->d_nmodes;
+    rp.nunits = h->nunits;
+    rp.NB = h->g.NB;
+    rp.L = L;
+    rp.D = h->d_radD;
+    rp.P = h->d_radP;
+    rp.drift = h->d_radDrift;
+    CKL(launch_reduce(rp, h->stream));
+    h->full_valid = false;
+  }
+  h->radial_valid = true;
+  return DDM_OK;
+}
+
+extern "C" int ddm_compute_temporal_async(ddm_engine *h, const uint32_t *order, const float *mask,
+                                          int32_t full) {
+  if (!h) return DDM_ERR_ARG;
+  return temporal_impl(h, order, mask, full);
+}
+
+extern "C" int ddm_compute_temporal(ddm_engine *h, const uint32_t *order, const float *mask,
+                                    int32_t full) {
+  if (!h) return DDM_ERR_ARG;
+  int rc = temporal_impl(h, order, mask, full);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(h->stream));
+  return DDM_OK;
+}
+
+extern "C" int ddm_read_radial(ddm_engine *h, double *D, double *P, double *drift) {
+  if (!h) return DDM_ERR_ARG;
+  cudaSetDevice(h->device);
+  if (!h->radial_valid) return fail(h, DDM_ERR_STATE, "readRadial: no computeTemporal since the last ingest");
+  const size_t NB = h->g.NB, L = h->g.L;
+  if (D) CK(cudaMemcpyAsync(D, h->d_radD, sizeof(double) * NB * L, cudaMemcpyDeviceToHost, h->stream));
+  if (P) CK(cudaMemcpyAsync(P, h->d_radP, sizeof(double) * NB, cudaMemcpyDeviceToHost, h->stream));
+  if (drift)
+    CK(cudaMemcpyAsync(drift, h->d_radDrift, sizeof(double) * NB * L * DRIFT, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return DDM_OK;
+}
+
+extern "C" int ddm_read_history(ddm_engine *h, float *out) {
+  if (!h || !out) return DDM_ERR_ARG;
+  cudaSetDevice(h->device);
+  CK(cudaMemcpyAsync(out, h->d_hist, sizeof(float2) * (size_t)h->modes * h->g.T, cudaMemcpyDeviceToHost,
+                     h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return DDM_OK;
+}
+
+extern "C" int ddm_read_temporal_full(ddm_engine *h, float *D, float *C, float *P) {
+  if (!h) return DDM_ERR_ARG;
+  cudaSetDevice(h->device);
+  if (!h->full_valid)
+    return fail(h, DDM_ERR_STATE, "readTemporalFull: the last computeTemporal did not keep full outputs");
+  const size_t M = h->modes, L = h->g.L;
+  if (D) CK(cudaMemcpyAsync(D, h->d_fullD, sizeof(float) * M * L, cudaMemcpyDeviceToHost, h->stream));
+  if (C) CK(cudaMemcpyAsync(C, h->d_fullC, sizeof(float2) * M * L, cudaMemcpyDeviceToHost, h->stream));
+  if (P) CK(cudaMemcpyAsync(P, h->d_fullP, sizeof(float) * M, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return DDM_OK;
+}
+
+extern "C" int ddm_read_mean(ddm_engine *h, double *mean) {
+  if (!h || !mean) return DDM_ERR_ARG;
+  cudaSetDevice(h->device);
+  if (h->last_mean_index < 0) return fail(h, DDM_ERR_STATE, "readMean: no frame ingested yet");
+  CK(cudaMemcpyAsync(mean, h->d_means + h->last_mean_index, sizeof(double), cudaMemcpyDeviceToHost,
+                     h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return DDM_OK;
+}
+
+extern "C" int ddm_idle(ddm_engine *h) {
+  if (!h) return DDM_ERR_ARG;
+  cudaSetDevice(h->device);
+  CK(cudaStreamSynchronize(h->copy_stream));
+  CK(cudaStreamSynchronize(h->stream));
+  prune_inflight(h);
+  return DDM_OK;
+}

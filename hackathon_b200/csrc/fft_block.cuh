@@ -1,0 +1,166 @@
+// Block-cooperative FP32 FFTs for sm_100a.
+//
+// An n-point complex transform is spread over n/8 threads, each holding 8
+// points in registers. Stages are radix-8 Stockham butterflies computed in
+// registers (with a final radix-4 or radix-2 stage when log2(n) is not a
+// multiple of 3); between stages the points are exchanged through shared
+// memory, ping-ponging between two padded buffers so each stage needs one
+// __syncthreads. The output is in natural order, like the reference's
+// radix-2 Stockham (motility-ddm/src/fft.js:59-93): same transform, unscaled
+// in both directions, fewer passes.
+//
+// Layout contract: on entry to a stage thread t holds v[q] = x[t + q*n/8],
+// q = 0..7, so a caller can feed the first stage straight from registers and
+// read the natural-order result from shared memory at pad(k).
+//
+// Twiddles come from a table tw[j] = exp(-2*pi*i*j/n), j < n, computed on the
+// host in FP64 and rounded once to FP32 (as the reference's gpuTwiddles,
+// ddm_ref.js:566-574); no sin/cos is evaluated on the device.
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace ddm {
+
+// Shared-memory index with one float2 of padding every 8: keeps the radix-8
+// store patterns (stride 8, 64, 512) free of 64-bit bank conflicts.
+__device__ __forceinline__ int pad(int i) { return i + (i >> 3); }
+__host__ __device__ constexpr int padded(int n) { return n + n / 8; }
+
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+}
+// multiply by -i (forward) or +i (inverse)
+template <bool INV>
+__device__ __forceinline__ float2 rot(float2 a) {
+  return INV ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
+}
+
+template <int R, bool INV>
+struct Dft;
+
+template <bool INV>
+struct Dft<2, INV> {
+  static __device__ __forceinline__ void run(float2* a) {
+    const float2 t = a[0];
+    a[0] = cadd(t, a[1]);
+    a[1] = csub(t, a[1]);
+  }
+};
+
+template <bool INV>
+struct Dft<4, INV> {
+  static __device__ __forceinline__ void run(float2* a) {
+    const float2 s02 = cadd(a[0], a[2]), d02 = csub(a[0], a[2]);
+    const float2 s13 = cadd(a[1], a[3]), d13 = rot<INV>(csub(a[1], a[3]));
+    a[0] = cadd(s02, s13);
+    a[2] = csub(s02, s13);
+    a[1] = cadd(d02, d13);
+    a[3] = csub(d02, d13);
+  }
+};
+
+template <bool INV>
+struct Dft<8, INV> {
+  static __device__ __forceinline__ void run(float2* a) {
+    float2 e[4] = {a[0], a[2], a[4], a[6]};
+    float2 o[4] = {a[1], a[3], a[5], a[7]};
+    Dft<4, INV>::run(e);
+    Dft<4, INV>::run(o);
+    const float c = 0.70710678118654752f;
+    // o[k] *= W8^k, W8 = exp(-+ 2 pi i / 8)
+    float2 w1, w3;
+    if (!INV) {
+      w1 = make_float2(c * (o[1].x + o[1].y), c * (o[1].y - o[1].x));
+      w3 = make_float2(c * (o[3].y - o[3].x), -c * (o[3].x + o[3].y));
+    } else {
+      w1 = make_float2(c * (o[1].x - o[1].y), c * (o[1].x + o[1].y));
+      w3 = make_float2(-c * (o[3].x + o[3].y), c * (o[3].x - o[3].y));
+    }
+    const float2 w2 = rot<INV>(o[2]);
+    a[0] = cadd(e[0], o[0]);
+    a[4] = csub(e[0], o[0]);
+    a[1] = cadd(e[1], w1);
+    a[5] = csub(e[1], w1);
+    a[2] = cadd(e[2], w2);
+    a[6] = csub(e[2], w2);
+    a[3] = cadd(e[3], w3);
+    a[7] = csub(e[3], w3);
+  }
+};
+
+// One radix-R Stockham stage at stride Ns. Thread t owns butterflies
+// j = t + i*n/8 (i < 8/R); butterfly j reads x[j + m*n/R] = v[i + (8/R)*m],
+// twiddles input m by exp(-+2*pi*i*m*(j%Ns)/(Ns*R)) and writes output m to
+// (j - j%Ns)*R + j%Ns + m*Ns.
+template <int n, int R, int Ns, bool INV>
+__device__ __forceinline__ void stage(float2 (&v)[8], int t, float2* __restrict__ out,
+                                      const float2* __restrict__ tw) {
+  constexpr int NT = n / 8;
+  constexpr int B = 8 / R;
+#pragma unroll
+  for (int i = 0; i < B; i++) {
+    const int j = t + i * NT;
+    const int k = j & (Ns - 1);
+    float2 a[R];
+#pragma unroll
+    for (int m = 0; m < R; m++) a[m] = v[i + B * m];
+    if (Ns > 1) {
+      constexpr int step = n / (Ns * R);
+#pragma unroll
+      for (int m = 1; m < R; m++) {
+        float2 w = __ldg(&tw[k * m * step]);
+        if (INV) w.y = -w.y;
+        a[m] = cmul(a[m], w);
+      }
+    }
+    Dft<R, INV>::run(a);
+    const int base = (j - k) * R + k;
+#pragma unroll
+    for (int m = 0; m < R; m++) out[pad(base + m * Ns)] = a[m];
+  }
+}
+
+template <int n>
+__device__ __forceinline__ void load8(float2 (&v)[8], int t, const float2* __restrict__ buf) {
+  constexpr int NT = n / 8;
+#pragma unroll
+  for (int q = 0; q < 8; q++) v[q] = buf[pad(t + q * NT)];
+}
+
+// Number of stages of an n-point transform (radix 8 while possible, then 4/2).
+__host__ __device__ constexpr int fft_stages(int n) {
+  int s = 0;
+  for (int ns = 1; ns < n; ns *= ((n / ns) >= 8 ? 8 : (n / ns))) s++;
+  return s;
+}
+
+template <int n, int Ns, bool INV>
+struct Stages {
+  // Runs the stages from stride Ns on; the stage writes `a`, the next one
+  // writes `b`. Ends with a __syncthreads after the last store.
+  static __device__ __forceinline__ void run(float2 (&v)[8], int t, float2* a, float2* b,
+                                             const float2* __restrict__ tw) {
+    constexpr int R = (n / Ns) >= 8 ? 8 : (n / Ns);
+    stage<n, R, Ns, INV>(v, t, a, tw);
+    __syncthreads();
+    if constexpr (Ns * R < n) {
+      load8<n>(v, t, a);
+      Stages<n, Ns * R, INV>::run(v, t, b, a, tw);
+    }
+  }
+};
+
+// Full n-point FFT of the 8 register points per thread (layout contract
+// above). Returns the buffer holding the natural-order result (read it at
+// pad(k)); the result lands in buf0 when the stage count is odd, else buf1.
+template <int n, bool INV>
+__device__ __forceinline__ float2* fft(float2 (&v)[8], int t, float2* buf0, float2* buf1,
+                                       const float2* __restrict__ tw) {
+  Stages<n, 1, INV>::run(v, t, buf0, buf1, tw);
+  return (fft_stages(n) & 1) ? buf0 : buf1;
+}
+
+}  // namespace ddm

@@ -1,0 +1,94 @@
+// Kernel parameter blocks and launchers shared by the engine.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace ddm {
+
+constexpr int KB = 2;       // kx columns per block of the row-spectrum scratch
+// frames per column-kernel CTA: 4 consecutive slots of a mode fill one 32 B
+// sector; 2 at N = 2048 to fit the CTA's tiles in shared memory
+__host__ __device__ constexpr int col_frames(int N) { return N >= 2048 ? 2 : 4; }
+constexpr int DRIFT = 8;    // drift fields per (bin, lag) (ddm_ref.js:28)
+constexpr int PFIELDS = 9;  // D + 8 drift sums per lag in a partial record
+
+struct RowParams {
+  const void* frames;      // [nframes][N][N] u8 / u16 / f32
+  long long frame_stride;  // elements between frames
+  int nframes;
+  const float* win;        // w(x), FP32 (from the FP64 window)
+  const float* wys;        // w(y) * scale
+  const double* ninv;      // 1 / (valid pixels of row y)
+  const uint8_t* smask;    // spatial mask [N][N] or nullptr (extension)
+  const float2* tw;        // exp(-2 pi i j / N), j < N
+  float2* rows;            // [nframes][NHB][N][KB]
+  double* rowsum;          // [nframes][N] masked row sums of the raw values
+};
+
+struct ColParams {
+  const float2* rows;      // [nframes][NHB][N][KB]
+  const double* rowsum;    // [nframes][N]
+  const double* ninv;      // [N]
+  const double* inv_total; // [1] 1 / (valid pixels of the frame)
+  const float* wys;        // w(y) * scale
+  const float2* wcorr;     // [N][NH] window spectrum per row, or [4] (separable)
+  int wcorr_full;          // 1: wcorr is per row and per kx (spatial mask)
+  const int* slots;        // [nframes] ring slot of each frame
+  const float2* tw;        // exp(-2 pi i j / N)
+  float2* hist;            // [modes][T]
+  double* means;           // [nframes] frame mean luma (out)
+  float scale;
+  int nframes, T, NH, NHB;
+};
+
+struct TemporalParams {
+  const float2* hist;      // [modes][T]
+  const uint32_t* order;   // [T]
+  const float* mask;       // [T] 0/1
+  const float* npairs;     // [L] exact valid-pair counts N(tau)
+  const float2* mspec;     // [TPAD] FFT of the zero-padded mask
+  const float2* tw;        // exp(-2 pi i j / TPAD)
+  const int4* items;       // (mode, kx, ky, bin); nullptr: item i is mode i
+  const int4* units;       // (first item, count, bin, 0)
+  int nunits;
+  int* unit_counter;
+  double* partials;        // [nunits][PFIELDS][L] + P at [nunits*PFIELDS*L + u]
+  float* outD;             // [modes][L] (full outputs) or nullptr
+  float2* outC;            // [modes][L]
+  float* outP;             // [modes]
+  int T, L;
+};
+
+struct ReduceParams {
+  const double* partials;
+  const int* bin_units;    // [NB+1] unit range of each bin
+  const uint32_t* nmodes;  // [NB]
+  int nunits, NB, L;
+  double* D;               // [NB][L]
+  double* P;               // [NB]
+  double* drift;           // [NB][L][8]
+};
+
+struct RadialFullParams {
+  const float* D;          // [modes][L]
+  const float2* C;         // [modes][L]
+  const float* P;          // [modes]
+  const int4* items;       // bin-sorted (mode, kx, ky, bin)
+  const uint32_t* offsets; // [NB+1]
+  int NB, L;
+  double* oD;
+  double* oP;
+  double* odrift;
+};
+
+// launchers (return cudaGetLastError())
+cudaError_t launch_rows(int N, int dtype, const RowParams& p, cudaStream_t s);
+cudaError_t launch_cols(int N, const ColParams& p, cudaStream_t s);
+cudaError_t launch_temporal(int TPAD, int L, bool full, const TemporalParams& p, int grid,
+                            cudaStream_t s);
+int temporal_max_grid(int TPAD, int L, bool full);
+cudaError_t launch_reduce(const ReduceParams& p, cudaStream_t s);
+cudaError_t launch_radial_full(const RadialFullParams& p, cudaStream_t s);
+
+}  // namespace ddm

@@ -1,0 +1,396 @@
+// Masked Wiener-Khinchin temporal analysis and the radial reduction.
+//
+// Reference semantics (motility-ddm/src/ddm_ref.js:229-288, ddm.wgsl:202-259):
+// for each Fourier mode, x(t) = hist[mode][order[t]] * mask[t], t < T, zero
+// padded to TPAD, p = |x|^2, and
+//   A(tau) + B(tau) = IFFT(2 Re(conj(M) P)),   G(tau) = IFFT(|Y|^2),
+//   D(tau) = (A + B - 2 Re G) / N(tau),  C(tau) = G / N(tau),  P = sum p / N(0)
+// with M = FFT(mask) and N(tau) the exact valid-pair counts (host, FP64).
+//
+// B200 formulation: one CTA of TPAD/8 threads processes modes in pairs (a, b)
+// with five register-resident FFTs per pair instead of the reference's four
+// per mode:
+//   Z  = FFT(p_a + i p_b)                 -> P_a, P_b by Hermitian split
+//   Y  = FFT(x_a);  W_a = IFFT(|Y|^2 + i 2 Re(conj(M) P_a))
+//   Y  = FFT(x_b);  W_b = IFFT(|Y|^2 + i 2 Re(conj(M) P_b))
+// |Y|^2 and 2 Re(conj(M) P) are both real, so W = n (G + i E) splits into
+//   G(tau) = (W(tau) + conj W(-tau)) / 2n,  E(tau) = Im(W(tau) - conj W(-tau)) / 2n
+// where E = A + B. That is 2.5 transforms per mode instead of 4.
+//
+// Two epilogues:
+//  * fused radial (default): modes are visited in bin order in "units" (a run
+//    of modes of one bin); each thread owns lags and accumulates the bin's D
+//    and the eight phase-drift sums of (tau, tau+1) (ddm_ref.js:360-382) in
+//    FP64 registers, writing one partial record per unit. reduce_kernel sums
+//    the units of each bin in a fixed order (deterministic) and divides by the
+//    bin's mode count (ddm_ref.js:404-412).
+//  * full outputs: per-mode D[mode][tau], C[mode][tau], P[mode] as the
+//    reference's GPU pass writes them (ddm.wgsl:243-258); radial_full_kernel
+//    then reduces them like the reference's `radial` pass (ddm.wgsl:265-322)
+//    but with FP64 sums.
+// Work is handed out through an atomic unit counter (no waiting on other
+// CTAs), so a persistent grid of one wave load-balances uneven bins.
+#include <cstdint>
+
+#include "fft_block.cuh"
+#include "kernels.cuh"
+
+namespace ddm {
+
+__device__ __forceinline__ int4 load_item(const int4* items, int i) {
+  return items ? items[i] : make_int4(i, 0, 0, 0);
+}
+
+template <int NP>
+struct TemporalCommon {
+  static constexpr int NT = NP / 8;
+  static constexpr int PN = padded(NP);
+};
+
+// Gathers x(t) = hist[mode][order[t]] * mask[t] into the FFT input pattern
+// (order and mask are read through L1; every CTA reads the same T entries).
+template <int NP>
+__device__ __forceinline__ void gather(float2 (&x)[8], const float2* __restrict__ h,
+                                       const uint32_t* __restrict__ order,
+                                       const float* __restrict__ mask, int t, int T, bool valid) {
+  constexpr int NT = NP / 8;
+#pragma unroll
+  for (int q = 0; q < 8; q++) {
+    const int i = t + q * NT;
+    float2 v = make_float2(0.f, 0.f);
+    if (valid && i < T) {
+      const float m = __ldg(&mask[i]);
+      if (m != 0.f) {
+        v = __ldg(&h[__ldg(&order[i])]);
+        v.x *= m;
+        v.y *= m;
+      }
+    }
+    x[q] = v;
+  }
+}
+
+// Spectrum V(k) = |Y(k)|^2 + i 2 Re(conj(M_k) P(k)) of one mode (P from the
+// packed Z buffer; `second` selects the imaginary half of the pack), left in
+// registers in the FFT input pattern.
+template <int NP>
+__device__ __forceinline__ void spectrum_v(float2 (&v)[8], int t, const float2* __restrict__ Y,
+                                           const float2* __restrict__ Z,
+                                           const float2* __restrict__ mspec, bool second) {
+  constexpr int NT = NP / 8;
+#pragma unroll
+  for (int q = 0; q < 8; q++) {
+    const int k = t + q * NT;
+    const float2 y = Y[pad(k)];
+    const float2 zk = Z[pad(k)];
+    const float2 zn = Z[pad((NP - k) & (NP - 1))];
+    const float2 M = __ldg(&mspec[k]);
+    const float Px = second ? 0.5f * (zk.y + zn.y) : 0.5f * (zk.x + zn.x);
+    const float Py = second ? -0.5f * (zk.x - zn.x) : 0.5f * (zk.y - zn.y);
+    const float S = fmaf(y.x, y.x, y.y * y.y);
+    const float R = 2.f * fmaf(M.x, Px, M.y * Py);
+    v[q] = make_float2(S, R);
+  }
+}
+
+// Occupancy hint: cap registers at 128 per thread (2+ CTAs of 256 threads).
+template <int NP>
+struct TemporalBounds {
+  static constexpr int NT = NP / 8;
+  static constexpr int MIN_BLOCKS = NT >= 512 ? 1 : 512 / NT;
+};
+
+template <int NP, int LPT, bool FULL>
+__global__ void __launch_bounds__(NP / 8, TemporalBounds<NP>::MIN_BLOCKS)
+    temporal_kernel(TemporalParams p) {
+  constexpr int NT = NP / 8;
+  constexpr int PN = padded(NP);
+  constexpr bool ODD = fft_stages(NP) & 1;
+  extern __shared__ float2 sm[];
+  float2* bufZ = sm;
+  float2* bufA = sm + PN;
+  float2* bufB = sm + 2 * PN;
+  __shared__ int s_unit;
+  const int t = threadIdx.x;
+  const int T = p.T, L = p.L;
+  const float np0 = p.npairs[0];
+  const float invn = 0.5f / NP;
+
+  for (;;) {
+    if (t == 0) s_unit = atomicAdd(p.unit_counter, 1);
+    __syncthreads();
+    const int u = s_unit;
+    if (u >= p.nunits) break;
+    const int4 U = p.units[u];
+    double acc[LPT][PFIELDS];
+#pragma unroll
+    for (int r = 0; r < LPT; r++)
+#pragma unroll
+      for (int c = 0; c < PFIELDS; c++) acc[r][c] = 0.0;
+    double accP = 0.0;
+
+    for (int k = 0; k < U.y; k += 2) {
+      const bool hasb = k + 1 < U.y;
+      const int4 ea = load_item(p.items, U.x + k);
+      const int4 eb = hasb ? load_item(p.items, U.x + k + 1) : ea;
+      const float2* ha = p.hist + (size_t)ea.x * T;
+      const float2* hb = p.hist + (size_t)eb.x * T;
+      float2 v[8];
+      {
+        float2 w[8];
+        gather<NP>(v, ha, p.order, p.mask, t, T, true);
+        gather<NP>(w, hb, p.order, p.mask, t, T, hasb);
+#pragma unroll
+        for (int q = 0; q < 8; q++)
+          v[q] = make_float2(fmaf(v[q].x, v[q].x, v[q].y * v[q].y), fmaf(w[q].x, w[q].x, w[q].y * w[q].y));
+      }
+      if (ODD)
+        fft<NP, false>(v, t, bufZ, bufA, p.tw);
+      else
+        fft<NP, false>(v, t, bufA, bufZ, p.tw);
+      const float2 zsum = bufZ[0];  // (sum p_a, sum p_b)
+
+#pragma unroll 1
+      for (int s = 0; s < 2; s++) {
+        if (s == 1 && !hasb) break;
+        const int4 e = s ? eb : ea;
+        gather<NP>(v, s ? hb : ha, p.order, p.mask, t, T, true);
+        const float2* Y = fft<NP, false>(v, t, bufA, bufB, p.tw);
+        spectrum_v<NP>(v, t, Y, bufZ, p.mspec, s == 1);
+        __syncthreads();
+        const float2* W = fft<NP, true>(v, t, bufA, bufB, p.tw);
+        const float ps = s ? zsum.y : zsum.x;
+        const float P = np0 > 0.5f ? ps / np0 : 0.f;
+        if (FULL) {
+          const size_t mode = (size_t)e.x;
+          for (int tau = t; tau < L; tau += NT) {
+            const float np = __ldg(&p.npairs[tau]);
+            const float inv = np > 0.5f ? 1.f / np : 0.f;
+            const float2 w0 = W[pad(tau)];
+            const float2 w1 = W[pad((NP - tau) & (NP - 1))];
+            const float gx = (w0.x + w1.x) * invn, gy = (w0.y - w1.y) * invn;
+            const float ee = (w0.y + w1.y) * invn;
+            p.outD[mode * L + tau] = (ee - 2.f * gx) * inv;
+            p.outC[mode * L + tau] = make_float2(gx * inv, gy * inv);
+          }
+          if (t == 0) p.outP[mode] = P;
+        } else {
+          // D and the drift sums of the lag pair (tau, tau+1) at owned lags
+          const double kx = e.y, ky = e.z;
+#pragma unroll
+          for (int r = 0; r < LPT; r++) {
+            const int tau = t + r * NT;
+            if (tau < L) {
+              const float n0 = __ldg(&p.npairs[tau]);
+              const float inp = n0 > 0.5f ? 1.f / n0 : 0.f;
+              const float2 w0 = W[pad(tau)];
+              const float2 w1 = W[pad((NP - tau) & (NP - 1))];
+              const float gx = (w0.x + w1.x) * invn, gy = (w0.y - w1.y) * invn;
+              const float ee = (w0.y + w1.y) * invn;
+              acc[r][0] += (double)((ee - 2.f * gx) * inp);
+              if (tau + 1 < L) {
+                const float n1 = __ldg(&p.npairs[tau + 1]);
+                const float inp1 = n1 > 0.5f ? 1.f / n1 : 0.f;
+                const float2 u0 = W[pad(tau + 1)];
+                const float2 u1 = W[pad((NP - tau - 1) & (NP - 1))];
+                const float cx = gx * inp, cy = gy * inp;
+                const float c1x = (u0.x + u1.x) * invn * inp1;
+                const float c1y = (u0.y - u1.y) * invn * inp1;
+                const float zr = fmaf(c1x, cx, c1y * cy);  // C(tau+1) conj C(tau)
+                const float zi = fmaf(c1y, cx, -c1x * cy);
+                const float w = sqrtf(fmaf(zr, zr, zi * zi));
+                if (w > 0.f) {
+                  const double wd = w, ph = atan2f(zi, zr);
+                  acc[r][1] += wd;
+                  acc[r][2] += wd * kx * kx;
+                  acc[r][3] += wd * kx * ky;
+                  acc[r][4] += wd * ky * ky;
+                  acc[r][5] += wd * kx * ph;
+                  acc[r][6] += wd * ky * ph;
+                  acc[r][7] += wd * ph * ph;
+                  acc[r][8] += 1.0;
+                }
+              }
+            }
+          }
+          accP += (double)P;
+        }
+        __syncthreads();
+      }
+    }
+    if (!FULL) {
+      // one partial record per unit: [u][field][tau], P after all records
+#pragma unroll
+      for (int r = 0; r < LPT; r++) {
+        const int tau = t + r * NT;
+        if (tau < L)
+#pragma unroll
+          for (int c = 0; c < PFIELDS; c++) p.partials[((size_t)u * PFIELDS + c) * L + tau] = acc[r][c];
+      }
+      if (t == 0) p.partials[(size_t)p.nunits * PFIELDS * L + u] = accP;
+    }
+    __syncthreads();
+  }
+}
+
+// Sums the unit partials of each bin in unit order (deterministic), divides
+// D and P by the bin's mode count (ddm_ref.js:404-412) and writes the
+// reference's Radial layout: D[b*L+tau], P[b], drift[(b*L+tau)*8+c].
+__global__ void reduce_kernel(ReduceParams p) {
+  const int b = blockIdx.x;
+  const int L = p.L;
+  const int u0 = p.bin_units[b], u1 = p.bin_units[b + 1];
+  const double n = (double)p.nmodes[b];
+  const double inv = n > 0 ? 1.0 / n : 0.0;
+  for (int tau = threadIdx.x; tau < L; tau += blockDim.x) {
+    double s[PFIELDS];
+#pragma unroll
+    for (int c = 0; c < PFIELDS; c++) s[c] = 0.0;
+    for (int u = u0; u < u1; u++)
+#pragma unroll
+      for (int c = 0; c < PFIELDS; c++) s[c] += p.partials[((size_t)u * PFIELDS + c) * L + tau];
+    p.D[(size_t)b * L + tau] = s[0] * inv;
+#pragma unroll
+    for (int c = 0; c < DRIFT; c++) p.drift[((size_t)b * L + tau) * DRIFT + c] = s[c + 1];
+  }
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int u = u0; u < u1; u++) s += p.partials[(size_t)p.nunits * PFIELDS * L + u];
+    p.P[b] = s * inv;
+  }
+}
+
+// Radial reduction of full per-mode outputs, one CTA per bin, one thread per
+// lag, modes of the bin in table order (ddm.wgsl:265-322 with FP64 sums).
+__global__ void radial_full_kernel(RadialFullParams p) {
+  const int b = blockIdx.x;
+  const int L = p.L;
+  const uint32_t i0 = p.offsets[b], i1 = p.offsets[b + 1];
+  const double n = (double)(i1 - i0);
+  const double inv = i1 > i0 ? 1.0 / n : 0.0;
+  for (int tau = threadIdx.x; tau < L; tau += blockDim.x) {
+    double s[PFIELDS];
+#pragma unroll
+    for (int c = 0; c < PFIELDS; c++) s[c] = 0.0;
+    for (uint32_t i = i0; i < i1; i++) {
+      const int4 e = p.items[i];
+      const size_t m = (size_t)e.x;
+      s[0] += (double)p.D[m * L + tau];
+      if (tau + 1 < L) {
+        const float2 a = p.C[m * L + tau], c1 = p.C[m * L + tau + 1];
+        const float zr = fmaf(c1.x, a.x, c1.y * a.y);
+        const float zi = fmaf(c1.y, a.x, -c1.x * a.y);
+        const float w = sqrtf(fmaf(zr, zr, zi * zi));
+        if (w > 0.f) {
+          const double wd = w, ph = atan2f(zi, zr), kx = e.y, ky = e.z;
+          s[1] += wd;
+          s[2] += wd * kx * kx;
+          s[3] += wd * kx * ky;
+          s[4] += wd * ky * ky;
+          s[5] += wd * kx * ph;
+          s[6] += wd * ky * ph;
+          s[7] += wd * ph * ph;
+          s[8] += 1.0;
+        }
+      }
+    }
+    p.oD[(size_t)b * L + tau] = s[0] * inv;
+#pragma unroll
+    for (int c = 0; c < DRIFT; c++) p.odrift[((size_t)b * L + tau) * DRIFT + c] = s[c + 1];
+  }
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (uint32_t i = i0; i < i1; i++) s += (double)p.P[p.items[i].x];
+    p.oP[b] = s * inv;
+  }
+}
+
+// ------------------------------------------------------------------ launchers
+
+template <int NP>
+static size_t temporal_smem() { return 3 * sizeof(float2) * padded(NP); }
+
+static int lpt_of(int TPAD, int L) {
+  const int NT = TPAD / 8;
+  const int r = (L + NT - 1) / NT;
+  return r <= 1 ? 1 : r <= 2 ? 2 : 4;
+}
+
+template <int NP, int LPT, bool FULL>
+static cudaError_t launch_k(const TemporalParams& p, int grid, cudaStream_t s) {
+  auto k = temporal_kernel<NP, LPT, FULL>;
+  const size_t sm = temporal_smem<NP>();
+  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  k<<<grid, NP / 8, sm, s>>>(p);
+  return cudaGetLastError();
+}
+
+template <typename K>
+static int occupancy_grid(K k, int threads, size_t smem) {
+  int dev = 0, sms = 0, per = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, threads, smem);
+  return sms * (per > 0 ? per : 1);
+}
+
+template <int NP>
+static cudaError_t dispatch_np(int L, bool full, const TemporalParams* p, int grid, cudaStream_t s,
+                               int* grid_out) {
+  const size_t sm = temporal_smem<NP>();
+  if (full) {
+    if (grid_out) *grid_out = occupancy_grid(temporal_kernel<NP, 1, true>, NP / 8, sm);
+    return p ? launch_k<NP, 1, true>(*p, grid, s) : cudaSuccess;
+  }
+  switch (lpt_of(NP, L)) {
+    case 1:
+      if (grid_out) *grid_out = occupancy_grid(temporal_kernel<NP, 1, false>, NP / 8, sm);
+      return p ? launch_k<NP, 1, false>(*p, grid, s) : cudaSuccess;
+    case 2:
+      if (grid_out) *grid_out = occupancy_grid(temporal_kernel<NP, 2, false>, NP / 8, sm);
+      return p ? launch_k<NP, 2, false>(*p, grid, s) : cudaSuccess;
+    default:
+      if (grid_out) *grid_out = occupancy_grid(temporal_kernel<NP, 4, false>, NP / 8, sm);
+      return p ? launch_k<NP, 4, false>(*p, grid, s) : cudaSuccess;
+  }
+}
+
+static cudaError_t dispatch(int TPAD, int L, bool full, const TemporalParams* p, int grid,
+                            cudaStream_t s, int* grid_out) {
+  switch (TPAD) {
+    case 128: return dispatch_np<128>(L, full, p, grid, s, grid_out);
+    case 256: return dispatch_np<256>(L, full, p, grid, s, grid_out);
+    case 512: return dispatch_np<512>(L, full, p, grid, s, grid_out);
+    case 1024: return dispatch_np<1024>(L, full, p, grid, s, grid_out);
+    case 2048: return dispatch_np<2048>(L, full, p, grid, s, grid_out);
+    case 4096: return dispatch_np<4096>(L, full, p, grid, s, grid_out);
+    case 8192: return dispatch_np<8192>(L, full, p, grid, s, grid_out);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t launch_temporal(int TPAD, int L, bool full, const TemporalParams& p, int grid,
+                            cudaStream_t s) {
+  return dispatch(TPAD, L, full, &p, grid, s, nullptr);
+}
+
+int temporal_max_grid(int TPAD, int L, bool full) {
+  int g = 0;
+  dispatch(TPAD, L, full, nullptr, 0, nullptr, &g);
+  return g;
+}
+
+cudaError_t launch_reduce(const ReduceParams& p, cudaStream_t s) {
+  const int threads = p.L >= 256 ? 256 : ((p.L + 31) / 32) * 32;
+  reduce_kernel<<<p.NB, threads, 0, s>>>(p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_radial_full(const RadialFullParams& p, cudaStream_t s) {
+  const int threads = p.L >= 256 ? 256 : ((p.L + 31) / 32) * 32;
+  radial_full_kernel<<<p.NB, threads, 0, s>>>(p);
+  return cudaGetLastError();
+}
+
+}  // namespace ddm

@@ -1,0 +1,267 @@
+"""DdmEngine: the reference's engine API (motility-ddm/src/ddm-engine.ts:62-426)
+over the C ABI of the sm_100a library.
+
+Same calls and data layouts as the TypeScript class, in Python naming:
+
+    reference (TS)                         here
+    DdmEngine.create(opts)                 DdmEngine.create(N=..., T=..., ...)
+    ingestLuma(luma, slot) -> boolean      ingest_luma(luma, slot) -> bool
+    ingestFrame(VideoFrame, slot)          ingest_frames(frames, slots, scale)
+                                           (raw u8/u16/f32 pixels; the graphics
+                                           import path has no equivalent here)
+    computeTemporal(order, mask)           compute_temporal(order, mask, full=False)
+    readRadial() -> Radial                 read_radial() -> Radial
+    readHistory()                          read_history()
+    readTemporalFull() -> {D, C, P}        read_temporal_full()
+    readMean()                             read_mean()
+    idle(), destroy()                      idle(), destroy()
+    saturated, pendingSubmits, throttled   saturated, pending_submits, throttled
+    waitForCapacity()                      wait_for_capacity()
+    bins                                   bins
+
+Errors raise DdmError (the reference throws Error); argument errors are also
+ValueError.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from .radial import Radial
+
+MAX_PENDING = 2  # ddm-engine.ts:46
+
+
+class DdmError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(msg)
+        self.code = code
+
+
+class DdmArgError(DdmError, ValueError):
+    pass
+
+
+def _ptr(a):
+    return C.c_void_p(a.ctypes.data) if a is not None else None
+
+
+class DdmEngine:
+    """One DDM analysis engine on the current CUDA device."""
+
+    def __init__(self, handle, geometry):
+        self._h = handle
+        self._lib = _lib.load()
+        self.geometry = geometry
+        self.N, self.T, self.TPAD, self.L = geometry.N, geometry.T, geometry.TPAD, geometry.L
+        self.NB = geometry.NB
+        self.NH = self.N // 2 + 1
+        self.modes = self.N * self.NH
+        self.bins = self._read_bins()
+        self._destroyed = False
+
+    # ------------------------------------------------------------ lifetime
+    @classmethod
+    def create(cls, N=256, T=256, TPAD=0, L=128, NB=32, kmin=4.0, kmax=100.0, knodes=4):
+        """DdmEngine.create (ddm-engine.ts:125-149). Defaults are the
+        reference's frozen geometry (ddm_ref.js:18-31)."""
+        lib = _lib.load()
+        g = _lib.Geometry(N, T, TPAD, L, NB, float(kmin), float(kmax), knodes, 0)
+        h = C.c_void_p()
+        rc = lib.ddm_create(C.byref(g), C.byref(h))
+        if rc != _lib.DDM_OK:
+            msg = lib.ddm_create_error().decode()
+            raise (DdmArgError if rc == _lib.DDM_ERR_ARG else DdmError)(rc, msg)
+        out = _lib.Geometry()
+        lib.ddm_get_geometry(h, C.byref(out))
+        return cls(h, out)
+
+    def destroy(self):
+        """DdmEngine.destroy (ddm-engine.ts:421-425)."""
+        if not self._destroyed:
+            self._destroyed = True
+            self._lib.ddm_destroy(self._h)
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.destroy()
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+    def _check(self, rc):
+        if rc != _lib.DDM_OK:
+            msg = self._lib.ddm_last_error(self._h).decode()
+            raise (DdmArgError if rc == _lib.DDM_ERR_ARG else DdmError)(rc, msg)
+
+    def _alive(self):
+        if self._destroyed:
+            raise DdmError(_lib.DDM_ERR_STATE, "engine destroyed")
+
+    def _read_bins(self):
+        n = self._lib.ddm_bins_count(self._h)
+        NB, K = self.geometry.NB, self.geometry.knodes
+        off = np.empty(NB + 1, np.uint32)
+        modes = np.empty((max(n, 1), 4), np.int32)
+        kc = np.empty(NB)
+        nm = np.empty(NB, np.uint32)
+        kn = np.empty(NB * K)
+        self._check(self._lib.ddm_get_bins(self._h, _ptr(off), _ptr(modes), _ptr(kc), _ptr(nm), _ptr(kn)))
+        return dict(N=self.N, NB=NB, kmin=self.geometry.kmin, kmax=self.geometry.kmax, knodes=K,
+                    binOffsets=off, binModes=modes[:n], kCenter=kc, nModes=nm, kNodes=kn)
+
+    # ------------------------------------------------------------ ingest
+    @property
+    def pending_submits(self):
+        return self._lib.ddm_pending(self._h)
+
+    @property
+    def saturated(self):
+        return self.pending_submits > MAX_PENDING
+
+    @property
+    def throttled(self):
+        return self._lib.ddm_throttled(self._h)
+
+    def wait_for_capacity(self):
+        self._check(self._lib.ddm_wait_for_capacity(self._h))
+
+    def ingest_luma(self, luma, slot):
+        """ingestLuma (ddm-engine.ts:308-324): N*N float luma, row-major.
+        Returns False if the frame was dropped because the queue is saturated."""
+        self._alive()
+        a = np.ascontiguousarray(luma, dtype=np.float32).reshape(-1)
+        if a.size != self.N * self.N:
+            raise DdmArgError(_lib.DDM_ERR_ARG, f"ingestLuma expects {self.N * self.N} values")
+        ok = C.c_int32(0)
+        self._check(self._lib.ddm_ingest_luma(self._h, _ptr(a), int(slot), C.byref(ok)))
+        return bool(ok.value)
+
+    def ingest_frames(self, frames, slots, scale=None):
+        """Raw frames [n, N, N] (numpy, or torch CPU/CUDA tensor) into ring slots
+        `slots[i] % T`. luma = value * scale; scale defaults to 1/255 for u8
+        (lumaOf, test/sim.mjs:189-193), 1/65535 for u16 and 1 for f32."""
+        self._alive()
+        slots = np.ascontiguousarray(slots, dtype=np.int32).reshape(-1)
+        dev_ptr = None
+        try:
+            import torch
+            if isinstance(frames, torch.Tensor):
+                if not frames.is_contiguous():
+                    frames = frames.contiguous()
+                dt = {torch.uint8: "u8", torch.int16: "u16", torch.uint16: "u16",
+                      torch.float32: "f32"}.get(frames.dtype)
+                if dt is None:
+                    raise DdmArgError(_lib.DDM_ERR_ARG, f"unsupported frame dtype {frames.dtype}")
+                n = frames.shape[0] if frames.dim() == 3 else 1
+                if frames.numel() != n * self.N * self.N:
+                    raise DdmArgError(_lib.DDM_ERR_ARG, f"frames must be [n, {self.N}, {self.N}]")
+                if frames.is_cuda:
+                    dev_ptr = frames.data_ptr()
+                else:
+                    host_ptr = frames.data_ptr()
+                keep = frames
+        except ImportError:
+            pass
+        if dev_ptr is None and "keep" not in locals():
+            arr = np.ascontiguousarray(frames)
+            dt = {np.dtype(np.uint8): "u8", np.dtype(np.uint16): "u16",
+                  np.dtype(np.float32): "f32"}.get(arr.dtype)
+            if dt is None:
+                raise DdmArgError(_lib.DDM_ERR_ARG, f"unsupported frame dtype {arr.dtype}")
+            n = arr.shape[0] if arr.ndim == 3 else 1
+            if arr.size != n * self.N * self.N:
+                raise DdmArgError(_lib.DDM_ERR_ARG, f"frames must be [n, {self.N}, {self.N}]")
+            host_ptr = arr.ctypes.data
+            keep = arr
+        if slots.size != n:
+            raise DdmArgError(_lib.DDM_ERR_ARG, f"{n} frames but {slots.size} slots")
+        if scale is None:
+            scale = {"u8": 1 / 255, "u16": 1 / 65535, "f32": 1.0}[dt]
+        code = _lib.DTYPES[dt]
+        if dev_ptr is not None:
+            rc = self._lib.ddm_ingest_frames_device(self._h, C.c_void_p(dev_ptr), code, n, _ptr(slots),
+                                                    float(scale))
+        else:
+            rc = self._lib.ddm_ingest_frames(self._h, C.c_void_p(host_ptr), code, n, _ptr(slots),
+                                             float(scale))
+        del keep
+        self._check(rc)
+
+    def set_spatial_mask(self, mask):
+        """Extension: N x N ROI mask (nonzero = used), or None."""
+        self._alive()
+        if mask is None:
+            self._check(self._lib.ddm_set_spatial_mask(self._h, None))
+            return
+        m = np.ascontiguousarray(mask, dtype=np.uint8).reshape(-1)
+        if m.size != self.N * self.N:
+            raise DdmArgError(_lib.DDM_ERR_ARG, f"mask must have {self.N * self.N} values")
+        self._check(self._lib.ddm_set_spatial_mask(self._h, _ptr(m)))
+
+    # ------------------------------------------------------------ analysis
+    def compute_temporal(self, order, mask, full=False, wait=True):
+        """computeTemporal (ddm-engine.ts:331-365). order[j] = slot of time
+        index j, mask[j] = 1 where time index j holds a valid frame."""
+        self._alive()
+        o = np.ascontiguousarray(order, dtype=np.uint32).reshape(-1)
+        m = np.ascontiguousarray(mask, dtype=np.float32).reshape(-1)
+        if o.size != self.T or m.size != self.T:
+            raise DdmArgError(_lib.DDM_ERR_ARG, f"temporalMeta: order/mask must have length {self.T}")
+        f = self._lib.ddm_compute_temporal if wait else self._lib.ddm_compute_temporal_async
+        self._check(f(self._h, _ptr(o), _ptr(m), 1 if full else 0))
+
+    def read_radial(self):
+        """readRadial (ddm-engine.ts:391-395) -> Radial (ddm_ref.js:336-348)."""
+        self._alive()
+        NB, L = self.NB, self.L
+        D = np.empty(NB * L)
+        P = np.empty(NB)
+        drift = np.empty(NB * L * 8)
+        self._check(self._lib.ddm_read_radial(self._h, _ptr(D), _ptr(P), _ptr(drift)))
+        b = self.bins
+        return Radial(N=self.N, NB=NB, L=L, kCenter=b["kCenter"].copy(), kNodes=b["kNodes"].copy(),
+                      nModes=b["nModes"].copy(), D=D, P=P, drift=drift, knodes=b["knodes"])
+
+    def read_history(self):
+        """readHistory (ddm-engine.ts:398-400): complex64 [modes, T]."""
+        self._alive()
+        out = np.empty((self.modes, self.T), np.complex64)
+        self._check(self._lib.ddm_read_history(self._h, _ptr(out)))
+        return out
+
+    def read_temporal_full(self):
+        """readTemporalFull (ddm-engine.ts:403-408): D [modes, L] f32,
+        C [modes, L] complex64, P [modes] f32."""
+        self._alive()
+        D = np.empty((self.modes, self.L), np.float32)
+        Cm = np.empty((self.modes, self.L), np.complex64)
+        P = np.empty(self.modes, np.float32)
+        self._check(self._lib.ddm_read_temporal_full(self._h, _ptr(D), _ptr(Cm), _ptr(P)))
+        return dict(D=D, C=Cm, P=P)
+
+    def read_mean(self):
+        """readMean (ddm-engine.ts:411-414)."""
+        self._alive()
+        v = C.c_double()
+        self._check(self._lib.ddm_read_mean(self._h, C.byref(v)))
+        return v.value
+
+    def idle(self):
+        """idle (ddm-engine.ts:417-419)."""
+        self._check(self._lib.ddm_idle(self._h))
+
+    # ------------------------------------------------------------ plumbing
+    def set_stream(self, stream_ptr):
+        """Queue the engine's work on a caller's CUDA stream (int handle) or
+        back on its own stream (None)."""
+        self._check(self._lib.ddm_set_stream(self._h, C.c_void_p(stream_ptr) if stream_ptr else None))
+
+    @property
+    def kernel_launches(self):
+        return self._lib.ddm_kernel_launches(self._h)

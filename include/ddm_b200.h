@@ -1,0 +1,149 @@
+/*
+ * ddm_b200 — C ABI of the B200 (sm_100a) DDM analysis library.
+ *
+ * Drop-in for the operator surface of motility-ddm's WebGPU engine
+ * (class DdmEngine, motility-ddm/src/ddm-engine.ts:62-426): the same calls,
+ * argument meanings, data layouts and error behaviour, behind plain C types so
+ * an N-API addon (Node), ctypes (Python) or any FFI can bind it. Each entry
+ * point names the reference member it replaces.
+ *
+ * Layouts (identical to the reference):
+ *   history   hist[(mode*T + slot)*2 + {re,im}], mode = ky*(N/2+1) + kx
+ *             (ddm_ref.js:175-206)
+ *   full      D[mode*L + tau], C[(mode*L + tau)*2 + {re,im}], P[mode]
+ *             (ddm-engine.ts:403-408)
+ *   radial    D[b*L + tau], P[b], drift[(b*L + tau)*8 + c] with
+ *             c = Sw, Sxx, Sxy, Syy, Rx, Ry, Rpp, count (ddm_ref.js:336-348)
+ *   bins      binOffsets[NB+1], binModes[4*i] = (mode, kx, ky, 0),
+ *             kCenter[NB], nModes[NB], kNodes[NB*knodes] (ddm_ref.js:84-170)
+ *
+ * Conventions: every call returns DDM_OK (0) or an error code; the message is
+ * available from ddm_last_error(). Input arrays are copied before a call
+ * returns (the reference's queue.writeBuffer semantics); read functions fill
+ * caller-owned arrays. One engine is single-threaded (like the reference's JS
+ * event loop); distinct engines are independent.
+ */
+#ifndef DDM_B200_H
+#define DDM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct ddm_engine ddm_engine;
+
+/* Geometry. The reference freezes N=256, T=256, TPAD=512, L=128, NB=32,
+ * KMIN=4, KMAX=100, KNODES=4 (ddm_ref.js:18-31); here they are parameters.
+ * Supported: N in {64..2048} and TPAD in {128..8192} powers of two,
+ * 2 <= L <= T <= TPAD/2. */
+typedef struct ddm_geometry {
+  int32_t N;       /* ROI side in pixels */
+  int32_t T;       /* history slots (frames) */
+  int32_t TPAD;    /* temporal FFT length; 0 = smallest power of two >= 2T */
+  int32_t L;       /* lags 0..L-1 */
+  int32_t NB;      /* radial q-bins */
+  double kmin;     /* inner edge of the first bin, FFT index units */
+  double kmax;     /* outer edge of the last bin */
+  int32_t knodes;  /* effective-|k| quadrature nodes per bin (4) */
+  int32_t reserved;
+} ddm_geometry;
+
+enum ddm_dtype { DDM_U8 = 0, DDM_U16 = 1, DDM_F32 = 2 };
+
+enum ddm_status {
+  DDM_OK = 0,
+  DDM_ERR_ARG = 1,     /* invalid argument (the reference throws) */
+  DDM_ERR_CUDA = 2,    /* CUDA runtime failure */
+  DDM_ERR_STATE = 3,   /* call not valid in the engine's state */
+  DDM_ERR_NOMEM = 4,   /* device allocation failed */
+  DDM_ERR_NODEV = 5    /* no usable sm_100 device */
+};
+
+/* DdmEngine.create (ddm-engine.ts:125-149): device buffers, bin table
+ * (makeBins, ddm_ref.js:84-170), window and twiddle tables. */
+int ddm_create(const ddm_geometry *geometry, ddm_engine **out);
+/* DdmEngine.destroy (ddm-engine.ts:421-425). NULL is ignored. */
+void ddm_destroy(ddm_engine *h);
+/* Message of the last failed call on this engine ("" if none). */
+const char *ddm_last_error(const ddm_engine *h);
+/* Message of the last failed ddm_create (no engine exists yet). */
+const char *ddm_create_error(void);
+
+/* Resolved geometry (TPAD filled in). */
+int ddm_get_geometry(const ddm_engine *h, ddm_geometry *out);
+/* DdmEngine.bins (ddm-engine.ts:69): number of binned modes, then the table. */
+int ddm_bins_count(const ddm_engine *h);
+int ddm_get_bins(const ddm_engine *h, uint32_t *binOffsets, int32_t *binModes,
+                 double *kCenter, uint32_t *nModes, double *kNodes);
+
+/* DdmEngine.ingestLuma (ddm-engine.ts:308-324): one N*N row-major luma frame
+ * (host memory) into ring slot `slot % T`. Returns DDM_OK, or sets *accepted
+ * to 0 and counts a throttled frame when more than 2 ingests are still in
+ * flight (the reference's MAX_PENDING back-pressure, ddm-engine.ts:46). */
+int ddm_ingest_luma(ddm_engine *h, const float *luma, int32_t slot,
+                    int32_t *accepted);
+
+/* Raw-frame ingest (replaces DdmEngine.ingestFrame, ddm-engine.ts:258-302,
+ * whose VideoFrame/external-texture import is a graphics path). `frames`
+ * holds n frames of N*N pixels of `dtype` in HOST memory; frame i goes to
+ * slot slots[i] % T with luma = value * scale (the reference's lumaOf uses
+ * 1/255 for 8-bit frames, test/sim.mjs:189-193). Slots within one call must
+ * be distinct. Pinned host memory is copied asynchronously, overlapped with
+ * the transforms of the previous chunk; the call returns once the frames have
+ * been copied off the caller's buffer. */
+int ddm_ingest_frames(ddm_engine *h, const void *frames, int32_t dtype,
+                      int32_t n, const int32_t *slots, float scale);
+/* Same, with `frames` already in device memory (cudaMalloc / torch). Work is
+ * queued on the engine's stream; the buffer must stay valid until it runs. */
+int ddm_ingest_frames_device(ddm_engine *h, const void *frames, int32_t dtype,
+                             int32_t n, const int32_t *slots, float scale);
+
+/* Spatial ROI mask (extension; the reference has none): N*N bytes, 1 = pixel
+ * used. Masked pixels are excluded from the frame mean and zeroed before the
+ * window. NULL restores the full frame. */
+int ddm_set_spatial_mask(ddm_engine *h, const uint8_t *mask);
+
+/* DdmEngine.computeTemporal (ddm-engine.ts:331-365): order[j] = ring slot of
+ * time index j, mask[j] = 1 if time index j holds a valid frame (length T;
+ * temporalMeta, ddm_ref.js:538-560). full = 0 computes the radial record
+ * only (binned modes, the reference's analyzeRadial, ddm_ref.js:425-437);
+ * full = 1 also keeps per-mode D, C, P for every mode (analyzeFull,
+ * ddm_ref.js:450-463). Blocks until the results are ready. */
+int ddm_compute_temporal(ddm_engine *h, const uint32_t *order,
+                         const float *mask, int32_t full);
+/* Same, without waiting: the work is queued on the engine's stream. */
+int ddm_compute_temporal_async(ddm_engine *h, const uint32_t *order,
+                               const float *mask, int32_t full);
+
+/* DdmEngine.readRadial (ddm-engine.ts:391-395) + radialFromGpu
+ * (ddm_ref.js:584-590): D[NB*L], P[NB], drift[NB*L*8] in FP64. */
+int ddm_read_radial(ddm_engine *h, double *D, double *P, double *drift);
+/* DdmEngine.readHistory (ddm-engine.ts:398-400): modes*T*2 floats. */
+int ddm_read_history(ddm_engine *h, float *out);
+/* DdmEngine.readTemporalFull (ddm-engine.ts:403-408); needs a preceding
+ * ddm_compute_temporal with full = 1, else DDM_ERR_STATE. */
+int ddm_read_temporal_full(ddm_engine *h, float *D, float *C, float *P);
+/* DdmEngine.readMean (ddm-engine.ts:411-414): last ingested frame's mean
+ * luma (over the spatial mask when one is set). */
+int ddm_read_mean(ddm_engine *h, double *mean);
+/* DdmEngine.idle (ddm-engine.ts:417-419): waits for all queued work. */
+int ddm_idle(ddm_engine *h);
+
+/* Back-pressure state (ddm-engine.ts:120-124, 216-224, 107). */
+int ddm_pending(ddm_engine *h);
+int ddm_wait_for_capacity(ddm_engine *h);
+int64_t ddm_throttled(const ddm_engine *h);
+
+/* Run the engine's work on a caller's CUDA stream (cudaStream_t as void*),
+ * e.g. to time it with events on that stream. NULL restores the engine's own
+ * stream. */
+int ddm_set_stream(ddm_engine *h, void *stream);
+/* Kernels launched by this engine so far (instrumentation). */
+int64_t ddm_kernel_launches(const ddm_engine *h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DDM_B200_H */

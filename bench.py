@@ -1,0 +1,348 @@
+"""Benchmark of the DDM analysis hot path: frames/s at 512^2 x 1024 uint16.
+
+One step = one full pass of the path over one video (1024 frames of 512^2
+u16): spatial FFT of every frame into the mode-major history, masked
+Wiener-Khinchin temporal analysis of every binned mode (TPAD 2048, L = 512
+lags), radial reduction into 256 q-bins (the reference's History.ingest ->
+analyzeRadial, motility-ddm/src/ddm_ref.js:196-206, 425-437).
+
+  value  frames/s with the frames already in HBM (device-timed, CUDA events on
+         the engine's stream, max over ranks, summed over ranks)
+  e2e    the same through the C ABI from pinned HOST frames: every step copies
+         its frames host->device and reads the radial record back
+Under torchrun each rank analyses its own video (weak scaling, no collective
+on the data path).
+
+--impl reference times the reference's CPU algorithm on the host cores: the
+reference is JavaScript with no runtime on this machine, so its FP64 C
+restatement (oracle/, test infrastructure) stands in, on a bounded sample.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N, T, TPAD, L, NB, KMIN, KMAX = 512, 1024, 2048, 512, 256, 4.0, 200.0
+METRIC = "DDM frames/s at 512²×1024"
+WORKLOAD = ("512x512x1024 u16 video: 2000 blobs sigma 2 px, 30% Brownian D=0.2 px^2/frame, 70% "
+            "straight swimmers Schulz vbar=1.5 px/frame Z=4 (+D=0.2), Poisson noise mean 400 "
+            "counts, circular ROI r=230 px, 2% dropped frames; TPAD=2048, L=512 lags, 256 q-bins "
+            "(kmin 4, kmax 200)")
+# algorithmic HBM bytes per frame: u16 input + spectrum write + spectrum read
+BYTES_PER_FRAME_IN = N * N * 2
+BYTES_PER_MODE_SLOT = 8
+
+
+def _peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock and throttle-reason samples during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.index)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, ValueError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def _profile_traffic():
+    """DRAM bytes per launch of the dominant kernel from the committed ncu
+    summary (profiles/ncu_traffic.txt, 'key value' lines), or None."""
+    p = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
+    if not os.path.exists(p):
+        return None
+    out = {}
+    for ln in open(p):
+        parts = ln.split()
+        if len(parts) == 2 and not ln.startswith("#"):
+            try:
+                out[parts[0]] = float(parts[1])
+            except ValueError:
+                pass
+    return out
+
+
+def cpu_baseline(frames_u16, valid, sample_frames=24, sample_modes=6144, threads=None):
+    """Times the FP64 oracle (the reference's CPU algorithm restated in C) on
+    a bounded sample of the workload and scales it to frames/s of the whole
+    video: spatial time per frame x T + temporal time per mode x binned modes."""
+    import oracle as O
+    threads = threads or os.cpu_count()
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    fr = frames_u16[:sample_frames].astype(np.float64) * (1.0 / 65535)
+    t0 = time.perf_counter()
+    hist = O.history_ingest(fr, np.arange(sample_frames, dtype=np.int32), T)
+    t_sp = (time.perf_counter() - t0) / sample_frames
+    bins = O.make_bins(N, NB, KMIN, KMAX)
+    nbinned = int(bins["binOffsets"][-1])
+    rng = np.random.default_rng(0)
+    pick = np.sort(rng.choice(nbinned, size=min(sample_modes, nbinned), replace=False))
+    modes = bins["binModes"][pick, 0].astype(np.int32)
+    # synthetic full-length series for the sampled modes (timing only)
+    h = np.zeros((N * (N // 2 + 1), T), np.complex128)
+    h[modes] = rng.standard_normal((modes.size, T)) + 1j * rng.standard_normal((modes.size, T))
+    order, mask = O.linear_order(valid)
+    t0 = time.perf_counter()
+    O.analyze_modes(h, order, mask, L, modes, TPAD=TPAD, threads=threads)
+    t_tm = (time.perf_counter() - t0) / modes.size
+    del hist, h
+    t_frame = t_sp + t_tm * nbinned / T
+    return {"value": 1.0 / t_frame, "unit": "frames/s", "cores": threads, "kind": "port",
+            "sample": f"{sample_frames} frames of the spatial FFT + {modes.size} of {nbinned} binned "
+                      f"modes of the TPAD={TPAD} masked WK, FP64, scaled to the {T}-frame video"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    import torch
+    from hackathon_b200 import synth
+    spec = synth.config2(seed=1)
+    frames, valid, _ = synth.generate(spec, device="cuda" if torch.cuda.is_available() else "cpu")
+    fr = frames.view(torch.int16).cpu().numpy().view(np.uint16)
+    for _ in range(args.warmup):
+        cpu_baseline(fr, valid, sample_frames=8, sample_modes=1024)
+    vals = []
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        vals.append(cpu_baseline(fr, valid, sample_frames=8, sample_modes=2048))
+    wall = time.perf_counter() - t0
+    v = statistics.median(x["value"] for x in vals)
+    line = {"metric": METRIC, "value": v, "unit": "frames/s", "impl": "reference", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * wall / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": WORKLOAD},
+            "cpu_baseline": {"value": v, "unit": "frames/s", "cores": vals[0]["cores"], "kind": "port",
+                             "sample": vals[0]["sample"]},
+            "e2e": {"value": v, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "the reference path is JavaScript (motility-ddm/src/ddm_ref.js, fft.js); no JS "
+                    "runtime exists on this box, so its FP64 C restatement runs on the host cores"}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+
+    import hackathon_b200 as H
+    from hackathon_b200 import synth
+
+    torch.cuda.set_device(local)
+    spec = synth.config2(seed=1 + rank)
+    frames, valid, truth = synth.generate(spec)
+    mask_roi = synth.roi_mask(spec)
+    slots = np.arange(T, dtype=np.int32)
+    order = np.arange(T, dtype=np.uint32)
+    tmask = valid.astype(np.float32)
+    eng = H.DdmEngine.create(N=N, T=T, TPAD=TPAD, L=L, NB=NB, kmin=KMIN, kmax=KMAX)
+    eng.set_spatial_mask(mask_roi)
+    stream = torch.cuda.current_stream()
+    eng.set_stream(stream.cuda_stream)
+    scale = 1.0 / 65535
+
+    def step():
+        eng.ingest_frames(frames, slots, scale)
+        eng.compute_temporal(order, tmask, full=False, wait=False)
+
+    # stage timing events (spatial, temporal) inside the timed region
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    l0 = eng.kernel_launches
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
+           torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    torch.cuda.synchronize()
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    for i in range(args.steps):
+        ev[i][0].record(stream)
+        eng.ingest_frames(frames, slots, scale)
+        ev[i][1].record(stream)
+        eng.compute_temporal(order, tmask, full=False, wait=False)
+        ev[i][2].record(stream)
+    end.record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    launches = eng.kernel_launches - l0
+    clk = clocks.stop()
+    ms = start.elapsed_time(end)
+    t_sp = statistics.mean(a.elapsed_time(b) for a, b, _ in ev)
+    t_tm = statistics.mean(b.elapsed_time(c) for _, b, c in ev)
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_step = ms / args.steps
+    value = world * T / (ms_step / 1e3)
+
+    # ---------------- e2e: pinned host frames through the C ABI
+    host = frames.view(torch.int16).cpu().pin_memory()
+    rad_bytes = 8 * (NB * L + NB + NB * L * 8)
+    eng.set_stream(stream.cuda_stream)
+    for _ in range(2):
+        eng.ingest_frames(host, slots, scale)
+        eng.compute_temporal(order, tmask, full=False, wait=False)
+        eng.read_radial()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.e2e_steps):
+        eng.ingest_frames(host, slots, scale)
+        eng.compute_temporal(order, tmask, full=False, wait=False)
+        radial = eng.read_radial()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_e2e = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([ms_e2e], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_e2e = float(t.item())
+    e2e = world * T * args.e2e_steps / (ms_e2e / 1e3)
+
+    # ---------------- roofline of the dominant stage
+    peak, peak_kind = _peaks()
+    nbinned = int(eng.bins["binOffsets"][-1])
+    modes = eng.modes
+    sp_bytes = T * (BYTES_PER_FRAME_IN + modes * BYTES_PER_MODE_SLOT)  # read frames, write history
+    tm_bytes = nbinned * T * BYTES_PER_MODE_SLOT                       # read binned series
+    stages = {
+        "spatial": {"ms": t_sp, "bytes": sp_bytes, "GBps": sp_bytes / (t_sp * 1e6)},
+        "temporal": {"ms": t_tm, "bytes": tm_bytes, "GBps": tm_bytes / (t_tm * 1e6)},
+    }
+    for s in stages.values():
+        s["frac"] = s["GBps"] / peak
+    # FP32 work, 5 n log2 n per complex FFT of n points
+    fl_sp = T * (N // 2 + N // 2 + 1) * 5 * N * np.log2(N)
+    fl_tm = nbinned * 2.5 * 5 * TPAD * np.log2(TPAD)
+    stages["spatial"]["gflop"] = fl_sp / 1e9
+    stages["temporal"]["gflop"] = fl_tm / 1e9
+    dom = max(stages, key=lambda k: stages[k]["ms"])
+    traffic = _profile_traffic() or {}
+    roof = {"bound": "hbm", "kernel": dom, "achieved": stages[dom]["GBps"], "peak": peak,
+            "unit": "GB/s", "frac": stages[dom]["frac"], "peak_source": peak_kind,
+            "traffic": traffic.get(f"{dom}_bytes_per_step"),
+            "algorithmic_bytes": stages[dom]["bytes"],
+            "pipeline_GBps": (sp_bytes + tm_bytes) / (ms_step * 1e6),
+            "pipeline_frac": (sp_bytes + tm_bytes) / (ms_step * 1e6) / peak,
+            "stages": stages}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        fr = frames.view(torch.int16).cpu().numpy().view(np.uint16)
+        cpu = cpu_baseline(fr, valid)
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded GPU generator, hackathon_b200/synth.py)",
+                "config": {"workload": WORKLOAD, "N": N, "T": T, "TPAD": TPAD, "L": L, "NB": NB,
+                           "frames_dtype": "u16", "parallelism": f"replicas x{world} (one video per GPU)",
+                           "l2": "inputs larger than L2 (537 MB frames, 1.08 GB history per video)"},
+                "e2e": {"value": e2e, "unit": "frames/s", "h2d_bytes_per_step": int(host.numel() * 2),
+                        "d2h_bytes_per_step": rad_bytes},
+                "gpu_launches": int(launches),
+                "roofline": roof,
+                "clocks": clk,
+                "cpu_baseline": cpu,
+                "binned_modes": nbinned}
+        print(json.dumps(line), flush=True)
+    eng.destroy()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

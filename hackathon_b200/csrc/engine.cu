@@ -51,8 +51,6 @@ struct ddm_engine {
   uint8_t *d_smask = nullptr;
   void *d_stage[NSTAGE]{};             // device staging for host frames
   size_t stage_bytes = 0;
-  int *d_slots = nullptr;              // [NSTAGE][chunk] (device copy of slots)
-  int *h_slots = nullptr;              // pinned [NSTAGE][chunk]
   double scale_last = 1.0;
   int last_mean_index = -1;
   bool have_frames = false;
@@ -124,13 +122,12 @@ static void release(ddm_engine *h) {
   if (h->copy_stream) cudaStreamSynchronize(h->copy_stream);
   void *dev[] = {h->d_hist, h->d_rows, h->d_rowsum, h->d_means, h->d_win, h->d_wys, h->d_ninv,
                  h->d_invtot, h->d_tw_s, h->d_tw_t, h->d_wcorr4, h->d_wcorr_full, h->d_smask,
-                 h->d_stage[0], h->d_stage[1], h->d_slots, h->d_order, h->d_mask, h->d_npairs,
+                 h->d_stage[0], h->d_stage[1], h->d_order, h->d_mask, h->d_npairs,
                  h->d_mspec, h->d_items, h->d_units, h->d_bin_units, h->d_offsets, h->d_nmodes,
                  h->d_units_full, h->d_counter, h->d_partials, h->d_radD, h->d_radP,
                  h->d_radDrift, h->d_fullD, h->d_fullP, h->d_fullC};
   for (void *p : dev)
     if (p) cudaFree(p);
-  if (h->h_slots) cudaFreeHost(h->h_slots);
   if (h->h_meta) cudaFreeHost(h->h_meta);
   for (int i = 0; i < NSTAGE; i++) {
     if (h->ready_ev[i]) cudaEventDestroy(h->ready_ev[i]);
@@ -245,8 +242,8 @@ extern "C" int ddm_create(const ddm_geometry *geometry, ddm_engine **out) {
   }
   *out = nullptr;
   ddm_geometry g = *geometry;
-  if (g.TPAD == 0) {
-    g.TPAD = 1;
+  if (g.TPAD == 0) {  // smallest supported power of two >= 2T
+    g.TPAD = 128;
     while (g.TPAD < 2 * g.T) g.TPAD <<= 1;
   }
   char msg[256] = {0};
@@ -290,7 +287,8 @@ extern "C" int ddm_create(const ddm_geometry *geometry, ddm_engine **out) {
   {
     const size_t per = (size_t)h->NHB * g.N * KB * sizeof(float2);
     const size_t target = 32u << 20;  // rows scratch stays L2-resident
-    h->chunk = (int)std::max<size_t>(4, std::min<size_t>(64, target / per));
+    h->chunk = (int)std::max<size_t>(4, std::min<size_t>(MAX_CHUNK, target / per));
+    h->chunk &= ~3;  // whole column-kernel frame groups
   }
   h->bins = make_bins(g.N, g.NB, g.kmin, g.kmax, g.knodes);
   int rc = DDM_OK;
@@ -319,7 +317,6 @@ extern "C" int ddm_create(const ddm_geometry *geometry, ddm_engine **out) {
       (rc = dalloc(h, &h->d_wys, N)) || (rc = dalloc(h, &h->d_ninv, N)) ||
       (rc = dalloc(h, &h->d_invtot, 1)) || (rc = dalloc(h, &h->d_tw_s, N)) ||
       (rc = dalloc(h, &h->d_tw_t, g.TPAD)) || (rc = dalloc(h, &h->d_wcorr4, 4)) ||
-      (rc = dalloc(h, &h->d_slots, (size_t)NSTAGE * h->chunk)) ||
       (rc = dalloc(h, (char **)&h->d_stage[0], h->stage_bytes)) ||
       (rc = dalloc(h, (char **)&h->d_stage[1], h->stage_bytes)) ||
       (rc = dalloc(h, &h->d_order, g.T)) || (rc = dalloc(h, &h->d_mask, g.T)) ||
@@ -329,9 +326,7 @@ extern "C" int ddm_create(const ddm_geometry *geometry, ddm_engine **out) {
     return bail(rc);
   h->meta_bytes = sizeof(uint32_t) * g.T + sizeof(float) * g.T + sizeof(float) * g.L +
                   sizeof(float2) * g.TPAD;
-  if (cudaHostAlloc((void **)&h->h_meta, h->meta_bytes, cudaHostAllocDefault) != cudaSuccess ||
-      cudaHostAlloc((void **)&h->h_slots, sizeof(int) * NSTAGE * h->chunk, cudaHostAllocDefault) !=
-          cudaSuccess) {
+  if (cudaHostAlloc((void **)&h->h_meta, h->meta_bytes, cudaHostAllocDefault) != cudaSuccess) {
     h->err = "pinned host allocation failed";
     return bail(DDM_ERR_NOMEM);
   }
@@ -402,7 +397,7 @@ extern "C" int ddm_set_stream(ddm_engine *h, void *stream) {
 extern "C" int64_t ddm_kernel_launches(const ddm_engine *h) { return h ? h->launches : 0; }
 
 // Rows + columns for one chunk of frames already in device memory.
-static int launch_chunk(ddm_engine *h, const void *dframes, int dtype, int n, const int *d_slots,
+static int launch_chunk(ddm_engine *h, const void *dframes, int dtype, int n, const int32_t *slots,
                         float scale) {
   const int N = h->g.N;
   // w(y) * scale for this call's scale
@@ -426,7 +421,7 @@ static int launch_chunk(ddm_engine *h, const void *dframes, int dtype, int n, co
   cp.wys = h->d_wys;
   cp.wcorr = h->d_smask ? h->d_wcorr_full : h->d_wcorr4;
   cp.wcorr_full = h->d_smask ? 1 : 0;
-  cp.slots = d_slots;
+  for (int i = 0; i < n; i++) cp.slots[i] = slots[i] % h->g.T;
   cp.tw = h->d_tw_s;
   cp.hist = h->d_hist;
   cp.means = h->d_means;
@@ -485,25 +480,21 @@ static int ingest_impl(ddm_engine *h, const void *frames, int dtype, int n, cons
   const size_t fbytes = (size_t)N * N * dtype_size(dtype);
   for (int c0 = 0, ci = 0; c0 < n; c0 += h->chunk, ci++) {
     const int m = std::min(h->chunk, n - c0);
-    const int s = ci % NSTAGE;
-    // slots of this chunk: pinned host -> device on the copy stream
-    CK(cudaEventSynchronize(h->free_ev[s]));
-    int *hs = h->h_slots + (size_t)s * h->chunk;
-    for (int i = 0; i < m; i++) hs[i] = slots[c0 + i] % h->g.T;
-    int *ds = h->d_slots + (size_t)s * h->chunk;
-    CK(cudaMemcpyAsync(ds, hs, sizeof(int) * m, cudaMemcpyHostToDevice, h->copy_stream));
     const void *src;
     if (device) {
       src = (const char *)frames + (size_t)c0 * fbytes;
     } else {
+      // staging buffer s is free once the chunk that last used it has run
+      const int s = ci % NSTAGE;
+      CK(cudaStreamWaitEvent(h->copy_stream, h->free_ev[s], 0));
       CK(cudaMemcpyAsync(h->d_stage[s], (const char *)frames + (size_t)c0 * fbytes, m * fbytes,
                          cudaMemcpyHostToDevice, h->copy_stream));
+      CK(cudaEventRecord(h->ready_ev[s], h->copy_stream));
+      CK(cudaStreamWaitEvent(h->stream, h->ready_ev[s], 0));
       src = h->d_stage[s];
     }
-    CK(cudaEventRecord(h->ready_ev[s], h->copy_stream));
-    CK(cudaStreamWaitEvent(h->stream, h->ready_ev[s], 0));
-    if ((rc = launch_chunk(h, src, dtype, m, ds, scale))) return rc;
-    CK(cudaEventRecord(h->free_ev[s], h->stream));
+    if ((rc = launch_chunk(h, src, dtype, m, slots + c0, scale))) return rc;
+    if (!device) CK(cudaEventRecord(h->free_ev[ci % NSTAGE], h->stream));
   }
   // the caller's host buffer is free once the copies have run
   CK(cudaStreamSynchronize(h->copy_stream));

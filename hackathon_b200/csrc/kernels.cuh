@@ -12,6 +12,7 @@ constexpr int KB = 2;       // kx columns per block of the row-spectrum scratch
 __host__ __device__ constexpr int col_frames(int N) { return N >= 2048 ? 2 : 4; }
 constexpr int DRIFT = 8;    // drift fields per (bin, lag) (ddm_ref.js:28)
 constexpr int PFIELDS = 9;  // D + 8 drift sums per lag in a partial record
+constexpr int MAX_CHUNK = 64;  // frames per spatial launch (slots travel as a kernel parameter)
 
 struct RowParams {
   const void* frames;      // [nframes][N][N] u8 / u16 / f32
@@ -34,7 +35,7 @@ struct ColParams {
   const float* wys;        // w(y) * scale
   const float2* wcorr;     // [N][NH] window spectrum per row, or [4] (separable)
   int wcorr_full;          // 1: wcorr is per row and per kx (spatial mask)
-  const int* slots;        // [nframes] ring slot of each frame
+  int slots[MAX_CHUNK];     // ring slot of each frame of the chunk
   const float2* tw;        // exp(-2 pi i j / N)
   float2* hist;            // [modes][T]
   double* means;           // [nframes] frame mean luma (out)

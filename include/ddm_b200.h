@@ -41,7 +41,7 @@ typedef struct ddm_engine ddm_engine;
 typedef struct ddm_geometry {
   int32_t N;       /* ROI side in pixels */
   int32_t T;       /* history slots (frames) */
-  int32_t TPAD;    /* temporal FFT length; 0 = smallest power of two >= 2T */
+  int32_t TPAD;    /* temporal FFT length; 0 = smallest power of two >= max(2T, 128) */
   int32_t L;       /* lags 0..L-1 */
   int32_t NB;      /* radial q-bins */
   double kmin;     /* inner edge of the first bin, FFT index units */

@@ -85,7 +85,8 @@ def test_ingest_luma_path(harness):
     rms = np.sqrt(np.mean(np.abs(ref[:, [0, 5]]) ** 2))
     assert np.abs(g[:, [0, 5]] - ref[:, [0, 5]]).max() / rms < 2e-5
     m = eng.read_mean()
-    assert abs(m - O.luma_of(fr[5]).mean()) < 1e-9
+    # exact mean of the f32 luma actually ingested
+    assert abs(m - (fr[5].astype(np.float32) / np.float32(255)).astype(np.float64).mean()) < 1e-12
     eng.destroy()
 
 
@@ -136,7 +137,9 @@ def test_radial_fused_parity(harness):
     # and the full-output path's radial agrees with the fused one
     eng.compute_temporal(order, mask, full=True)
     rf = eng.read_radial()
-    assert np.allclose(rf.D, rg.D, rtol=1e-6, atol=0)
+    for b in range(rg.NB):  # D relative to each bin's scale (D(0) ~ 0)
+        sc = np.abs(rg.D.reshape(-1, rg.L)[b]).max()
+        assert np.abs(rf.D.reshape(-1, rg.L)[b] - rg.D.reshape(-1, rg.L)[b]).max() <= 1e-6 * sc
     assert np.allclose(rf.P, rg.P, rtol=1e-6, atol=0)
     assert np.allclose(rf.drift, rg.drift, rtol=1e-4, atol=1e-6 * np.abs(rg.drift).max())
 
@@ -205,8 +208,10 @@ def test_temporal_edge_cases(case):
     eng.compute_temporal(order, mask, full=False)
     rg = eng.read_radial()
     ro = O.analyze_radial(hist, order, mask.astype(np.float64), bins, L, TPAD=eng.TPAD)
-    assert np.allclose(rg.D.reshape(-1, L), ro["D"], rtol=1e-4, atol=1e-7 * max(ro["D"].max(), 1e-30))
-    assert np.allclose(rg.P, ro["P"], rtol=1e-4, atol=1e-7 * max(ro["P"].max(), 1e-30))
+    # radial D against D's natural scale 2P (harness.ts:147), P relative
+    pscale = max(ro["P"].max(), 1e-30)
+    assert np.abs(rg.D.reshape(-1, L) - ro["D"]).max() <= 1e-4 * 2 * pscale
+    assert np.abs(rg.P - ro["P"]).max() <= 1e-5 * pscale
     eng.destroy()
 
 

@@ -218,7 +218,11 @@ def main():
     tmask = valid.astype(np.float32)
     eng = H.DdmEngine.create(N=N, T=T, TPAD=TPAD, L=L, NB=NB, kmin=KMIN, kmax=KMAX)
     eng.set_spatial_mask(mask_roi)
-    stream = torch.cuda.current_stream()
+    # a dedicated stream: the engine queues its kernels there and the CUDA
+    # events below are recorded on the same stream
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    assert stream.cuda_stream != 0
     eng.set_stream(stream.cuda_stream)
     scale = 1.0 / 65535
 

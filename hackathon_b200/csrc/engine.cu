@@ -42,7 +42,8 @@ struct ddm_engine {
   BinTable bins;
   float2 *d_hist = nullptr;            // [modes][T]
   float2 *d_rows = nullptr;            // [chunk][NHB][N][KB]
-  double *d_rowsum = nullptr;          // [chunk][N]
+  float *d_rowc = nullptr;             // [chunk][N] per-row reference levels
+  double *d_framesum = nullptr;        // [chunk] pixel sums
   double *d_means = nullptr;           // [chunk]
   float *d_win = nullptr, *d_wys = nullptr;
   double *d_ninv = nullptr, *d_invtot = nullptr;
@@ -69,6 +70,7 @@ struct ddm_engine {
   int4 *d_units_full = nullptr;
   int nunits_full = 0;
   int *d_counter = nullptr;
+  int *d_err = nullptr;                // device error word (bounded waits)
   double *d_partials = nullptr;
   double *d_radD = nullptr, *d_radP = nullptr, *d_radDrift = nullptr;
   float *d_fullD = nullptr, *d_fullP = nullptr;
@@ -120,11 +122,11 @@ static void release(ddm_engine *h) {
   cudaSetDevice(h->device);
   if (h->own_stream) cudaStreamSynchronize(h->own_stream);
   if (h->copy_stream) cudaStreamSynchronize(h->copy_stream);
-  void *dev[] = {h->d_hist, h->d_rows, h->d_rowsum, h->d_means, h->d_win, h->d_wys, h->d_ninv,
+  void *dev[] = {h->d_hist, h->d_rows, h->d_rowc, h->d_framesum, h->d_means, h->d_win, h->d_wys, h->d_ninv,
                  h->d_invtot, h->d_tw_s, h->d_tw_t, h->d_wcorr4, h->d_wcorr_full, h->d_smask,
                  h->d_stage[0], h->d_stage[1], h->d_order, h->d_mask, h->d_npairs,
                  h->d_mspec, h->d_items, h->d_units, h->d_bin_units, h->d_offsets, h->d_nmodes,
-                 h->d_units_full, h->d_counter, h->d_partials, h->d_radD, h->d_radP,
+                 h->d_units_full, h->d_counter, h->d_err, h->d_partials, h->d_radD, h->d_radP,
                  h->d_radDrift, h->d_fullD, h->d_fullP, h->d_fullC};
   for (void *p : dev)
     if (p) cudaFree(p);
@@ -144,7 +146,7 @@ static int build_units(ddm_engine *h) {
   // fused path: runs of up to U modes inside one bin, bins in order
   const int NB = h->g.NB;
   const int total = (int)h->bins.offsets[NB];
-  const int grid = std::max(1, temporal_max_grid(h->g.TPAD, h->g.L, false));
+  const int grid = std::max(1, temporal_max_grid(h->g.TPAD, h->g.T, h->g.L, false));
   int U = total / (3 * grid);
   U = std::max(16, std::min(256, U + (U & 1)));
   std::vector<int4> units;
@@ -171,9 +173,10 @@ static int build_units(ddm_engine *h) {
   if ((rc = dalloc(h, &h->d_items, items.size())) || (rc = dalloc(h, &h->d_units, units.size())) ||
       (rc = dalloc(h, &h->d_bin_units, NB + 1)) || (rc = dalloc(h, &h->d_offsets, NB + 1)) ||
       (rc = dalloc(h, &h->d_nmodes, NB)) || (rc = dalloc(h, &h->d_units_full, uf.size())) ||
-      (rc = dalloc(h, &h->d_counter, 1)) ||
+      (rc = dalloc(h, &h->d_counter, 1)) || (rc = dalloc(h, &h->d_err, 1)) ||
       (rc = dalloc(h, &h->d_partials, (size_t)h->nunits * PFIELDS * h->g.L + h->nunits)))
     return rc;
+  CK(cudaMemset(h->d_err, 0, sizeof(int)));
   CK(cudaMemcpy(h->d_items, items.data(), sizeof(int4) * items.size(), cudaMemcpyHostToDevice));
   if (!units.empty())
     CK(cudaMemcpy(h->d_units, units.data(), sizeof(int4) * units.size(), cudaMemcpyHostToDevice));
@@ -252,6 +255,8 @@ extern "C" int ddm_create(const ddm_geometry *geometry, ddm_engine **out) {
   else if (g.T < 2 || !is_pow2(g.TPAD) || g.TPAD < 128 || g.TPAD > 8192 || 2 * g.T > g.TPAD)
     snprintf(msg, sizeof msg, "T = %d, TPAD = %d: need TPAD a power of two in [128, 8192] and TPAD >= 2T",
              g.T, g.TPAD);
+  else if (g.T & 1)
+    snprintf(msg, sizeof msg, "T = %d: must be even (time series are staged in 16-byte units)", g.T);
   else if (g.L < 2 || g.L > g.T)
     snprintf(msg, sizeof msg, "L = %d: need 2 <= L <= T", g.L);
   else if (g.NB < 1 || !(g.kmax > g.kmin) || g.kmin < 0)
@@ -287,8 +292,10 @@ extern "C" int ddm_create(const ddm_geometry *geometry, ddm_engine **out) {
   {
     const size_t per = (size_t)h->NHB * g.N * KB * sizeof(float2);
     const size_t target = 32u << 20;  // rows scratch stays L2-resident
-    h->chunk = (int)std::max<size_t>(4, std::min<size_t>(MAX_CHUNK, target / per));
-    h->chunk &= ~3;  // whole column-kernel frame groups
+    const int fg = frames_per_col_cta(g.N);
+    size_t c = std::max<size_t>(1, target / per);
+    c = std::min<size_t>(MAX_CHUNK, std::max<size_t>(c, fg));
+    h->chunk = (int)(c / fg * fg);  // whole column-kernel frame groups
   }
   h->bins = make_bins(g.N, g.NB, g.kmin, g.kmax, g.knodes);
   int rc = DDM_OK;
@@ -312,7 +319,8 @@ extern "C" int ddm_create(const ddm_geometry *geometry, ddm_engine **out) {
   h->stage_bytes = (size_t)h->chunk * N * N * sizeof(float);
   if ((rc = dalloc(h, &h->d_hist, (size_t)h->modes * g.T)) ||
       (rc = dalloc(h, &h->d_rows, (size_t)h->chunk * h->NHB * N * KB)) ||
-      (rc = dalloc(h, &h->d_rowsum, (size_t)h->chunk * N)) ||
+      (rc = dalloc(h, &h->d_rowc, (size_t)h->chunk * N)) ||
+      (rc = dalloc(h, &h->d_framesum, (size_t)h->chunk)) ||
       (rc = dalloc(h, &h->d_means, (size_t)h->chunk)) || (rc = dalloc(h, &h->d_win, N)) ||
       (rc = dalloc(h, &h->d_wys, N)) || (rc = dalloc(h, &h->d_ninv, N)) ||
       (rc = dalloc(h, &h->d_invtot, 1)) || (rc = dalloc(h, &h->d_tw_s, N)) ||
@@ -407,16 +415,17 @@ static int launch_chunk(ddm_engine *h, const void *dframes, int dtype, int n, co
   rp.nframes = n;
   rp.win = h->d_win;
   rp.wys = h->d_wys;
-  rp.ninv = h->d_ninv;
   rp.smask = h->d_smask;
   rp.tw = h->d_tw_s;
   rp.rows = h->d_rows;
-  rp.rowsum = h->d_rowsum;
+  rp.rowc = h->d_rowc;
+  rp.framesum = h->d_framesum;
+  CK(cudaMemsetAsync(h->d_framesum, 0, sizeof(double) * n, h->stream));
   CKL(launch_rows(N, dtype, rp, h->stream));
   ColParams cp{};
   cp.rows = h->d_rows;
-  cp.rowsum = h->d_rowsum;
-  cp.ninv = h->d_ninv;
+  cp.rowc = h->d_rowc;
+  cp.framesum = h->d_framesum;
   cp.inv_total = h->d_invtot;
   cp.wys = h->d_wys;
   cp.wcorr = h->d_smask ? h->d_wcorr_full : h->d_wcorr4;
@@ -592,6 +601,7 @@ static int temporal_impl(ddm_engine *h, const uint32_t *order, const float *mask
   tp.mspec = h->d_mspec;
   tp.tw = h->d_tw_t;
   tp.unit_counter = h->d_counter;
+  tp.err = h->d_err;
   tp.T = T;
   tp.L = L;
   int rc;
@@ -607,7 +617,7 @@ static int temporal_impl(ddm_engine *h, const uint32_t *order, const float *mask
     tp.outD = h->d_fullD;
     tp.outC = h->d_fullC;
     tp.outP = h->d_fullP;
-    const int grid = std::min(temporal_max_grid(TPAD, L, true), h->nunits_full);
+    const int grid = std::min(temporal_max_grid(TPAD, T, L, true), h->nunits_full);
     CK(cudaMemsetAsync(h->d_counter, 0, sizeof(int), h->stream));
     CKL(launch_temporal(TPAD, L, true, tp, std::max(grid, 1), h->stream));
     RadialFullParams rp{};
@@ -628,7 +638,7 @@ static int temporal_impl(ddm_engine *h, const uint32_t *order, const float *mask
     tp.units = h->d_units;
     tp.nunits = h->nunits;
     tp.partials = h->d_partials;
-    const int grid = std::min(temporal_max_grid(TPAD, L, false), h->nunits);
+    const int grid = std::min(temporal_max_grid(TPAD, T, L, false), h->nunits);
     CK(cudaMemsetAsync(h->d_counter, 0, sizeof(int), h->stream));
     if (h->nunits > 0) CKL(launch_temporal(TPAD, L, false, tp, std::max(grid, 1), h->stream));
     ReduceParams rp{};
@@ -648,6 +658,19 @@ static int temporal_impl(ddm_engine *h, const uint32_t *order, const float *mask
   return DDM_OK;
 }
 
+// After a synchronisation: surfaces a device-side error word (a bounded wait
+// in a kernel that gave up) as an error status, and clears it.
+static int check_device_error(ddm_engine *h) {
+  int e = 0;
+  CK(cudaMemcpy(&e, h->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (e) {
+    CK(cudaMemset(h->d_err, 0, sizeof(int)));
+    h->radial_valid = h->full_valid = false;
+    return fail(h, DDM_ERR_CUDA, "temporal kernel: a staged copy did not complete in time (code %d)", e);
+  }
+  return DDM_OK;
+}
+
 extern "C" int ddm_compute_temporal_async(ddm_engine *h, const uint32_t *order, const float *mask,
                                           int32_t full) {
   if (!h) return DDM_ERR_ARG;
@@ -660,7 +683,7 @@ extern "C" int ddm_compute_temporal(ddm_engine *h, const uint32_t *order, const 
   int rc = temporal_impl(h, order, mask, full);
   if (rc) return rc;
   CK(cudaStreamSynchronize(h->stream));
-  return DDM_OK;
+  return check_device_error(h);
 }
 
 extern "C" int ddm_read_radial(ddm_engine *h, double *D, double *P, double *drift) {
@@ -673,7 +696,7 @@ extern "C" int ddm_read_radial(ddm_engine *h, double *D, double *P, double *drif
   if (drift)
     CK(cudaMemcpyAsync(drift, h->d_radDrift, sizeof(double) * NB * L * DRIFT, cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
-  return DDM_OK;
+  return check_device_error(h);
 }
 
 extern "C" int ddm_read_history(ddm_engine *h, float *out) {
@@ -695,7 +718,7 @@ extern "C" int ddm_read_temporal_full(ddm_engine *h, float *D, float *C, float *
   if (C) CK(cudaMemcpyAsync(C, h->d_fullC, sizeof(float2) * M * L, cudaMemcpyDeviceToHost, h->stream));
   if (P) CK(cudaMemcpyAsync(P, h->d_fullP, sizeof(float) * M, cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
-  return DDM_OK;
+  return check_device_error(h);
 }
 
 extern "C" int ddm_read_mean(ddm_engine *h, double *mean) {
@@ -714,5 +737,5 @@ extern "C" int ddm_idle(ddm_engine *h) {
   CK(cudaStreamSynchronize(h->copy_stream));
   CK(cudaStreamSynchronize(h->stream));
   prune_inflight(h);
-  return DDM_OK;
+  return check_device_error(h);
 }

@@ -22,10 +22,13 @@
 
 namespace ddm {
 
-// Shared-memory index with one float2 of padding every 8: keeps the radix-8
-// store patterns (stride 8, 64, 512) free of 64-bit bank conflicts.
-__device__ __forceinline__ int pad(int i) { return i + (i >> 3); }
-__host__ __device__ constexpr int padded(int n) { return n + n / 8; }
+// Shared-memory index with one float2 of padding every 16. 64-bit accesses
+// are served per half-warp (16 lanes over 16 bank pairs): this keeps the
+// stage loads and the stride-1, -64 and -512 stage stores conflict-free; the
+// stride-8 stores and reversed reads stay 2-way (checked by simulating every
+// access pattern of the 512- and 2048-point transforms).
+__device__ __forceinline__ int pad(int i) { return i + (i >> 4); }
+__host__ __device__ constexpr int padded(int n) { return n + n / 16; }
 
 __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
@@ -95,7 +98,9 @@ struct Dft<8, INV> {
 // j = t + i*n/8 (i < 8/R); butterfly j reads x[j + m*n/R] = v[i + (8/R)*m],
 // twiddles input m by exp(-+2*pi*i*m*(j%Ns)/(Ns*R)) and writes output m to
 // (j - j%Ns)*R + j%Ns + m*Ns.
-template <int n, int R, int Ns, bool INV>
+// TW_SMEM: the twiddle table is in shared memory (plain loads) rather than
+// global memory (read-only cache loads).
+template <int n, int R, int Ns, bool INV, bool TW_SMEM>
 __device__ __forceinline__ void stage(float2 (&v)[8], int t, float2* __restrict__ out,
                                       const float2* __restrict__ tw) {
   constexpr int NT = n / 8;
@@ -111,7 +116,7 @@ __device__ __forceinline__ void stage(float2 (&v)[8], int t, float2* __restrict_
       constexpr int step = n / (Ns * R);
 #pragma unroll
       for (int m = 1; m < R; m++) {
-        float2 w = __ldg(&tw[k * m * step]);
+        float2 w = TW_SMEM ? tw[k * m * step] : __ldg(&tw[k * m * step]);
         if (INV) w.y = -w.y;
         a[m] = cmul(a[m], w);
       }
@@ -137,18 +142,18 @@ __host__ __device__ constexpr int fft_stages(int n) {
   return s;
 }
 
-template <int n, int Ns, bool INV>
+template <int n, int Ns, bool INV, bool TW_SMEM>
 struct Stages {
   // Runs the stages from stride Ns on; the stage writes `a`, the next one
   // writes `b`. Ends with a __syncthreads after the last store.
   static __device__ __forceinline__ void run(float2 (&v)[8], int t, float2* a, float2* b,
                                              const float2* __restrict__ tw) {
     constexpr int R = (n / Ns) >= 8 ? 8 : (n / Ns);
-    stage<n, R, Ns, INV>(v, t, a, tw);
+    stage<n, R, Ns, INV, TW_SMEM>(v, t, a, tw);
     __syncthreads();
     if constexpr (Ns * R < n) {
       load8<n>(v, t, a);
-      Stages<n, Ns * R, INV>::run(v, t, b, a, tw);
+      Stages<n, Ns * R, INV, TW_SMEM>::run(v, t, b, a, tw);
     }
   }
 };
@@ -156,10 +161,10 @@ struct Stages {
 // Full n-point FFT of the 8 register points per thread (layout contract
 // above). Returns the buffer holding the natural-order result (read it at
 // pad(k)); the result lands in buf0 when the stage count is odd, else buf1.
-template <int n, bool INV>
+template <int n, bool INV, bool TW_SMEM = false>
 __device__ __forceinline__ float2* fft(float2 (&v)[8], int t, float2* buf0, float2* buf1,
                                        const float2* __restrict__ tw) {
-  Stages<n, 1, INV>::run(v, t, buf0, buf1, tw);
+  Stages<n, 1, INV, TW_SMEM>::run(v, t, buf0, buf1, tw);
   return (fft_stages(n) & 1) ? buf0 : buf1;
 }
 

@@ -7,9 +7,6 @@
 namespace ddm {
 
 constexpr int KB = 2;       // kx columns per block of the row-spectrum scratch
-// frames per column-kernel CTA: 4 consecutive slots of a mode fill one 32 B
-// sector; 2 at N = 2048 to fit the CTA's tiles in shared memory
-__host__ __device__ constexpr int col_frames(int N) { return N >= 2048 ? 2 : 4; }
 constexpr int DRIFT = 8;    // drift fields per (bin, lag) (ddm_ref.js:28)
 constexpr int PFIELDS = 9;  // D + 8 drift sums per lag in a partial record
 constexpr int MAX_CHUNK = 64;  // frames per spatial launch (slots travel as a kernel parameter)
@@ -20,22 +17,22 @@ struct RowParams {
   int nframes;
   const float* win;        // w(x), FP32 (from the FP64 window)
   const float* wys;        // w(y) * scale
-  const double* ninv;      // 1 / (valid pixels of row y)
   const uint8_t* smask;    // spatial mask [N][N] or nullptr (extension)
   const float2* tw;        // exp(-2 pi i j / N), j < N
   float2* rows;            // [nframes][NHB][N][KB]
-  double* rowsum;          // [nframes][N] masked row sums of the raw values
+  float* rowc;             // [nframes][N] per-row reference level c_y (raw units)
+  double* framesum;        // [nframes] masked pixel sums (zeroed before launch)
 };
 
 struct ColParams {
   const float2* rows;      // [nframes][NHB][N][KB]
-  const double* rowsum;    // [nframes][N]
-  const double* ninv;      // [N]
+  const float* rowc;       // [nframes][N]
+  const double* framesum;  // [nframes]
   const double* inv_total; // [1] 1 / (valid pixels of the frame)
   const float* wys;        // w(y) * scale
   const float2* wcorr;     // [N][NH] window spectrum per row, or [4] (separable)
   int wcorr_full;          // 1: wcorr is per row and per kx (spatial mask)
-  int slots[MAX_CHUNK];     // ring slot of each frame of the chunk
+  int slots[MAX_CHUNK];    // ring slot of each frame of the chunk
   const float2* tw;        // exp(-2 pi i j / N)
   float2* hist;            // [modes][T]
   double* means;           // [nframes] frame mean luma (out)
@@ -58,6 +55,7 @@ struct TemporalParams {
   float* outD;             // [modes][L] (full outputs) or nullptr
   float2* outC;            // [modes][L]
   float* outP;             // [modes]
+  int* err;                // error word (bounded waits that timed out)
   int T, L;
 };
 
@@ -86,9 +84,12 @@ struct RadialFullParams {
 // launchers (return cudaGetLastError())
 cudaError_t launch_rows(int N, int dtype, const RowParams& p, cudaStream_t s);
 cudaError_t launch_cols(int N, const ColParams& p, cudaStream_t s);
+// frames handled by one column-kernel CTA (one per FFT group); ingest chunks
+// are multiples of it
+int frames_per_col_cta(int N);
 cudaError_t launch_temporal(int TPAD, int L, bool full, const TemporalParams& p, int grid,
                             cudaStream_t s);
-int temporal_max_grid(int TPAD, int L, bool full);
+int temporal_max_grid(int TPAD, int T, int L, bool full);
 cudaError_t launch_reduce(const ReduceParams& p, cudaStream_t s);
 cudaError_t launch_radial_full(const RadialFullParams& p, cudaStream_t s);
 

@@ -32,6 +32,7 @@
 // CTAs), so a persistent grid of one wave load-balances uneven bins.
 #include <cstdint>
 
+#include "async_copy.cuh"
 #include "fft_block.cuh"
 #include "kernels.cuh"
 
@@ -47,27 +48,20 @@ struct TemporalCommon {
   static constexpr int PN = padded(NP);
 };
 
-// Gathers x(t) = hist[mode][order[t]] * mask[t] into the FFT input pattern
-// (order and mask are read through L1; every CTA reads the same T entries).
+// Gathers x(t) = row[order[t]] * mask[t] from the staged time series into the
+// FFT input pattern. T <= TPAD/2, so only q < 4 can hold samples; q >= 4 are
+// the zero padding and stay compile-time zeros (the first FFT stage folds
+// them away).
 template <int NP>
-__device__ __forceinline__ void gather(float2 (&x)[8], const float2* __restrict__ h,
-                                       const uint32_t* __restrict__ order,
-                                       const float* __restrict__ mask, int t, int T, bool valid) {
-  constexpr int NT = NP / 8;
+__device__ __forceinline__ void gather(float2 (&x)[8], const float2* __restrict__ row,
+                                       const uint32_t (&ord)[4], const float (&msk)[4]) {
 #pragma unroll
-  for (int q = 0; q < 8; q++) {
-    const int i = t + q * NT;
-    float2 v = make_float2(0.f, 0.f);
-    if (valid && i < T) {
-      const float m = __ldg(&mask[i]);
-      if (m != 0.f) {
-        v = __ldg(&h[__ldg(&order[i])]);
-        v.x *= m;
-        v.y *= m;
-      }
-    }
-    x[q] = v;
+  for (int q = 0; q < 4; q++) {
+    float2 v = row[ord[q]];
+    x[q] = make_float2(v.x * msk[q], v.y * msk[q]);
   }
+#pragma unroll
+  for (int q = 4; q < 8; q++) x[q] = make_float2(0.f, 0.f);
 }
 
 // Spectrum V(k) = |Y(k)|^2 + i 2 Re(conj(M_k) P(k)) of one mode (P from the
@@ -100,136 +94,209 @@ struct TemporalBounds {
   static constexpr int MIN_BLOCKS = NT >= 512 ? 1 : 512 / NT;
 };
 
+// Thread 0: stage the time series of pair k of `unit` into staging buffer b.
+__device__ __forceinline__ void issue_pair(const TemporalParams& p, int unit, int k, float2* stage,
+                                           uint64_t* bar) {
+  const int4 U = p.units[unit];
+  const bool hasb = k + 1 < U.y;
+  const int ma = load_item(p.items, U.x + k).x;
+  const uint32_t bytes = (uint32_t)p.T * sizeof(float2);
+  mbar_arrive_expect_tx(bar, hasb ? 2 * bytes : bytes);
+  bulk_g2s(stage, p.hist + (size_t)ma * p.T, bytes, bar);
+  if (hasb) {
+    const int mb = load_item(p.items, U.x + k + 1).x;
+    bulk_g2s(stage + p.T, p.hist + (size_t)mb * p.T, bytes, bar);
+  }
+}
+
 template <int NP, int LPT, bool FULL>
 __global__ void __launch_bounds__(NP / 8, TemporalBounds<NP>::MIN_BLOCKS)
     temporal_kernel(TemporalParams p) {
   constexpr int NT = NP / 8;
   constexpr int PN = padded(NP);
   constexpr bool ODD = fft_stages(NP) & 1;
-  extern __shared__ float2 sm[];
+  extern __shared__ __align__(16) float2 sm[];
   float2* bufZ = sm;
   float2* bufA = sm + PN;
   float2* bufB = sm + 2 * PN;
-  __shared__ int s_unit;
+  __shared__ __align__(8) uint64_t mbar[2];
+  __shared__ int s_next;
   const int t = threadIdx.x;
   const int T = p.T, L = p.L;
+  float2* stage = sm + 3 * PN;        // [2 buffers][2 rows][T]
+  float2* s_tw = stage + 4 * T;       // twiddles exp(-2 pi i j / NP)
+  float* s_np = (float*)(s_tw + NP);  // N(tau), tau < L
   const float np0 = p.npairs[0];
   const float invn = 0.5f / NP;
+  for (int i = t; i < NP; i += NT) s_tw[i] = p.tw[i];
+  for (int i = t; i < L; i += NT) s_np[i] = p.npairs[i];
 
-  for (;;) {
-    if (t == 0) s_unit = atomicAdd(p.unit_counter, 1);
-    __syncthreads();
-    const int u = s_unit;
-    if (u >= p.nunits) break;
+  uint32_t ord[4];
+  float msk[4];
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const int i = t + q * NT;
+    ord[q] = i < T ? __ldg(&p.order[i]) : 0u;
+    msk[q] = i < T ? __ldg(&p.mask[i]) : 0.f;
+  }
+  if (t == 0) {
+    mbar_init(&mbar[0], 1);
+    mbar_init(&mbar[1], 1);
+    fence_barrier_init();
+    s_next = atomicAdd(p.unit_counter, 1);
+  }
+  __syncthreads();
+  int u = s_next;
+  __syncthreads();
+  if (t == 0) {
+    s_next = atomicAdd(p.unit_counter, 1);
+    if (u < p.nunits) issue_pair(p, u, 0, stage, &mbar[0]);
+  }
+  __syncthreads();
+  int unext = s_next;
+  int k = 0, buf = 0;
+  uint32_t phase = 0;  // bit b: parity to wait for on mbar[b]
+  double acc[LPT][PFIELDS];
+  double accP = 0.0;
+#pragma unroll
+  for (int r = 0; r < LPT; r++)
+#pragma unroll
+    for (int c = 0; c < PFIELDS; c++) acc[r][c] = 0.0;
+
+  while (u < p.nunits) {
     const int4 U = p.units[u];
-    double acc[LPT][PFIELDS];
-#pragma unroll
-    for (int r = 0; r < LPT; r++)
-#pragma unroll
-      for (int c = 0; c < PFIELDS; c++) acc[r][c] = 0.0;
-    double accP = 0.0;
-
-    for (int k = 0; k < U.y; k += 2) {
-      const bool hasb = k + 1 < U.y;
-      const int4 ea = load_item(p.items, U.x + k);
-      const int4 eb = hasb ? load_item(p.items, U.x + k + 1) : ea;
-      const float2* ha = p.hist + (size_t)ea.x * T;
-      const float2* hb = p.hist + (size_t)eb.x * T;
-      float2 v[8];
-      {
-        float2 w[8];
-        gather<NP>(v, ha, p.order, p.mask, t, T, true);
-        gather<NP>(w, hb, p.order, p.mask, t, T, hasb);
-#pragma unroll
-        for (int q = 0; q < 8; q++)
-          v[q] = make_float2(fmaf(v[q].x, v[q].x, v[q].y * v[q].y), fmaf(w[q].x, w[q].x, w[q].y * w[q].y));
-      }
-      if (ODD)
-        fft<NP, false>(v, t, bufZ, bufA, p.tw);
+    // prefetch the next pair (this unit's, or the next unit's first) into the
+    // other staging buffer; its last readers finished before the loop-end sync
+    int nu = u, nk = k + 2;
+    if (nk >= U.y) {
+      nu = unext;
+      nk = 0;
+    }
+    const bool prefetched = nu < p.nunits;
+    if (t == 0 && prefetched) issue_pair(p, nu, nk, stage + (buf ^ 1) * 2 * T, &mbar[buf ^ 1]);
+    if (!mbar_wait(&mbar[buf], (phase >> buf) & 1u, p.err, 1)) {
+      // give up: let the copy in flight land (bounded), then stop
+      if (prefetched) mbar_wait(&mbar[buf ^ 1], (phase >> (buf ^ 1)) & 1u, p.err, 1);
+      return;
+    }
+    phase ^= 1u << buf;
+    const float2* rowa = stage + buf * 2 * T;
+    const float2* rowb = rowa + T;
+    const bool hasb = k + 1 < U.y;
+    const int4 ea = load_item(p.items, U.x + k);
+    const int4 eb = hasb ? load_item(p.items, U.x + k + 1) : ea;
+    float2 v[8];
+    {
+      float2 w[8];
+      gather<NP>(v, rowa, ord, msk);
+      if (hasb)
+        gather<NP>(w, rowb, ord, msk);
       else
-        fft<NP, false>(v, t, bufA, bufZ, p.tw);
-      const float2 zsum = bufZ[0];  // (sum p_a, sum p_b)
+#pragma unroll
+        for (int q = 0; q < 8; q++) w[q] = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int q = 0; q < 8; q++)
+        v[q] = make_float2(fmaf(v[q].x, v[q].x, v[q].y * v[q].y), fmaf(w[q].x, w[q].x, w[q].y * w[q].y));
+    }
+    if (ODD)
+      fft<NP, false, true>(v, t, bufZ, bufA, s_tw);
+    else
+      fft<NP, false, true>(v, t, bufA, bufZ, s_tw);
+    const float2 zsum = bufZ[0];  // (sum p_a, sum p_b)
 
 #pragma unroll 1
-      for (int s = 0; s < 2; s++) {
-        if (s == 1 && !hasb) break;
-        const int4 e = s ? eb : ea;
-        gather<NP>(v, s ? hb : ha, p.order, p.mask, t, T, true);
-        const float2* Y = fft<NP, false>(v, t, bufA, bufB, p.tw);
-        spectrum_v<NP>(v, t, Y, bufZ, p.mspec, s == 1);
-        __syncthreads();
-        const float2* W = fft<NP, true>(v, t, bufA, bufB, p.tw);
-        const float ps = s ? zsum.y : zsum.x;
-        const float P = np0 > 0.5f ? ps / np0 : 0.f;
-        if (FULL) {
-          const size_t mode = (size_t)e.x;
-          for (int tau = t; tau < L; tau += NT) {
-            const float np = __ldg(&p.npairs[tau]);
-            const float inv = np > 0.5f ? 1.f / np : 0.f;
+    for (int s = 0; s < 2; s++) {
+      if (s == 1 && !hasb) break;
+      const int4 e = s ? eb : ea;
+      gather<NP>(v, s ? rowb : rowa, ord, msk);
+      const float2* Y = fft<NP, false, true>(v, t, bufA, bufB, s_tw);
+      spectrum_v<NP>(v, t, Y, bufZ, p.mspec, s == 1);
+      __syncthreads();
+      const float2* W = fft<NP, true, true>(v, t, bufA, bufB, s_tw);
+      const float ps = s ? zsum.y : zsum.x;
+      const float P = np0 > 0.5f ? ps / np0 : 0.f;
+      if (FULL) {
+        const size_t mode = (size_t)e.x;
+        for (int tau = t; tau < L; tau += NT) {
+          const float np = s_np[tau];
+          const float inv = np > 0.5f ? 1.f / np : 0.f;
+          const float2 w0 = W[pad(tau)];
+          const float2 w1 = W[pad((NP - tau) & (NP - 1))];
+          const float gx = (w0.x + w1.x) * invn, gy = (w0.y - w1.y) * invn;
+          const float ee = (w0.y + w1.y) * invn;
+          p.outD[mode * L + tau] = (ee - 2.f * gx) * inv;
+          p.outC[mode * L + tau] = make_float2(gx * inv, gy * inv);
+        }
+        if (t == 0) p.outP[mode] = P;
+      } else {
+        // D and the drift sums of the lag pair (tau, tau+1) at owned lags
+        const double kx = e.y, ky = e.z;
+#pragma unroll
+        for (int r = 0; r < LPT; r++) {
+          const int tau = t + r * NT;
+          if (tau < L) {
+            const float n0 = s_np[tau];
+            const float inp = n0 > 0.5f ? 1.f / n0 : 0.f;
             const float2 w0 = W[pad(tau)];
             const float2 w1 = W[pad((NP - tau) & (NP - 1))];
             const float gx = (w0.x + w1.x) * invn, gy = (w0.y - w1.y) * invn;
             const float ee = (w0.y + w1.y) * invn;
-            p.outD[mode * L + tau] = (ee - 2.f * gx) * inv;
-            p.outC[mode * L + tau] = make_float2(gx * inv, gy * inv);
-          }
-          if (t == 0) p.outP[mode] = P;
-        } else {
-          // D and the drift sums of the lag pair (tau, tau+1) at owned lags
-          const double kx = e.y, ky = e.z;
-#pragma unroll
-          for (int r = 0; r < LPT; r++) {
-            const int tau = t + r * NT;
-            if (tau < L) {
-              const float n0 = __ldg(&p.npairs[tau]);
-              const float inp = n0 > 0.5f ? 1.f / n0 : 0.f;
-              const float2 w0 = W[pad(tau)];
-              const float2 w1 = W[pad((NP - tau) & (NP - 1))];
-              const float gx = (w0.x + w1.x) * invn, gy = (w0.y - w1.y) * invn;
-              const float ee = (w0.y + w1.y) * invn;
-              acc[r][0] += (double)((ee - 2.f * gx) * inp);
-              if (tau + 1 < L) {
-                const float n1 = __ldg(&p.npairs[tau + 1]);
-                const float inp1 = n1 > 0.5f ? 1.f / n1 : 0.f;
-                const float2 u0 = W[pad(tau + 1)];
-                const float2 u1 = W[pad((NP - tau - 1) & (NP - 1))];
-                const float cx = gx * inp, cy = gy * inp;
-                const float c1x = (u0.x + u1.x) * invn * inp1;
-                const float c1y = (u0.y - u1.y) * invn * inp1;
-                const float zr = fmaf(c1x, cx, c1y * cy);  // C(tau+1) conj C(tau)
-                const float zi = fmaf(c1y, cx, -c1x * cy);
-                const float w = sqrtf(fmaf(zr, zr, zi * zi));
-                if (w > 0.f) {
-                  const double wd = w, ph = atan2f(zi, zr);
-                  acc[r][1] += wd;
-                  acc[r][2] += wd * kx * kx;
-                  acc[r][3] += wd * kx * ky;
-                  acc[r][4] += wd * ky * ky;
-                  acc[r][5] += wd * kx * ph;
-                  acc[r][6] += wd * ky * ph;
-                  acc[r][7] += wd * ph * ph;
-                  acc[r][8] += 1.0;
-                }
+            acc[r][0] += (double)((ee - 2.f * gx) * inp);
+            if (tau + 1 < L) {
+              const float n1 = s_np[tau + 1];
+              const float inp1 = n1 > 0.5f ? 1.f / n1 : 0.f;
+              const float2 u0 = W[pad(tau + 1)];
+              const float2 u1 = W[pad((NP - tau - 1) & (NP - 1))];
+              const float cx = gx * inp, cy = gy * inp;
+              const float c1x = (u0.x + u1.x) * invn * inp1;
+              const float c1y = (u0.y - u1.y) * invn * inp1;
+              const float zr = fmaf(c1x, cx, c1y * cy);  // C(tau+1) conj C(tau)
+              const float zi = fmaf(c1y, cx, -c1x * cy);
+              const float w = sqrtf(fmaf(zr, zr, zi * zi));
+              if (w > 0.f) {
+                const double wd = w, ph = atan2f(zi, zr);
+                acc[r][1] += wd;
+                acc[r][2] += wd * kx * kx;
+                acc[r][3] += wd * kx * ky;
+                acc[r][4] += wd * ky * ky;
+                acc[r][5] += wd * kx * ph;
+                acc[r][6] += wd * ky * ph;
+                acc[r][7] += wd * ph * ph;
+                acc[r][8] += 1.0;
               }
             }
           }
-          accP += (double)P;
         }
-        __syncthreads();
+        accP += (double)P;
       }
+      __syncthreads();
     }
-    if (!FULL) {
-      // one partial record per unit: [u][field][tau], P after all records
+    if (k + 2 >= U.y) {
+      if (!FULL) {
+        // one partial record per unit: [u][field][tau], P after all records
 #pragma unroll
-      for (int r = 0; r < LPT; r++) {
-        const int tau = t + r * NT;
-        if (tau < L)
+        for (int r = 0; r < LPT; r++) {
+          const int tau = t + r * NT;
+          if (tau < L)
 #pragma unroll
-          for (int c = 0; c < PFIELDS; c++) p.partials[((size_t)u * PFIELDS + c) * L + tau] = acc[r][c];
+            for (int c = 0; c < PFIELDS; c++) {
+              p.partials[((size_t)u * PFIELDS + c) * L + tau] = acc[r][c];
+              acc[r][c] = 0.0;
+            }
+        }
+        if (t == 0) p.partials[(size_t)p.nunits * PFIELDS * L + u] = accP;
+        accP = 0.0;
       }
-      if (t == 0) p.partials[(size_t)p.nunits * PFIELDS * L + u] = accP;
+      u = unext;
+      k = 0;
+      if (t == 0) s_next = atomicAdd(p.unit_counter, 1);
+    } else {
+      k += 2;
     }
+    buf ^= 1;
+    fence_proxy_async_smem();  // this CTA's reads of the staged rows before the next TMA write
     __syncthreads();
+    unext = s_next;
   }
 }
 
@@ -308,7 +375,9 @@ __global__ void radial_full_kernel(RadialFullParams p) {
 // ------------------------------------------------------------------ launchers
 
 template <int NP>
-static size_t temporal_smem() { return 3 * sizeof(float2) * padded(NP); }
+static size_t temporal_smem(int T, int L) {
+  return sizeof(float2) * (3 * (size_t)padded(NP) + 4 * (size_t)T + NP) + sizeof(float) * (size_t)L;
+}
 
 static int lpt_of(int TPAD, int L) {
   const int NT = TPAD / 8;
@@ -319,7 +388,7 @@ static int lpt_of(int TPAD, int L) {
 template <int NP, int LPT, bool FULL>
 static cudaError_t launch_k(const TemporalParams& p, int grid, cudaStream_t s) {
   auto k = temporal_kernel<NP, LPT, FULL>;
-  const size_t sm = temporal_smem<NP>();
+  const size_t sm = temporal_smem<NP>(p.T, p.L);
   cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   k<<<grid, NP / 8, sm, s>>>(p);
   return cudaGetLastError();
@@ -336,9 +405,9 @@ static int occupancy_grid(K k, int threads, size_t smem) {
 }
 
 template <int NP>
-static cudaError_t dispatch_np(int L, bool full, const TemporalParams* p, int grid, cudaStream_t s,
-                               int* grid_out) {
-  const size_t sm = temporal_smem<NP>();
+static cudaError_t dispatch_np(int T, int L, bool full, const TemporalParams* p, int grid,
+                               cudaStream_t s, int* grid_out) {
+  const size_t sm = temporal_smem<NP>(T, L);
   if (full) {
     if (grid_out) *grid_out = occupancy_grid(temporal_kernel<NP, 1, true>, NP / 8, sm);
     return p ? launch_k<NP, 1, true>(*p, grid, s) : cudaSuccess;
@@ -356,28 +425,28 @@ static cudaError_t dispatch_np(int L, bool full, const TemporalParams* p, int gr
   }
 }
 
-static cudaError_t dispatch(int TPAD, int L, bool full, const TemporalParams* p, int grid,
+static cudaError_t dispatch(int TPAD, int T, int L, bool full, const TemporalParams* p, int grid,
                             cudaStream_t s, int* grid_out) {
   switch (TPAD) {
-    case 128: return dispatch_np<128>(L, full, p, grid, s, grid_out);
-    case 256: return dispatch_np<256>(L, full, p, grid, s, grid_out);
-    case 512: return dispatch_np<512>(L, full, p, grid, s, grid_out);
-    case 1024: return dispatch_np<1024>(L, full, p, grid, s, grid_out);
-    case 2048: return dispatch_np<2048>(L, full, p, grid, s, grid_out);
-    case 4096: return dispatch_np<4096>(L, full, p, grid, s, grid_out);
-    case 8192: return dispatch_np<8192>(L, full, p, grid, s, grid_out);
+    case 128: return dispatch_np<128>(T, L, full, p, grid, s, grid_out);
+    case 256: return dispatch_np<256>(T, L, full, p, grid, s, grid_out);
+    case 512: return dispatch_np<512>(T, L, full, p, grid, s, grid_out);
+    case 1024: return dispatch_np<1024>(T, L, full, p, grid, s, grid_out);
+    case 2048: return dispatch_np<2048>(T, L, full, p, grid, s, grid_out);
+    case 4096: return dispatch_np<4096>(T, L, full, p, grid, s, grid_out);
+    case 8192: return dispatch_np<8192>(T, L, full, p, grid, s, grid_out);
     default: return cudaErrorInvalidValue;
   }
 }
 
 cudaError_t launch_temporal(int TPAD, int L, bool full, const TemporalParams& p, int grid,
                             cudaStream_t s) {
-  return dispatch(TPAD, L, full, &p, grid, s, nullptr);
+  return dispatch(TPAD, p.T, L, full, &p, grid, s, nullptr);
 }
 
-int temporal_max_grid(int TPAD, int L, bool full) {
+int temporal_max_grid(int TPAD, int T, int L, bool full) {
   int g = 0;
-  dispatch(TPAD, L, full, nullptr, 0, nullptr, &g);
+  dispatch(TPAD, T, L, full, nullptr, 0, nullptr, &g);
   return g;
 }
 

@@ -164,6 +164,15 @@ double or_eval_model(const or_radial *r, const or_options *opt, double vbar,
                      double Z, double Dd, double Vmag, double alpha, int swim,
                      double *amps);
 
+/* ------------------------------------------------------------ per-bin LM (new) */
+/* FP64 Levenberg-Marquardt on one bin (see lm.c). bounds6 = (vmin, vmax,
+ * Zmin, Zmax, Dmin, Dmax); theta = (A, B, alpha, ln vbar, ln Z, ln D) in/out.
+ * Returns the iteration count. */
+int or_lm_fit(int nt, int K, const double *d, const double *tau, const double *qn, double w,
+              const double *bounds6, double *theta, int max_iter, double tol, double *cost_out);
+void or_lm_model(int nt, int K, const double *tau, const double *qn, const double *theta,
+                 double *y);
+
 /* ------------------------------------------------------------ sim.mjs */
 typedef struct {
   int N, T;

@@ -124,6 +124,9 @@ def lib():
         "or_eval_model": (C.c_double, [C.POINTER(_Radial), C.POINTER(_Options),
                                        C.c_double, C.c_double, C.c_double, C.c_double,
                                        C.c_double, C.c_int, _dp]),
+        "or_lm_fit": (C.c_int, [C.c_int, C.c_int, _dp, _dp, _dp, C.c_double, _dp, _dp, C.c_int,
+                                C.c_double, C.POINTER(C.c_double)]),
+        "or_lm_model": (None, [C.c_int, C.c_int, _dp, _dp, _dp, _dp]),
         "or_simulate": (None, [C.POINTER(_SimParams), _u8p, _u8p, _dp]),
         "or_mulberry32": (None, [C.c_uint32, _dp, C.c_int]),
         "or_rng_normals": (None, [C.c_uint32, _dp, C.c_int]),
@@ -508,3 +511,23 @@ def check_scenario(sc, res):
         if not d <= deg:
             fails.append(f"angle {res['driftAngleDeg']:.1f}")
     return fails
+
+
+# ------------------------------------------------------------------ per-bin LM (new)
+
+def lm_fit(d, tau, qn, w, bounds6, theta0, max_iter=200, tol=1e-10):
+    """FP64 LM on one bin (oracle/lm.c) -> (theta, cost, iterations)."""
+    th = np.array(theta0, np.float64)
+    cost = C.c_double()
+    it = lib().or_lm_fit(len(d), len(qn), np.ascontiguousarray(d, np.float64),
+                         np.ascontiguousarray(tau, np.float64), np.ascontiguousarray(qn, np.float64),
+                         float(w), np.ascontiguousarray(bounds6, np.float64), th, max_iter, tol,
+                         C.byref(cost))
+    return th, cost.value, it
+
+
+def lm_model(tau, qn, theta):
+    y = np.empty(len(tau))
+    lib().or_lm_model(len(tau), len(qn), np.ascontiguousarray(tau, np.float64),
+                      np.ascontiguousarray(qn, np.float64), np.ascontiguousarray(theta, np.float64), y)
+    return y

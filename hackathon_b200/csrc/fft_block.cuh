@@ -13,9 +13,12 @@
 // q = 0..7, so a caller can feed the first stage straight from registers and
 // read the natural-order result from shared memory at pad(k).
 //
-// Twiddles come from a table tw[j] = exp(-2*pi*i*j/n), j < n, computed on the
-// host in FP64 and rounded once to FP32 (as the reference's gpuTwiddles,
-// ddm_ref.js:566-574); no sin/cos is evaluated on the device.
+// Twiddles come from a host table computed in FP64 and rounded once to FP32
+// (as the reference's gpuTwiddles, ddm_ref.js:566-574); no sin/cos is
+// evaluated on the device. The table holds, for every stage with stride
+// Ns > 1 and radix R, a block w[(m-1)*Ns + k] = exp(-2*pi*i*m*k/(Ns*R)),
+// m = 1..R-1, k = 0..Ns-1: the lanes of a warp read consecutive k, so a
+// load is one wavefront (shared memory) or one cache line (global).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -40,6 +43,25 @@ template <bool INV>
 __device__ __forceinline__ float2 rot(float2 a) {
   return INV ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
 }
+
+// Number of stages of an n-point transform (radix 8 while possible, then 4/2).
+__host__ __device__ constexpr int fft_stages(int n) {
+  int s = 0;
+  for (int ns = 1; ns < n; ns *= ((n / ns) >= 8 ? 8 : (n / ns))) s++;
+  return s;
+}
+
+// Offset of the twiddle block of the stage with stride Ns, and table size.
+__host__ __device__ constexpr int tw_offset(int n, int Ns) {
+  int off = 0;
+  for (int ns = 1; ns < Ns;) {
+    const int r = (n / ns) >= 8 ? 8 : (n / ns);
+    if (ns > 1) off += (r - 1) * ns;
+    ns *= r;
+  }
+  return off;
+}
+__host__ __device__ constexpr int tw_size(int n) { return tw_offset(n, n); }
 
 template <int R, bool INV>
 struct Dft;
@@ -113,10 +135,10 @@ __device__ __forceinline__ void stage(float2 (&v)[8], int t, float2* __restrict_
 #pragma unroll
     for (int m = 0; m < R; m++) a[m] = v[i + B * m];
     if (Ns > 1) {
-      constexpr int step = n / (Ns * R);
+      const float2* tws = tw + tw_offset(n, Ns) + k;
 #pragma unroll
       for (int m = 1; m < R; m++) {
-        float2 w = TW_SMEM ? tw[k * m * step] : __ldg(&tw[k * m * step]);
+        float2 w = TW_SMEM ? tws[(m - 1) * Ns] : __ldg(&tws[(m - 1) * Ns]);
         if (INV) w.y = -w.y;
         a[m] = cmul(a[m], w);
       }
@@ -135,25 +157,39 @@ __device__ __forceinline__ void load8(float2 (&v)[8], int t, const float2* __res
   for (int q = 0; q < 8; q++) v[q] = buf[pad(t + q * NT)];
 }
 
-// Number of stages of an n-point transform (radix 8 while possible, then 4/2).
-__host__ __device__ constexpr int fft_stages(int n) {
-  int s = 0;
-  for (int ns = 1; ns < n; ns *= ((n / ns) >= 8 ? 8 : (n / ns))) s++;
-  return s;
+// Barrier between stages, scoped to the threads that share the transform:
+// SYNC_CTA the whole CTA; SYNC_GROUP a named barrier of the n/8 threads of
+// this group (id 1 + group); SYNC_WARP the warp (groups of <= 32 threads).
+enum { SYNC_CTA = 0, SYNC_GROUP = 1, SYNC_WARP = 2 };
+
+template <int n, int SYNC>
+__device__ __forceinline__ void stage_sync(int bar_id) {
+  if constexpr (SYNC == SYNC_WARP) {
+    __syncwarp();
+  } else if constexpr (SYNC == SYNC_GROUP) {
+    asm volatile("bar.sync %0, %1;" ::"r"(bar_id), "n"(n / 8) : "memory");
+  } else {
+    __syncthreads();
+  }
 }
 
-template <int n, int Ns, bool INV, bool TW_SMEM>
+// Sync scope for groups of n/8 threads, `groups` of them per CTA.
+__host__ __device__ constexpr int sync_kind(int n, int groups) {
+  return groups == 1 ? SYNC_CTA : (n / 8 <= 32 ? SYNC_WARP : SYNC_GROUP);
+}
+
+template <int n, int Ns, bool INV, bool TW_SMEM, int SYNC>
 struct Stages {
   // Runs the stages from stride Ns on; the stage writes `a`, the next one
-  // writes `b`. Ends with a __syncthreads after the last store.
+  // writes `b`. Ends with a barrier after the last store.
   static __device__ __forceinline__ void run(float2 (&v)[8], int t, float2* a, float2* b,
-                                             const float2* __restrict__ tw) {
+                                             const float2* __restrict__ tw, int bar_id) {
     constexpr int R = (n / Ns) >= 8 ? 8 : (n / Ns);
     stage<n, R, Ns, INV, TW_SMEM>(v, t, a, tw);
-    __syncthreads();
+    stage_sync<n, SYNC>(bar_id);
     if constexpr (Ns * R < n) {
       load8<n>(v, t, a);
-      Stages<n, Ns * R, INV, TW_SMEM>::run(v, t, b, a, tw);
+      Stages<n, Ns * R, INV, TW_SMEM, SYNC>::run(v, t, b, a, tw, bar_id);
     }
   }
 };
@@ -161,10 +197,10 @@ struct Stages {
 // Full n-point FFT of the 8 register points per thread (layout contract
 // above). Returns the buffer holding the natural-order result (read it at
 // pad(k)); the result lands in buf0 when the stage count is odd, else buf1.
-template <int n, bool INV, bool TW_SMEM = false>
+template <int n, bool INV, bool TW_SMEM = false, int SYNC = SYNC_CTA>
 __device__ __forceinline__ float2* fft(float2 (&v)[8], int t, float2* buf0, float2* buf1,
-                                       const float2* __restrict__ tw) {
-  Stages<n, 1, INV, TW_SMEM>::run(v, t, buf0, buf1, tw);
+                                       const float2* __restrict__ tw, int bar_id = 0) {
+  Stages<n, 1, INV, TW_SMEM, SYNC>::run(v, t, buf0, buf1, tw, bar_id);
   return (fft_stages(n) & 1) ? buf0 : buf1;
 }
 

@@ -38,12 +38,20 @@ std::vector<double> blackman_harris(int n) {
 }
 
 std::vector<float> twiddle_table(int n) {
-  std::vector<float> t(2 * (size_t)n);
-  for (int j = 0; j < n; j++) {
-    const double a = -2.0 * M_PI * j / n;
-    t[2 * j] = (float)std::cos(a);
-    t[2 * j + 1] = (float)std::sin(a);
+  // stage blocks w[(m-1)*Ns + k] = exp(-2 pi i m k / (Ns R)) (fft_block.cuh)
+  std::vector<float> t;
+  for (int ns = 1; ns < n;) {
+    const int r = (n / ns) >= 8 ? 8 : (n / ns);
+    if (ns > 1)
+      for (int m = 1; m < r; m++)
+        for (int k = 0; k < ns; k++) {
+          const double a = -2.0 * M_PI * (double)(m * k) / (double)(ns * r);
+          t.push_back((float)std::cos(a));
+          t.push_back((float)std::sin(a));
+        }
+    ns *= r;
   }
+  if (t.empty()) t.assign(2, 0.f);
   return t;
 }
 

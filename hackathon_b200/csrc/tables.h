@@ -18,7 +18,8 @@ void host_fft(std::vector<cd>& a, bool inverse);
 // 4-term periodic Blackman-Harris window (fft.js:126-133).
 std::vector<double> blackman_harris(int n);
 
-// exp(-2 pi i j / n), j < n, rounded to FP32 (re, im interleaved).
+// Per-stage twiddle blocks of the n-point device FFT (layout in
+// fft_block.cuh), FP64 rounded to FP32, re/im interleaved.
 std::vector<float> twiddle_table(int n);
 
 struct BinTable {

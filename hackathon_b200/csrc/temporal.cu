@@ -124,11 +124,11 @@ __global__ void __launch_bounds__(NP / 8, TemporalBounds<NP>::MIN_BLOCKS)
   const int t = threadIdx.x;
   const int T = p.T, L = p.L;
   float2* stage = sm + 3 * PN;        // [2 buffers][2 rows][T]
-  float2* s_tw = stage + 4 * T;       // twiddles exp(-2 pi i j / NP)
-  float* s_np = (float*)(s_tw + NP);  // N(tau), tau < L
+  float2* s_tw = stage + 4 * T;       // per-stage twiddle blocks
+  float* s_np = (float*)(s_tw + tw_size(NP));  // N(tau), tau < L
   const float np0 = p.npairs[0];
   const float invn = 0.5f / NP;
-  for (int i = t; i < NP; i += NT) s_tw[i] = p.tw[i];
+  for (int i = t; i < tw_size(NP); i += NT) s_tw[i] = p.tw[i];
   for (int i = t; i < L; i += NT) s_np[i] = p.npairs[i];
 
   uint32_t ord[4];
@@ -376,7 +376,7 @@ __global__ void radial_full_kernel(RadialFullParams p) {
 
 template <int NP>
 static size_t temporal_smem(int T, int L) {
-  return sizeof(float2) * (3 * (size_t)padded(NP) + 4 * (size_t)T + NP) + sizeof(float) * (size_t)L;
+  return sizeof(float2) * (3 * (size_t)padded(NP) + 4 * (size_t)T + tw_size(NP)) + sizeof(float) * (size_t)L;
 }
 
 static int lpt_of(int TPAD, int L) {

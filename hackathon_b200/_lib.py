@@ -45,6 +45,7 @@ _SIGS = {
     "ddm_throttled": (C.c_int64, [_vp]),
     "ddm_set_stream": (C.c_int, [_vp, _vp]),
     "ddm_kernel_launches": (C.c_int64, [_vp]),
+    "ddm_spectra_noalloc": (C.c_int, [_vp, _i32, _i32, _i32, _i32, _vp, C.c_float, _vp, _vp]),
 }
 
 _lib = None

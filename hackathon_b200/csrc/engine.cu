@@ -235,6 +235,10 @@ static int upload_mask_tables(ddm_engine *h, const uint8_t *mask) {
   return DDM_OK;
 }
 
+// Message slot shared by the calls that have no engine (ddm_create,
+// ddm_spectra_noalloc in noalloc.cu).
+std::string &ddm_detached_error() { return g_create_error; }
+
 extern "C" const char *ddm_create_error(void) { return g_create_error.c_str(); }
 
 extern "C" int ddm_create(const ddm_geometry *geometry, ddm_engine **out) {

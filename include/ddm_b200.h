@@ -58,7 +58,8 @@ enum ddm_status {
   DDM_ERR_CUDA = 2,    /* CUDA runtime failure */
   DDM_ERR_STATE = 3,   /* call not valid in the engine's state */
   DDM_ERR_NOMEM = 4,   /* device allocation failed */
-  DDM_ERR_NODEV = 5    /* no usable sm_100 device */
+  DDM_ERR_NODEV = 5,   /* no usable sm_100 device */
+  DDM_ERR_TOO_LARGE = 6 /* request exceeds a fixed maximum (ddm_spectra_noalloc) */
 };
 
 /* DdmEngine.create (ddm-engine.ts:125-149): device buffers, bin table
@@ -68,7 +69,8 @@ int ddm_create(const ddm_geometry *geometry, ddm_engine **out);
 void ddm_destroy(ddm_engine *h);
 /* Message of the last failed call on this engine ("" if none). */
 const char *ddm_last_error(const ddm_engine *h);
-/* Message of the last failed ddm_create (no engine exists yet). */
+/* Message of the last failed call that has no engine on this thread:
+ * ddm_create or ddm_spectra_noalloc. */
 const char *ddm_create_error(void);
 
 /* Resolved geometry (TPAD filled in). */
@@ -142,6 +144,31 @@ int64_t ddm_throttled(const ddm_engine *h);
 int ddm_set_stream(ddm_engine *h, void *stream);
 /* Kernels launched by this engine so far (instrumentation). */
 int64_t ddm_kernel_launches(const ddm_engine *h);
+
+/* Allocation-free spatial stage. No counterpart in the reference (its WebGPU
+ * engine allocates all buffers at create time); this is for callers that may
+ * not allocate device memory at all -- a host framework that owns every
+ * device allocation and only lends its plugins planned buffers, or a capture
+ * loop that must not enter cudaMalloc, which can stall on device-wide
+ * synchronisation. Needs no engine.
+ *
+ * Transforms n frames (DEVICE memory, N*N pixels of `dtype` each, luma =
+ * value * scale) exactly as ddm_ingest_frames_device does and writes frame i
+ * into ring slot slots[i] % T of the caller's DEVICE history `hist`
+ * (float2 [N*(N/2+1)][T], the readHistory layout), on `stream`
+ * (cudaStream_t as void*; NULL = legacy default stream). No spatial mask.
+ * It calls no cudaMalloc/cudaFree: its scratch is a fixed 8 MiB file-scope
+ * device array (plus < 1 MiB of tables) that every GPU loading the library
+ * holds until exit, so N is limited to 64..512 (DDM_ERR_TOO_LARGE above).
+ * The first call on a device, and any call that changes N or scale, does
+ * set-up (symbol lookups, table uploads, a stream synchronisation): make the
+ * first call before any stream capture. All calls share the scratch: calls
+ * whose work overlaps on the GPU race, so serialise them. Errors: DDM_ERR_ARG,
+ * DDM_ERR_TOO_LARGE, DDM_ERR_CUDA, DDM_ERR_NODEV; message from
+ * ddm_create_error(). */
+int ddm_spectra_noalloc(const void *frames, int32_t dtype, int32_t n, int32_t N,
+                        int32_t T, const int32_t *slots, float scale, void *hist,
+                        void *stream);
 
 #ifdef __cplusplus
 }

@@ -45,6 +45,8 @@ _SIGS = {
     "ddm_throttled": (C.c_int64, [_vp]),
     "ddm_set_stream": (C.c_int, [_vp, _vp]),
     "ddm_kernel_launches": (C.c_int64, [_vp]),
+    "ddm_fit_lm": (C.c_int, [_i32, _i32, _i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i32, _i32,
+                             C.c_double, _i32, _vp, _vp, _vp, _vp, _i32, _vp]),
     "ddm_spectra_noalloc": (C.c_int, [_vp, _i32, _i32, _i32, _i32, _vp, C.c_float, _vp, _vp]),
 }
 

@@ -81,6 +81,25 @@ struct RadialFullParams {
   double* odrift;
 };
 
+enum { LM_PLAIN = 0, LM_SEEDED = 1 };
+
+struct LmParams {
+  int nfit, nt_max, K;
+  const int* nt;           // [nfit] lags used by each fit (<= nt_max, <= 128)
+  const float* d;          // [nfit][nt_max] D(q_b, tau_j)
+  const float* tau;        // [nfit][nt_max] lag times
+  const float* qn;         // [nfit][K] effective-|k| nodes as q
+  const float* w;          // [nfit] weight (1 / max d, motility_fit.js:391)
+  const float* bounds;     // [nfit][6] vmin vmax Zmin Zmax Dmin Dmax
+  const float* start;      // [nfit][4] alpha vbar Z D (LM_SEEDED)
+  double* theta;           // [nfit][6] out: A B alpha ln vbar ln Z ln D
+  double* cost;            // [nfit] out
+  int* iters;              // [nfit] out (or nullptr)
+  int* evals;              // [nfit] out (or nullptr)
+  int mode, max_iter, nrefine;
+  double tol;
+};
+
 // launchers (return cudaGetLastError())
 cudaError_t launch_rows(int N, int dtype, const RowParams& p, cudaStream_t s);
 cudaError_t launch_cols(int N, const ColParams& p, cudaStream_t s);
@@ -92,5 +111,6 @@ cudaError_t launch_temporal(int TPAD, int L, bool full, const TemporalParams& p,
 int temporal_max_grid(int TPAD, int T, int L, bool full);
 cudaError_t launch_reduce(const ReduceParams& p, cudaStream_t s);
 cudaError_t launch_radial_full(const RadialFullParams& p, cudaStream_t s);
+cudaError_t launch_lm(const LmParams& p, cudaStream_t s);
 
 }  // namespace ddm

@@ -1,0 +1,520 @@
+// Batched Levenberg-Marquardt fit of the motility model, one warp per q-bin.
+//
+// Model (the reference's model column, motility_fit.js:417-432, per bin):
+//   y(tau) = A c(tau) + B,
+//   c(tau) = 1 - <exp(-D q^2 tau) (1 - alpha + alpha g(q vbar tau; Z))>_nodes
+// with g the Schulz-averaged 3D swimmer ISF (isf3d, motility_fit.js:140-144)
+// averaged over the bin's effective-|k| nodes. Parameters
+//   theta = (A, B, alpha, ln vbar, ln Z, ln D),  A, B >= 0, alpha in [0, 1],
+// ln vbar, ln Z, ln D clamped to the reference's bounds (bounds(),
+// motility_fit.js:480-491). The reference fits (alpha, vbar, Z, D) globally by
+// VarPro + Nelder-Mead (motility_fit.js:577-611); it has no LM. This kernel
+// solves the per-bin problem; the FP64 LM of oracle/lm.c is its checker.
+//
+// Per iteration each lane evaluates the model and the analytic Jacobian at its
+// lags (FP32, the ISF derivatives in closed form), accumulates J^T J, J^T r
+// and the cost in FP64, the warp reduces them, and every lane solves
+// (J^T J + lambda diag J^T J) delta = -J^T r by FP64 Cholesky (same values on
+// every lane, so control flow stays warp-uniform). Marquardt's rule: accept a
+// step that lowers the cost (lambda /= 3) else reject it (lambda *= 4); stop
+// after two consecutive accepted steps with relative decrease < tol, when
+// lambda > 1e12, or at max_iter -- the iteration of oracle/lm.c.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "../../include/ddm_b200.h"
+#include "kernels.cuh"
+
+namespace ddm {
+
+constexpr int LM_NP = 6;
+constexpr int LM_MAX_LAGS = 128;   // 4 per lane
+constexpr int LM_MAX_NODES = 8;
+constexpr int LM_WARPS = 8;        // fits per 256-thread CTA
+
+// g(x; Z) and its log-derivatives x dg/dx, Z dg/dZ (FP32).
+__device__ __forceinline__ void isf3d_d(float x, float Z, float& g, float& gx, float& gz) {
+  const float Z1 = Z + 1.f;
+  const float L = x / Z1;
+  if (L < 1e-4f) {
+    const float x2 = x * x;
+    g = 1.f - x2 * (Z + 2.f) / (6.f * Z1);
+    gx = -2.f * x2 * (Z + 2.f) / (6.f * Z1);
+    gz = x2 * Z / (6.f * Z1 * Z1);
+    return;
+  }
+  const float a = atanf(L), u = 1.f + L * L, lu = log1pf(L * L);
+  const float U = expf(0.5f * Z * lu);
+  float s, c;
+  sincosf(Z * a, &s, &c);
+  const float G = s / (Z * L * U);
+  const float LgL = c / (u * U) - G * (1.f + Z * L * L / u);
+  g = G;
+  gx = LgL;
+  gz = a * c / (L * U) - G - 0.5f * Z * G * lu - (Z / Z1) * LgL;
+}
+
+struct LmProblem {
+  int nt, K;
+  float w;
+  float qn[LM_MAX_NODES];
+  float d[4], tau[4];  // this lane's lags j = lane + 32 r
+  double lo[LM_NP], hi[LM_NP];
+};
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;  // the xor butterfly leaves the same bits on every lane
+}
+
+// Model column c(tau) at this lane's lags (FP32), 0 beyond nt.
+__device__ __forceinline__ void model_c(const LmProblem& P, int lane, float al, float v, float Z, float D,
+                                        float (&c)[4]) {
+  const float iK = 1.f / P.K;
+#pragma unroll
+  for (int r = 0; r < 4; r++) {
+    const int j = lane + 32 * r;
+    c[r] = 0.f;
+    if (j >= P.nt) continue;
+    const float t = P.tau[r];
+    float sE = 0.f;
+    for (int n = 0; n < P.K; n++) {
+      const float q = P.qn[n];
+      const float E = expf(-D * q * q * t);
+      if (al > 0.f) {
+        float g, gx, gz;
+        isf3d_d(q * v * t, Z, g, gx, gz);
+        sE += E * (1.f - al + al * g);
+      } else {
+        sE += E;
+      }
+    }
+    c[r] = 1.f - sE * iK;
+  }
+}
+
+// VarPro amplitudes at fixed nonlinear parameters: the 2-column NNLS of the
+// reference's evalModel (motility_fit.js:450-474) by nnls3's support
+// enumeration (:243-263) over {A}, {B}, {A, B}. Returns the weighted cost.
+__device__ __forceinline__ double varpro(const LmProblem& P, int lane, double al, double lv, double lZ,
+                                         double lD, double& A, double& B) {
+  float c[4];
+  model_c(P, lane, (float)al, (float)exp(lv), (float)exp(lZ), (float)exp(lD), c);
+  double g11 = 0, g12 = 0, h1 = 0, h2 = 0, dd = 0;
+#pragma unroll
+  for (int r = 0; r < 4; r++) {
+    if (lane + 32 * r >= P.nt) continue;
+    const double cc = c[r], d = P.d[r];
+    g11 += cc * cc;
+    g12 += cc;
+    h1 += cc * d;
+    h2 += d;
+    dd += d * d;
+  }
+  g11 = warp_sum(g11);
+  g12 = warp_sum(g12);
+  h1 = warp_sum(h1);
+  h2 = warp_sum(h2);
+  dd = warp_sum(dd);
+  const double n = P.nt;
+  double best = dd, bA = 0, bB = 0;
+  if (g11 > 1e-300) {
+    const double a = h1 / g11, rs = dd - a * h1;
+    if (a >= 0 && rs < best) best = rs, bA = a, bB = 0;
+  }
+  {
+    const double b = h2 / n, rs = dd - b * h2;
+    if (b >= 0 && rs < best) best = rs, bA = 0, bB = b;
+  }
+  {
+    const double det = g11 * n - g12 * g12, sc = fmax(g11, n);
+    if (fabs(det) > 1e-11 * sc * sc) {
+      const double a = (h1 * n - g12 * h2) / det, b = (g11 * h2 - g12 * h1) / det;
+      const double rs = dd - a * h1 - b * h2;
+      if (a >= 0 && b >= 0 && rs < best) best = rs, bA = a, bB = b;
+    }
+  }
+  A = bA;
+  B = bB;
+  return fmax(best, 0.0) * (double)P.w * (double)P.w;
+}
+
+// Normal equations at theta: H (upper triangle, 21), g (6), cost; warp-reduced.
+__device__ __forceinline__ void lm_normal(const LmProblem& P, const double (&th)[LM_NP], int lane,
+                                          double (&H)[21], double (&gr)[LM_NP], double& cost) {
+  const float A = (float)th[0], B = (float)th[1], al = (float)th[2];
+  const float v = (float)exp(th[3]), Z = (float)exp(th[4]), D = (float)exp(th[5]);
+  for (int i = 0; i < 21; i++) H[i] = 0.0;
+  for (int i = 0; i < LM_NP; i++) gr[i] = 0.0;
+  cost = 0.0;
+  const float iK = 1.f / P.K;
+#pragma unroll
+  for (int r = 0; r < 4; r++) {
+    const int j = lane + 32 * r;
+    if (j >= P.nt) break;
+    const float t = P.tau[r];
+    float sE = 0.f, sEg = 0.f, sdD = 0.f, sgx = 0.f, sgz = 0.f;
+    for (int n = 0; n < P.K; n++) {
+      const float q = P.qn[n];
+      const float E = expf(-D * q * q * t);
+      float g, gx, gz;
+      isf3d_d(q * v * t, Z, g, gx, gz);
+      const float mix = 1.f - al + al * g;
+      sE += E * mix;
+      sEg += E * (g - 1.f);
+      sdD += E * D * q * q * t * mix;
+      sgx += E * al * gx;
+      sgz += E * al * gz;
+    }
+    const float c = 1.f - sE * iK;
+    const double rr = (double)P.w * ((double)A * c + (double)B - (double)P.d[r]);
+    double J[LM_NP];
+    J[0] = (double)P.w * c;
+    J[1] = (double)P.w;
+    J[2] = (double)(-P.w * A * sEg * iK);
+    J[3] = (double)(-P.w * A * sgx * iK);
+    J[4] = (double)(-P.w * A * sgz * iK);
+    J[5] = (double)(P.w * A * sdD * iK);
+    cost += rr * rr;
+    int k = 0;
+#pragma unroll
+    for (int a = 0; a < LM_NP; a++) {
+      gr[a] += J[a] * rr;
+#pragma unroll
+      for (int b = a; b < LM_NP; b++) H[k++] += J[a] * J[b];
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 21; i++) H[i] = warp_sum(H[i]);
+#pragma unroll
+  for (int i = 0; i < LM_NP; i++) gr[i] = warp_sum(gr[i]);
+  cost = warp_sum(cost);
+}
+
+// (H + lambda diag H) delta = -g by Cholesky; false if not positive definite.
+__device__ __forceinline__ bool lm_solve(const double (&H)[21], const double (&gr)[LM_NP], double lambda,
+                                         double (&delta)[LM_NP]) {
+  double M[LM_NP][LM_NP];
+  int k = 0;
+#pragma unroll
+  for (int a = 0; a < LM_NP; a++)
+#pragma unroll
+    for (int b = a; b < LM_NP; b++) M[a][b] = M[b][a] = H[k++];
+#pragma unroll
+  for (int a = 0; a < LM_NP; a++) M[a][a] += lambda * (M[a][a] > 0 ? M[a][a] : 1e-30);
+  double Lm[LM_NP][LM_NP];
+#pragma unroll
+  for (int i = 0; i < LM_NP; i++) {
+#pragma unroll
+    for (int j = 0; j <= i; j++) {
+      double s = M[i][j];
+#pragma unroll
+      for (int q = 0; q < j; q++) s -= Lm[i][q] * Lm[j][q];
+      if (i == j) {
+        if (!(s > 0)) return false;
+        Lm[i][i] = sqrt(s);
+      } else {
+        Lm[i][j] = s / Lm[j][j];
+      }
+    }
+  }
+  double y[LM_NP];
+#pragma unroll
+  for (int i = 0; i < LM_NP; i++) {
+    double s = -gr[i];
+#pragma unroll
+    for (int q = 0; q < i; q++) s -= Lm[i][q] * y[q];
+    y[i] = s / Lm[i][i];
+  }
+#pragma unroll
+  for (int i = LM_NP - 1; i >= 0; i--) {
+    double s = y[i];
+#pragma unroll
+    for (int q = i + 1; q < LM_NP; q++) s -= Lm[q][i] * delta[q];
+    delta[i] = s / Lm[i][i];
+  }
+  return true;
+}
+
+// Marquardt iteration from th (projected, amplitudes set); returns iterations.
+__device__ int lm_run(const LmProblem& P, int lane, double (&th)[LM_NP], double& cost, int max_iter,
+                      double tol) {
+  double H[21], gr[LM_NP];
+  lm_normal(P, th, lane, H, gr, cost);
+  double lambda = 1e-3;
+  int small = 0, it = 0;
+  for (it = 0; it < max_iter; it++) {
+    double delta[LM_NP];
+    if (!lm_solve(H, gr, lambda, delta)) {
+      lambda *= 4;
+      if (lambda > 1e12) break;
+      continue;
+    }
+    double th2[LM_NP];
+#pragma unroll
+    for (int a = 0; a < LM_NP; a++) th2[a] = fmin(P.hi[a], fmax(P.lo[a], th[a] + delta[a]));
+    double H2[21], g2[LM_NP], c2;
+    lm_normal(P, th2, lane, H2, g2, c2);
+    if (c2 < cost) {
+      const double rel = (cost - c2) / (cost > 0 ? cost : 1e-300);
+#pragma unroll
+      for (int a = 0; a < LM_NP; a++) {
+        th[a] = th2[a];
+        gr[a] = g2[a];
+      }
+#pragma unroll
+      for (int i = 0; i < 21; i++) H[i] = H2[i];
+      cost = c2;
+      lambda = fmax(lambda / 3, 1e-12);
+      small = rel < tol ? small + 1 : 0;
+      if (small >= 2) {
+        it++;
+        break;
+      }
+    } else {
+      lambda *= 4;
+      if (lambda > 1e12) break;
+    }
+  }
+  return it;
+}
+
+__global__ void __launch_bounds__(32 * LM_WARPS) lm_kernel(LmParams p) {
+  const int lane = threadIdx.x & 31;
+  const int fit = blockIdx.x * LM_WARPS + (threadIdx.x >> 5);
+  if (fit >= p.nfit) return;  // whole warp
+  LmProblem P;
+  P.nt = min(p.nt[fit], min(p.nt_max, LM_MAX_LAGS));
+  P.K = min(p.K, LM_MAX_NODES);
+  P.w = p.w[fit];
+#pragma unroll
+  for (int n = 0; n < LM_MAX_NODES; n++) P.qn[n] = n < P.K ? p.qn[(size_t)fit * p.K + n] : 0.f;
+#pragma unroll
+  for (int r = 0; r < 4; r++) {
+    const int j = lane + 32 * r;
+    const bool in = j < P.nt;
+    P.d[r] = in ? p.d[(size_t)fit * p.nt_max + j] : 0.f;
+    P.tau[r] = in ? p.tau[(size_t)fit * p.nt_max + j] : 0.f;
+  }
+  const float* bd = p.bounds + (size_t)fit * 6;
+  P.lo[0] = 0.0;
+  P.hi[0] = 1e300;
+  P.lo[1] = 0.0;
+  P.hi[1] = 1e300;
+  P.lo[2] = 0.0;
+  P.hi[2] = 1.0;
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    P.lo[3 + a] = log((double)bd[2 * a]);
+    P.hi[3 + a] = log((double)bd[2 * a + 1]);
+  }
+  double th[LM_NP], cost = 0;
+  int iters = 0, evals = 0;
+  if (p.mode == LM_SEEDED) {
+    const float* s = p.start + (size_t)fit * 4;
+    th[2] = (double)s[0];
+    th[3] = log((double)s[1]);
+    th[4] = log((double)s[2]);
+    th[5] = log((double)s[3]);
+#pragma unroll
+    for (int a = 2; a < LM_NP; a++) th[a] = fmin(P.hi[a], fmax(P.lo[a], th[a]));
+    varpro(P, lane, th[2], th[3], th[4], th[5], th[0], th[1]);
+    iters = lm_run(P, lane, th, cost, p.max_iter, p.tol);
+    evals = 2 + iters;
+  } else {
+    // the reference's start strategy (fitBrownian, motility_fit.js:500-536;
+    // fitSwimmer :577-611), per bin; oracle/lm.c or_lm_fit_plain
+    double A, B;
+    const double lo = P.lo[5], hi = P.hi[5];
+    int bi = 0;
+    double bf = 1e308;
+    for (int i = 0; i <= 48; i++) {
+      const double x = lo + ((hi - lo) * i) / 48;
+      const double v = varpro(P, lane, 0.0, P.lo[3], 0.0, x, A, B);
+      if (v < bf) bf = v, bi = i;
+    }
+    evals += 49;
+    double a = lo + ((hi - lo) * (bi > 0 ? bi - 1 : 0)) / 48;
+    double b = lo + ((hi - lo) * (bi < 48 ? bi + 1 : 48)) / 48;
+    const double gr = (sqrt(5.0) - 1) / 2;
+    double c = b - gr * (b - a), dd = a + gr * (b - a);
+    double fc = varpro(P, lane, 0.0, P.lo[3], 0.0, c, A, B);
+    double fd = varpro(P, lane, 0.0, P.lo[3], 0.0, dd, A, B);
+    evals += 2;
+    for (int it = 0; it < 60 && b - a > 1e-6; it++) {
+      if (fc < fd) {
+        b = dd;
+        dd = c;
+        fd = fc;
+        c = b - gr * (b - a);
+        fc = varpro(P, lane, 0.0, P.lo[3], 0.0, c, A, B);
+      } else {
+        a = c;
+        c = dd;
+        fc = fd;
+        dd = a + gr * (b - a);
+        fd = varpro(P, lane, 0.0, P.lo[3], 0.0, dd, A, B);
+      }
+      evals++;
+    }
+    const double lD0 = fc < fd ? c : dd;
+    // 64 starts: lane l holds starts 2l and 2l+1 (index = 4 iv + 2 iz + ia)
+    const double lZs0 = fmin(P.hi[4], fmax(P.lo[4], log(1.5)));
+    const double lZs1 = fmin(P.hi[4], fmax(P.lo[4], log(8.0)));
+    double sc[2];
+    for (int s = 0; s < 64; s++) {
+      const int iv = s >> 2, iz = (s >> 1) & 1, ia = s & 1;
+      const double lv = P.lo[3] + ((P.hi[3] - P.lo[3]) * (iv + 0.5)) / 16;
+      const double f = varpro(P, lane, ia ? 0.8 : 0.3, lv, iz ? lZs1 : lZs0, lD0, A, B);
+      if ((s >> 1) == lane) sc[s & 1] = f;
+    }
+    evals += 64;
+    double best = 1e308;
+    double bth[LM_NP] = {0, 0, 0, 0, 0, 0};
+    for (int k = 0; k < p.nrefine && k < 64; k++) {
+      // k-th smallest cost, lowest index on ties (a stable sort's order)
+      double m = sc[0] <= sc[1] ? sc[0] : sc[1];
+      int mi = sc[0] <= sc[1] ? 2 * lane : 2 * lane + 1;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const double m2 = __shfl_xor_sync(0xffffffffu, m, o);
+        const int i2 = __shfl_xor_sync(0xffffffffu, mi, o);
+        if (m2 < m || (m2 == m && i2 < mi)) m = m2, mi = i2;
+      }
+      if ((mi >> 1) == lane) sc[mi & 1] = 1e308;  // taken
+      const int iv = mi >> 2, iz = (mi >> 1) & 1, ia = mi & 1;
+      double t2[LM_NP];
+      t2[2] = ia ? 0.8 : 0.3;
+      t2[3] = P.lo[3] + ((P.hi[3] - P.lo[3]) * (iv + 0.5)) / 16;
+      t2[4] = iz ? lZs1 : lZs0;
+      t2[5] = lD0;
+      varpro(P, lane, t2[2], t2[3], t2[4], t2[5], t2[0], t2[1]);
+      double cst;
+      const int it = lm_run(P, lane, t2, cst, p.max_iter, p.tol);
+      iters += it;
+      evals += 2 + it;
+      if (cst < best) {
+        best = cst;
+#pragma unroll
+        for (int q = 0; q < LM_NP; q++) bth[q] = t2[q];
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < LM_NP; q++) th[q] = bth[q];
+    cost = best;
+  }
+#pragma unroll
+  for (int a = 0; a < LM_NP; a++)
+    if (lane == a) p.theta[(size_t)fit * LM_NP + a] = th[a];
+  if (lane == 0) {
+    p.cost[fit] = cost;
+    if (p.iters) p.iters[fit] = iters;
+    if (p.evals) p.evals[fit] = evals;
+  }
+}
+
+cudaError_t launch_lm(const LmParams& p, cudaStream_t s) {
+  if (p.nfit <= 0) return cudaSuccess;
+  const int grid = (p.nfit + LM_WARPS - 1) / LM_WARPS;
+  lm_kernel<<<grid, 32 * LM_WARPS, 0, s>>>(p);
+  return cudaGetLastError();
+}
+
+}  // namespace ddm
+
+// ------------------------------------------------------------------ C ABI
+#include <cstdarg>
+#include <cstdio>
+#include <string>
+
+extern std::string& ddm_detached_error();  // message slot of calls without an engine (engine.cu)
+
+namespace {
+
+int lm_fail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  ddm_detached_error() = buf;
+  return code;
+}
+
+template <typename T>
+cudaError_t stage_in(T** dst, const T* src, size_t n, cudaStream_t s) {
+  cudaError_t e = cudaMallocAsync((void**)dst, sizeof(T) * (n ? n : 1), s);
+  if (e != cudaSuccess || !src) return e;
+  return cudaMemcpyAsync(*dst, src, sizeof(T) * n, cudaMemcpyHostToDevice, s);
+}
+
+}  // namespace
+
+extern "C" int ddm_fit_lm(int32_t nfit, int32_t nt_max, int32_t K, const int32_t* nt, const float* d,
+                          const float* tau, const float* qn, const float* w, const float* bounds,
+                          const float* start, int32_t mode, int32_t max_iter, double tol,
+                          int32_t nrefine, double* theta, double* cost, int32_t* iters, int32_t* evals,
+                          int32_t on_device, void* stream) {
+  ddm_detached_error().clear();
+  if (nfit < 0 || nt_max < 1 || nt_max > ddm::LM_MAX_LAGS || K < 1 || K > ddm::LM_MAX_NODES)
+    return lm_fail(DDM_ERR_ARG, "ddm_fit_lm: need nfit >= 0, 1 <= nt_max <= %d, 1 <= K <= %d",
+                   ddm::LM_MAX_LAGS, ddm::LM_MAX_NODES);
+  if (mode != ddm::LM_PLAIN && mode != ddm::LM_SEEDED)
+    return lm_fail(DDM_ERR_ARG, "ddm_fit_lm: mode must be 0 (reference starts) or 1 (seeded)");
+  if (max_iter < 1 || nrefine < 1 || nrefine > 64 || !(tol >= 0))
+    return lm_fail(DDM_ERR_ARG, "ddm_fit_lm: need max_iter >= 1, 1 <= nrefine <= 64, tol >= 0");
+  if (nfit == 0) return DDM_OK;
+  if (!nt || !d || !tau || !qn || !w || !bounds || !theta || !cost || (mode == ddm::LM_SEEDED && !start))
+    return lm_fail(DDM_ERR_ARG, "ddm_fit_lm: null array");
+  cudaStream_t s = (cudaStream_t)stream;
+  ddm::LmParams p{};
+  p.nfit = nfit;
+  p.nt_max = nt_max;
+  p.K = K;
+  p.mode = mode;
+  p.max_iter = max_iter;
+  p.nrefine = nrefine;
+  p.tol = tol;
+  if (on_device) {
+    p.nt = nt; p.d = d; p.tau = tau; p.qn = qn; p.w = w; p.bounds = bounds; p.start = start;
+    p.theta = theta; p.cost = cost; p.iters = iters; p.evals = evals;
+    cudaError_t e = ddm::launch_lm(p, s);
+    if (e != cudaSuccess) return lm_fail(DDM_ERR_CUDA, "ddm_fit_lm: %s", cudaGetErrorString(e));
+    return DDM_OK;
+  }
+  const size_t nf = (size_t)nfit, nd = nf * nt_max;
+  int *dnt = nullptr, *dit = nullptr, *dev = nullptr;
+  float *dd = nullptr, *dtau = nullptr, *dqn = nullptr, *dw = nullptr, *db = nullptr, *ds = nullptr;
+  double *dth = nullptr, *dc = nullptr;
+  cudaError_t e = cudaSuccess;
+  auto step = [&](cudaError_t x) { if (e == cudaSuccess) e = x; };
+  step(stage_in(&dnt, nt, nf, s));
+  step(stage_in(&dd, d, nd, s));
+  step(stage_in(&dtau, tau, nd, s));
+  step(stage_in(&dqn, qn, nf * K, s));
+  step(stage_in(&dw, w, nf, s));
+  step(stage_in(&db, bounds, nf * 6, s));
+  if (mode == ddm::LM_SEEDED) step(stage_in(&ds, start, nf * 4, s));
+  step(stage_in<double>(&dth, nullptr, nf * 6, s));
+  step(stage_in<double>(&dc, nullptr, nf, s));
+  step(stage_in<int>(&dit, nullptr, nf, s));
+  step(stage_in<int>(&dev, nullptr, nf, s));
+  if (e == cudaSuccess) {
+    p.nt = dnt; p.d = dd; p.tau = dtau; p.qn = dqn; p.w = dw; p.bounds = db; p.start = ds;
+    p.theta = dth; p.cost = dc; p.iters = dit; p.evals = dev;
+    step(ddm::launch_lm(p, s));
+    step(cudaMemcpyAsync(theta, dth, sizeof(double) * nf * 6, cudaMemcpyDeviceToHost, s));
+    step(cudaMemcpyAsync(cost, dc, sizeof(double) * nf, cudaMemcpyDeviceToHost, s));
+    if (iters) step(cudaMemcpyAsync(iters, dit, sizeof(int) * nf, cudaMemcpyDeviceToHost, s));
+    if (evals) step(cudaMemcpyAsync(evals, dev, sizeof(int) * nf, cudaMemcpyDeviceToHost, s));
+  }
+  for (void* ptr : {(void*)dnt, (void*)dd, (void*)dtau, (void*)dqn, (void*)dw, (void*)db, (void*)ds,
+                    (void*)dth, (void*)dc, (void*)dit, (void*)dev})
+    if (ptr) cudaFreeAsync(ptr, s);
+  step(cudaStreamSynchronize(s));
+  if (e != cudaSuccess) return lm_fail(DDM_ERR_CUDA, "ddm_fit_lm: %s", cudaGetErrorString(e));
+  return DDM_OK;
+}

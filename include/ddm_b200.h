@@ -145,6 +145,35 @@ int ddm_set_stream(ddm_engine *h, void *stream);
 /* Kernels launched by this engine so far (instrumentation). */
 int64_t ddm_kernel_launches(const ddm_engine *h);
 
+/* Batched per-bin Levenberg-Marquardt fit of the motility model (the fit
+ * stage of analyzeMotility, motility-ddm/src/motility_fit.js:577-611, per
+ * q-bin). The reference fits (alpha, vbar, Z, D) globally by VarPro +
+ * Nelder-Mead and has no LM; this solves, for each of nfit bins, one warp per
+ * bin,
+ *   min sum_j (w (A c(tau_j) + B - d_j))^2,
+ *   c = 1 - <exp(-D q^2 tau) (1 - alpha + alpha g(q vbar tau; Z))>_nodes
+ * (modelColumn, motility_fit.js:417-432, 3D Schulz swimmer ISF g) over
+ * theta = (A, B, alpha, ln vbar, ln Z, ln D), A, B >= 0, alpha in [0, 1], the
+ * rest clamped to bounds[6*i..] = (vmin, vmax, Zmin, Zmax, Dmin, Dmax)
+ * (bounds(), :480-491). Model in FP32, normal equations (J^T J + lambda I,
+ * Marquardt scaling) and the Cholesky solve in FP64.
+ *   mode 0: the reference's start strategy per bin -- 49-point ln D Brownian
+ *           scan + golden section (fitBrownian :500-536), then 64 starts
+ *           (16 vbar x Z in {1.5, 8} x alpha in {0.3, 0.8}, fitSwimmer
+ *           :589-601) ranked by VarPro cost, LM from the best `nrefine`.
+ *   mode 1: LM from start[4*i..] = (alpha, vbar, Z, D) (e.g. the surrogate's
+ *           prediction), amplitudes from VarPro.
+ * Arrays: nt[nfit] lags per fit (<= nt_max <= 128), d and tau [nfit][nt_max],
+ * qn [nfit][K] (K <= 8), w[nfit], bounds [nfit][6], start [nfit][4];
+ * out theta [nfit][6], cost[nfit], iters/evals [nfit] (may be NULL).
+ * on_device = 0: host arrays, blocks until done; 1: device arrays, queued on
+ * `stream` (cudaStream_t as void*). Errors via ddm_create_error(). */
+int ddm_fit_lm(int32_t nfit, int32_t nt_max, int32_t K, const int32_t *nt, const float *d,
+               const float *tau, const float *qn, const float *w, const float *bounds,
+               const float *start, int32_t mode, int32_t max_iter, double tol, int32_t nrefine,
+               double *theta, double *cost, int32_t *iters, int32_t *evals, int32_t on_device,
+               void *stream);
+
 /* Allocation-free spatial stage. No counterpart in the reference (its WebGPU
  * engine allocates all buffers at create time); this is for callers that may
  * not allocate device memory at all -- a host framework that owns every

@@ -213,3 +213,188 @@ void or_lm_model(int nt, int K, const double *tau, const double *qn, const doubl
   model(&P, theta, r, NULL);
   for (int j = 0; j < nt; j++) y[j] = r[j];
 }
+
+/* ------------------------------------------------------------------ starts */
+
+/* VarPro amplitudes at fixed (alpha, vbar, Z, D): the 2-column NNLS of
+ * evalModel (motility_fit.js:450-474) by nnls3's support enumeration
+ * (:243-263) over {A}, {B}, {A, B}; returns the weighted cost and A, B. */
+static double varpro(const lm_prob *P, double al, double lv, double lZ, double lD, double *A,
+                     double *B) {
+  double th[NP] = {1, 0, al, lv, lZ, lD}, r[512];
+  /* model() with A = 1, B = 0 and d = 0 gives w*c in r */
+  lm_prob Q = *P;
+  double zero[512];
+  memset(zero, 0, sizeof(double) * P->nt);
+  Q.d = zero;
+  Q.w = 1.0;
+  model(&Q, th, r, NULL);
+  double g11 = 0, g12 = 0, h1 = 0, h2 = 0, dd = 0;
+  for (int j = 0; j < P->nt; j++) {
+    const double c = r[j], d = P->d[j];
+    g11 += c * c;
+    g12 += c;
+    h1 += c * d;
+    h2 += d;
+    dd += d * d;
+  }
+  const double n = P->nt;
+  double best = dd, bA = 0, bB = 0;
+  /* {A} */
+  if (g11 > 1e-300) {
+    const double a = h1 / g11;
+    const double rs = dd - a * h1;
+    if (a >= 0 && rs < best) best = rs, bA = a, bB = 0;
+  }
+  /* {B} */
+  {
+    const double b = h2 / n;
+    const double rs = dd - b * h2;
+    if (b >= 0 && rs < best) best = rs, bA = 0, bB = b;
+  }
+  /* {A, B} */
+  {
+    const double det = g11 * n - g12 * g12;
+    const double sc = fmax(g11, n);
+    if (fabs(det) > 1e-11 * sc * sc) {
+      const double a = (h1 * n - g12 * h2) / det, b = (g11 * h2 - g12 * h1) / det;
+      const double rs = dd - a * h1 - b * h2;
+      if (a >= 0 && b >= 0 && rs < best) best = rs, bA = a, bB = b;
+    }
+  }
+  *A = bA;
+  *B = bB;
+  return fmax(best, 0.0) * P->w * P->w;
+}
+
+static void init_prob(lm_prob *P, int nt, int K, const double *d, const double *tau,
+                      const double *qn, double w, const double *bounds6) {
+  P->nt = nt;
+  P->K = K;
+  P->d = d;
+  P->tau = tau;
+  P->qn = qn;
+  P->w = w;
+  P->lo[0] = 0;
+  P->hi[0] = INFINITY;
+  P->lo[1] = 0;
+  P->hi[1] = INFINITY;
+  P->lo[2] = 0;
+  P->hi[2] = 1;
+  P->lo[3] = log(bounds6[0]);
+  P->hi[3] = log(bounds6[1]);
+  P->lo[4] = log(bounds6[2]);
+  P->hi[4] = log(bounds6[3]);
+  P->lo[5] = log(bounds6[4]);
+  P->hi[5] = log(bounds6[5]);
+}
+
+/* LM from one start (alpha, vbar, Z, D), amplitudes from VarPro. */
+int or_lm_fit_start(int nt, int K, const double *d, const double *tau, const double *qn, double w,
+                    const double *bounds6, const double *start4, int max_iter, double tol,
+                    double *theta, double *cost_out) {
+  lm_prob P;
+  init_prob(&P, nt, K, d, tau, qn, w, bounds6);
+  double th[NP] = {0, 0, start4[0], log(start4[1]), log(start4[2]), log(start4[3])};
+  project(&P, th);
+  varpro(&P, th[2], th[3], th[4], th[5], &th[0], &th[1]);
+  memcpy(theta, th, sizeof th);
+  return or_lm_fit(nt, K, d, tau, qn, w, bounds6, theta, max_iter, tol, cost_out);
+}
+
+/* The reference's start strategy, per bin (fitBrownian :500-536 then
+ * fitSwimmer :577-611 with LM in place of Nelder-Mead):
+ *  1. Brownian null (alpha = 0): 49-point scan of ln D over [Dmin, Dmax],
+ *     golden section on the bracketing interval (<= 60 steps, width 1e-6);
+ *  2. 64 starts at that D: 16 ln vbar at the centres of equal cells of
+ *     [vmin, vmax], Z in {1.5, 8}, alpha in {0.3, 0.8}, ranked by the VarPro
+ *     cost (stable order on ties);
+ *  3. LM from the best `nrefine` starts; the lowest cost wins (first on ties).
+ * Returns total LM iterations; *evals counts model evaluations. */
+int or_lm_fit_plain(int nt, int K, const double *d, const double *tau, const double *qn, double w,
+                    const double *bounds6, int max_iter, double tol, int nrefine, double *theta,
+                    double *cost_out, int *evals) {
+  lm_prob P;
+  init_prob(&P, nt, K, d, tau, qn, w, bounds6);
+  double A, B;
+  int ne = 0;
+  const double lo = P.lo[5], hi = P.hi[5];
+  const int n = 48;
+  int bi = 0;
+  double bf = INFINITY, xs[49];
+  for (int i = 0; i <= n; i++) {
+    xs[i] = lo + ((hi - lo) * i) / n;
+    const double v = varpro(&P, 0, P.lo[3], 0, xs[i], &A, &B);
+    ne++;
+    if (v < bf) bf = v, bi = i;
+  }
+  double a = xs[bi > 0 ? bi - 1 : 0], b = xs[bi < n ? bi + 1 : n];
+  const double gr = (sqrt(5.0) - 1) / 2;
+  double c = b - gr * (b - a), dd = a + gr * (b - a);
+  double fc = varpro(&P, 0, P.lo[3], 0, c, &A, &B), fd = varpro(&P, 0, P.lo[3], 0, dd, &A, &B);
+  ne += 2;
+  for (int it = 0; it < 60 && b - a > 1e-6; it++) {
+    if (fc < fd) {
+      b = dd;
+      dd = c;
+      fd = fc;
+      c = b - gr * (b - a);
+      fc = varpro(&P, 0, P.lo[3], 0, c, &A, &B);
+    } else {
+      a = c;
+      c = dd;
+      fc = fd;
+      dd = a + gr * (b - a);
+      fd = varpro(&P, 0, P.lo[3], 0, dd, &A, &B);
+    }
+    ne++;
+  }
+  const double lD0 = fc < fd ? c : dd;
+  /* 64 starts */
+  double su[64][3], sf[64];
+  int ord[64], ns = 0;
+  const double lZs[2] = {log(1.5), log(8.0)}, als[2] = {0.3, 0.8};
+  for (int i = 0; i < 16; i++) {
+    const double lv = P.lo[3] + ((P.hi[3] - P.lo[3]) * (i + 0.5)) / 16;
+    for (int z = 0; z < 2; z++)
+      for (int q = 0; q < 2; q++) {
+        const double lZ = fmin(P.hi[4], fmax(P.lo[4], lZs[z]));
+        su[ns][0] = als[q];
+        su[ns][1] = lv;
+        su[ns][2] = lZ;
+        sf[ns] = varpro(&P, als[q], lv, lZ, lD0, &A, &B);
+        ord[ns] = ns;
+        ns++;
+        ne++;
+      }
+  }
+  for (int i = 1; i < ns; i++) { /* stable insertion sort by cost */
+    const int o = ord[i];
+    int j = i - 1;
+    while (j >= 0 && sf[ord[j]] > sf[o]) {
+      ord[j + 1] = ord[j];
+      j--;
+    }
+    ord[j + 1] = o;
+  }
+  double best = INFINITY, bth[NP] = {0};
+  int iters = 0;
+  for (int s = 0; s < nrefine && s < ns; s++) {
+    const int o = ord[s];
+    double th[NP] = {0, 0, su[o][0], su[o][1], su[o][2], lD0};
+    varpro(&P, th[2], th[3], th[4], th[5], &th[0], &th[1]);
+    ne++;
+    double cst;
+    const int it = or_lm_fit(nt, K, d, tau, qn, w, bounds6, th, max_iter, tol, &cst);
+    iters += it;
+    ne += 1 + it;
+    if (cst < best) {
+      best = cst;
+      memcpy(bth, th, sizeof th);
+    }
+  }
+  memcpy(theta, bth, sizeof bth);
+  *cost_out = best;
+  if (evals) *evals = ne;
+  return iters;
+}

@@ -172,6 +172,15 @@ int or_lm_fit(int nt, int K, const double *d, const double *tau, const double *q
               const double *bounds6, double *theta, int max_iter, double tol, double *cost_out);
 void or_lm_model(int nt, int K, const double *tau, const double *qn, const double *theta,
                  double *y);
+/* LM from start4 = (alpha, vbar, Z, D) with VarPro amplitudes. */
+int or_lm_fit_start(int nt, int K, const double *d, const double *tau, const double *qn, double w,
+                    const double *bounds6, const double *start4, int max_iter, double tol,
+                    double *theta, double *cost_out);
+/* LM from the reference's start strategy (Brownian scan, 64 starts, best
+ * nrefine refined). */
+int or_lm_fit_plain(int nt, int K, const double *d, const double *tau, const double *qn, double w,
+                    const double *bounds6, int max_iter, double tol, int nrefine, double *theta,
+                    double *cost_out, int *evals);
 
 /* ------------------------------------------------------------ sim.mjs */
 typedef struct {

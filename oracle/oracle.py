@@ -127,6 +127,11 @@ def lib():
         "or_lm_fit": (C.c_int, [C.c_int, C.c_int, _dp, _dp, _dp, C.c_double, _dp, _dp, C.c_int,
                                 C.c_double, C.POINTER(C.c_double)]),
         "or_lm_model": (None, [C.c_int, C.c_int, _dp, _dp, _dp, _dp]),
+        "or_lm_fit_start": (C.c_int, [C.c_int, C.c_int, _dp, _dp, _dp, C.c_double, _dp, _dp,
+                                      C.c_int, C.c_double, _dp, C.POINTER(C.c_double)]),
+        "or_lm_fit_plain": (C.c_int, [C.c_int, C.c_int, _dp, _dp, _dp, C.c_double, _dp, C.c_int,
+                                      C.c_double, C.c_int, _dp, C.POINTER(C.c_double),
+                                      C.POINTER(C.c_int)]),
         "or_simulate": (None, [C.POINTER(_SimParams), _u8p, _u8p, _dp]),
         "or_mulberry32": (None, [C.c_uint32, _dp, C.c_int]),
         "or_rng_normals": (None, [C.c_uint32, _dp, C.c_int]),
@@ -531,3 +536,27 @@ def lm_model(tau, qn, theta):
     lib().or_lm_model(len(tau), len(qn), np.ascontiguousarray(tau, np.float64),
                       np.ascontiguousarray(qn, np.float64), np.ascontiguousarray(theta, np.float64), y)
     return y
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, np.float64)
+
+
+def lm_fit_start(d, tau, qn, w, bounds6, start4, max_iter=200, tol=1e-10):
+    """FP64 LM from (alpha, vbar, Z, D) with VarPro amplitudes -> (theta, cost, iters)."""
+    th = np.zeros(6)
+    cost = C.c_double()
+    it = lib().or_lm_fit_start(len(d), len(qn), _f64(d), _f64(tau), _f64(qn), float(w),
+                               _f64(bounds6), _f64(start4), max_iter, tol, th, C.byref(cost))
+    return th, cost.value, it
+
+
+def lm_fit_plain(d, tau, qn, w, bounds6, max_iter=200, tol=1e-10, nrefine=3):
+    """FP64 LM from the reference's start strategy -> (theta, cost, iters, evals)."""
+    th = np.zeros(6)
+    cost = C.c_double()
+    ev = C.c_int()
+    it = lib().or_lm_fit_plain(len(d), len(qn), _f64(d), _f64(tau), _f64(qn), float(w),
+                               _f64(bounds6), max_iter, tol, nrefine, th, C.byref(cost),
+                               C.byref(ev))
+    return th, cost.value, it, ev.value

@@ -42,13 +42,13 @@ struct ddm_engine {
   BinTable bins;
   float2 *d_hist = nullptr;            // [modes][T]
   float2 *d_rows = nullptr;            // [chunk][NHB][N][KB]
-  float *d_rowc = nullptr;             // [chunk][N] per-row reference levels
+  float *d_rowc = nullptr;             // [chunk] frame reference levels c_f
   double *d_framesum = nullptr;        // [chunk] pixel sums
   double *d_means = nullptr;           // [chunk]
   float *d_win = nullptr, *d_wys = nullptr;
   double *d_ninv = nullptr, *d_invtot = nullptr;
   float2 *d_tw_s = nullptr, *d_tw_t = nullptr;
-  float2 *d_wcorr4 = nullptr, *d_wcorr_full = nullptr;
+  float2 *d_wcorr4 = nullptr, *d_wcorr_full = nullptr;  // W(k), k < 4; FFT2(w m) [NH][N]
   uint8_t *d_smask = nullptr;
   void *d_stage[NSTAGE]{};             // device staging for host frames
   size_t stage_bytes = 0;
@@ -220,15 +220,21 @@ static int upload_mask_tables(ddm_engine *h, const uint8_t *mask) {
   std::vector<uint8_t> m01((size_t)N * N);
   for (size_t i = 0; i < m01.size(); i++) m01[i] = mask[i] ? 1 : 0;
   CK(cudaMemcpy(h->d_smask, m01.data(), m01.size(), cudaMemcpyHostToDevice));
-  // per-row window spectrum W_y(kx) = sum_x w(x) S(x,y) exp(-2 pi i kx x/N)
-  std::vector<float> wc(2 * (size_t)N * NH);
-  std::vector<cd> row(N);
+  // 2D spectrum of the masked window, W2(ky, kx) = FFT2(w(x) w(y) m(x, y)),
+  // FP64, stored kx-major as FP32 (the mean correction's table)
+  std::vector<std::vector<cd>> rs(N, std::vector<cd>(N));
   for (int y = 0; y < N; y++) {
-    for (int x = 0; x < N; x++) row[x] = cd(w[x] * m01[(size_t)y * N + x], 0);
-    host_fft(row, false);
-    for (int kx = 0; kx < NH; kx++) {
-      wc[2 * ((size_t)y * NH + kx)] = (float)row[kx].real();
-      wc[2 * ((size_t)y * NH + kx) + 1] = (float)row[kx].imag();
+    for (int x = 0; x < N; x++) rs[y][x] = cd(w[x] * w[y] * m01[(size_t)y * N + x], 0);
+    host_fft(rs[y], false);
+  }
+  std::vector<float> wc(2 * (size_t)N * NH);
+  std::vector<cd> col(N);
+  for (int kx = 0; kx < NH; kx++) {
+    for (int y = 0; y < N; y++) col[y] = rs[y][kx];
+    host_fft(col, false);
+    for (int ky = 0; ky < N; ky++) {
+      wc[2 * ((size_t)kx * N + ky)] = (float)col[ky].real();
+      wc[2 * ((size_t)kx * N + ky) + 1] = (float)col[ky].imag();
     }
   }
   CK(cudaMemcpy(h->d_wcorr_full, wc.data(), sizeof(float) * wc.size(), cudaMemcpyHostToDevice));
@@ -422,18 +428,18 @@ static int launch_chunk(ddm_engine *h, const void *dframes, int dtype, int n, co
   rp.smask = h->d_smask;
   rp.tw = h->d_tw_s;
   rp.rows = h->d_rows;
-  rp.rowc = h->d_rowc;
+  rp.framec = h->d_rowc;
   rp.framesum = h->d_framesum;
+  rp.err = h->d_err;
   CK(cudaMemsetAsync(h->d_framesum, 0, sizeof(double) * n, h->stream));
   CKL(launch_rows(N, dtype, rp, h->stream));
   ColParams cp{};
   cp.rows = h->d_rows;
-  cp.rowc = h->d_rowc;
+  cp.framec = h->d_rowc;
   cp.framesum = h->d_framesum;
   cp.inv_total = h->d_invtot;
-  cp.wys = h->d_wys;
-  cp.wcorr = h->d_smask ? h->d_wcorr_full : h->d_wcorr4;
-  cp.wcorr_full = h->d_smask ? 1 : 0;
+  cp.w2d = h->d_smask ? h->d_wcorr_full : nullptr;
+  cp.wc4 = h->d_wcorr4;
   for (int i = 0; i < n; i++) cp.slots[i] = slots[i] % h->g.T;
   cp.tw = h->d_tw_s;
   cp.hist = h->d_hist;
@@ -443,6 +449,7 @@ static int launch_chunk(ddm_engine *h, const void *dframes, int dtype, int n, co
   cp.T = h->g.T;
   cp.NH = h->NH;
   cp.NHB = h->NHB;
+  cp.err = h->d_err;
   CKL(launch_cols(N, cp, h->stream));
   h->last_mean_index = n - 1;
   h->have_frames = true;
@@ -488,6 +495,8 @@ static int ingest_impl(ddm_engine *h, const void *frames, int dtype, int n, cons
   cudaSetDevice(h->device);
   int rc = check_frames_args(h, frames, dtype, n, slots);
   if (rc) return rc;
+  if (device && ((uintptr_t)frames & 15))
+    return fail(h, DDM_ERR_ARG, "device frames must be 16-byte aligned (they are staged by bulk copies)");
   if ((rc = set_scale(h, scale))) return rc;
   const int N = h->g.N;
   const size_t fbytes = (size_t)N * N * dtype_size(dtype);
@@ -670,7 +679,8 @@ static int check_device_error(ddm_engine *h) {
   if (e) {
     CK(cudaMemset(h->d_err, 0, sizeof(int)));
     h->radial_valid = h->full_valid = false;
-    return fail(h, DDM_ERR_CUDA, "temporal kernel: a staged copy did not complete in time (code %d)", e);
+    return fail(h, DDM_ERR_CUDA,
+                "a staged copy did not complete in time (code %d: 1 temporal, 2 row, 3 column kernel)", e);
   }
   return DDM_OK;
 }

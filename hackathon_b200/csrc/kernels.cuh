@@ -12,32 +12,33 @@ constexpr int PFIELDS = 9;  // D + 8 drift sums per lag in a partial record
 constexpr int MAX_CHUNK = 64;  // frames per spatial launch (slots travel as a kernel parameter)
 
 struct RowParams {
-  const void* frames;      // [nframes][N][N] u8 / u16 / f32
+  const void* frames;      // [nframes][N][N] u8 / u16 / f32 (16-byte aligned)
   long long frame_stride;  // elements between frames
   int nframes;
   const float* win;        // w(x), FP32 (from the FP64 window)
   const float* wys;        // w(y) * scale
   const uint8_t* smask;    // spatial mask [N][N] or nullptr (extension)
-  const float2* tw;        // exp(-2 pi i j / N), j < N
+  const float2* tw;        // per-stage twiddle blocks of the N-point FFT
   float2* rows;            // [nframes][NHB][N][KB]
-  float* rowc;             // [nframes][N] per-row reference level c_y (raw units)
+  float* framec;           // [nframes] frame reference level c_f (raw units, out)
   double* framesum;        // [nframes] masked pixel sums (zeroed before launch)
+  int* err;                // error word (bounded waits that timed out), or nullptr
 };
 
 struct ColParams {
   const float2* rows;      // [nframes][NHB][N][KB]
-  const float* rowc;       // [nframes][N]
+  const float* framec;     // [nframes] c_f
   const double* framesum;  // [nframes]
   const double* inv_total; // [1] 1 / (valid pixels of the frame)
-  const float* wys;        // w(y) * scale
-  const float2* wcorr;     // [N][NH] window spectrum per row, or [4] (separable)
-  int wcorr_full;          // 1: wcorr is per row and per kx (spatial mask)
+  const float2* w2d;       // [NH][N] 2D spectrum of w(x) w(y) m(x,y) (kx-major), or nullptr
+  const float2* wc4;       // [4] window spectrum W(k), k = 0..3 (separable case)
   int slots[MAX_CHUNK];    // ring slot of each frame of the chunk
-  const float2* tw;        // exp(-2 pi i j / N)
+  const float2* tw;        // per-stage twiddle blocks of the N-point FFT
   float2* hist;            // [modes][T]
   double* means;           // [nframes] frame mean luma (out)
   float scale;
   int nframes, T, NH, NHB;
+  int* err;                // error word (bounded waits that timed out), or nullptr
 };
 
 struct TemporalParams {

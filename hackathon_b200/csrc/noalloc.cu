@@ -96,6 +96,7 @@ extern "C" int ddm_spectra_noalloc(const void* frames, int32_t dtype, int32_t n,
   if (n < 0 || T < 1) return nf_fail(DDM_ERR_ARG, "ddm_spectra_noalloc: need n >= 0 and T >= 1");
   if (n > 0 && (!frames || !slots || !hist)) return nf_fail(DDM_ERR_ARG, "ddm_spectra_noalloc: null pointer");
   if (!(scale > 0) || !std::isfinite(scale)) return nf_fail(DDM_ERR_ARG, "ddm_spectra_noalloc: scale must be > 0");
+  if ((uintptr_t)frames & 15) return nf_fail(DDM_ERR_ARG, "ddm_spectra_noalloc: frames must be 16-byte aligned");
   for (int i = 0; i < n; i++)
     if (slots[i] < 0) return nf_fail(DDM_ERR_ARG, "ddm_spectra_noalloc: slots must be >= 0");
   if (n == 0) return DDM_OK;
@@ -167,18 +168,18 @@ extern "C" int ddm_spectra_noalloc(const void* frames, int32_t dtype, int32_t n,
     rp.smask = nullptr;
     rp.tw = st.tw;
     rp.rows = st.rows;
-    rp.rowc = st.rowc;
+    rp.framec = st.rowc;
     rp.framesum = st.framesum;
+    rp.err = nullptr;  // bounded waits still end; there is no engine to report to
     if (launch_rows(N, dtype, rp, s) != cudaSuccess)
       return nf_fail(DDM_ERR_CUDA, "ddm_spectra_noalloc: row kernel launch failed");
     ColParams cp{};
     cp.rows = st.rows;
-    cp.rowc = st.rowc;
+    cp.framec = st.rowc;
     cp.framesum = st.framesum;
     cp.inv_total = st.invtot;
-    cp.wys = st.wys;
-    cp.wcorr = st.wcorr4;
-    cp.wcorr_full = 0;
+    cp.w2d = nullptr;
+    cp.wc4 = st.wcorr4;
     for (int i = 0; i < m; i++) cp.slots[i] = slots[c0 + i] % T;
     cp.tw = st.tw;
     cp.hist = (float2*)hist;
@@ -188,6 +189,7 @@ extern "C" int ddm_spectra_noalloc(const void* frames, int32_t dtype, int32_t n,
     cp.T = T;
     cp.NH = NH;
     cp.NHB = NHB;
+    cp.err = nullptr;
     if (launch_cols(N, cp, s) != cudaSuccess)
       return nf_fail(DDM_ERR_CUDA, "ddm_spectra_noalloc: column kernel launch failed");
   }

@@ -6,30 +6,30 @@
 // hist[m*T + slot].
 //
 // B200 formulation, two kernels per chunk of frames:
-//  rows_kernel  reads raw u8/u16/f32 pixels (convert and luma scale fused
-//               into the load) and transforms two rows per complex FFT
-//               (real-input packing) after subtracting a per-row reference
-//               level c_y (the mean of four pixels of the row, exact in FP32
-//               for integer frames). It writes the row spectra to an
-//               L2-resident scratch in a [frame][kx/2][y][2] blocked layout
-//               (full 32 B sectors), c_y, and one FP64 atomic per CTA into
-//               the frame's pixel sum.
-//  cols_kernel  restores the exact frame mean by linearity:
-//                 FFT_x((I - mu) w) = FFT_x((I - c_y) w) + (c_y - mu) W(kx),
-//               W the window's DFT (non-zero only at kx <= 3 for the 4-term
-//               Blackman-Harris; a per-row table when a spatial ROI mask is
-//               set), computed in FP64. One FFT group per frame reads its
-//               column pair straight into registers (one float4 per row),
-//               runs the column FFTs, scales by 1/N, and the CTA stores the
-//               FG frames of a mode together: FG consecutive ring slots form
-//               one 32 B sector.
-// Subtracting c_y keeps the FP32 row transform free of the large DC term
-// (the cancellation the reference avoids with its (hi, lo) mean,
-// ddm.wgsl:129-150); the correction term is the small (c_y - mu) and is
-// formed in FP64.
+//  rows_kernel  stages batches of raw u8/u16/f32 rows (and the spatial mask's
+//               rows) into shared memory with bulk copies, converts, subtracts
+//               a frame reference level c_f (mean of four fixed pixels of the
+//               frame, exact in FP32 for integer frames), multiplies by
+//               w(x) w(y) scale m(x,y), and transforms two rows per complex
+//               FFT (real-input packing). It writes the row spectra to an
+//               L2-resident scratch in a [frame][kx/2][y][2] blocked layout,
+//               c_f, and one FP64 atomic per CTA into the frame's pixel sum.
+//  cols_kernel  stages a tile (column pair, G frames) of row spectra with bulk
+//               copies, runs the column FFTs and restores the exact frame mean
+//               by linearity on the way out:
+//                 FFT2((I - mu) w m) = FFT2((I - c_f) w m) + (c_f - mu) FFT2(w m),
+//               FFT2(w m) a host FP64 table (non-zero only at kx <= 3 and
+//               |ky| <= 3 for the separable 4-term Blackman-Harris window
+//               without a mask), the coefficient c_f - mu in FP64. The CTA
+//               stores the G frames of a mode together: G consecutive ring
+//               slots form one 32 B sector.
+// Subtracting c_f keeps the FP32 transforms free of the large DC term (the
+// cancellation the reference avoids with its (hi, lo) mean,
+// ddm.wgsl:129-150); the correction term is the small (c_f - mu).
 #include <cstdint>
 #include <type_traits>
 
+#include "async_copy.cuh"
 #include "fft_block.cuh"
 #include "kernels.cuh"
 
@@ -40,192 +40,224 @@ __device__ __forceinline__ float ld_pix(const Tin* p) {
   return (float)__ldg(p);
 }
 
-// Pixels of one row pair (8 per thread per row, FFT input pattern) and the
-// rows' reference levels, loaded one iteration ahead of their use.
-template <int N, typename Tin>
-struct RowInput {
-  float a0[8], a1[8];
-  float c0, c1;
-  __device__ __forceinline__ void load(const RowParams& p, long long pair, int t) {
-    constexpr int NT = N / 8;
-    const bool valid = pair < (long long)p.nframes * (N / 2);
-    const int f = valid ? (int)(pair / (N / 2)) : 0;
-    const int y0 = valid ? 2 * (int)(pair % (N / 2)) : 0;
-    const Tin* r0 = (const Tin*)p.frames + (size_t)f * p.frame_stride + (size_t)y0 * N;
-    const Tin* r1 = r0 + N;
-    c0 = c1 = 0.f;
-    if (valid) {
-      // per-row reference level: mean of four pixels (broadcast loads)
-      c0 = 0.25f * ((ld_pix(r0) + ld_pix(r0 + N / 4)) + (ld_pix(r0 + N / 2) + ld_pix(r0 + 3 * N / 4)));
-      c1 = 0.25f * ((ld_pix(r1) + ld_pix(r1 + N / 4)) + (ld_pix(r1 + N / 2) + ld_pix(r1 + 3 * N / 4)));
-    }
-#pragma unroll
-    for (int q = 0; q < 8; q++) {
-      a0[q] = valid ? ld_pix(r0 + t + q * NT) : 0.f;
-      a1[q] = valid ? ld_pix(r1 + t + q * NT) : 0.f;
-    }
-  }
-};
+template <int N>
+__host__ __device__ constexpr int row_groups() {
+  return 256 / (N / 8) >= 1 ? 256 / (N / 8) : 1;
+}
+constexpr int ROW_STAGES = 2;  // depth of the row-batch staging ring
 
-// Persistent: each CTA walks batches of G row pairs (one frame per batch),
-// prefetching the next batch's pixels while it transforms the current one.
+// The pixels whose mean is a frame's reference level c_f.
+template <int N>
+__device__ __forceinline__ int cref_offset(int i) {
+  return (N / 4 + (i >> 1) * (N / 2)) * N + N / 4 + (i & 1) * (N / 2);
+}
+
+// Persistent: each CTA walks batches of G row pairs (2G consecutive rows of
+// one frame; G divides N/2, so a batch never straddles frames). A batch (and
+// the mask's matching rows) is staged into shared memory by bulk copies (TMA,
+// cp.async.bulk) issued ROW_STAGES batches ahead into a ring, so raw pixels
+// never sit in registers waiting and the copy engine, not the warps, moves
+// them.
 template <int N, typename Tin>
 __global__ void __launch_bounds__(256) rows_kernel(RowParams p) {
   constexpr int NT = N / 8;
-  constexpr int G = 256 / NT >= 1 ? 256 / NT : 1;
+  constexpr int G = row_groups<N>();
   constexpr int PN = padded(N);
   constexpr int NHB = (N / 2 + 1 + KB - 1) / KB;
   constexpr int WARPS = (G * NT + 31) / 32;
   constexpr int SYNC = sync_kind(N, G);
-  extern __shared__ float2 sm[];
+  constexpr int BPF = N / (2 * G);  // batches per frame
+  constexpr uint32_t BATCH_ELEMS = 2u * G * N;
+  constexpr uint32_t BATCH_BYTES = BATCH_ELEMS * sizeof(Tin);
+  static_assert(BATCH_BYTES % 16 == 0 && BATCH_ELEMS % 16 == 0, "bulk copies move multiples of 16 bytes");
+  extern __shared__ __align__(16) float2 sm[];
   __shared__ double red[WARPS];
+  __shared__ __align__(8) uint64_t bar[ROW_STAGES];
   const int g = threadIdx.x / NT, t = threadIdx.x % NT;
   float2* buf0 = sm + (size_t)g * 2 * PN;
   float2* buf1 = buf0 + PN;
   float2* s_tw = sm + (size_t)G * 2 * PN;
+  float* s_wy = (float*)(s_tw + tw_size(N));                     // [N] w(y) scale
+  Tin* ring = (Tin*)(s_wy + N);                                   // [ROW_STAGES][2G][N]
+  uint8_t* mring = (uint8_t*)(ring + ROW_STAGES * BATCH_ELEMS);  // [ROW_STAGES][2G][N]
   for (int i = threadIdx.x; i < tw_size(N); i += blockDim.x) s_tw[i] = p.tw[i];
-  const long long npairs = (long long)p.nframes * (N / 2);
-  const long long nbatch = (npairs + G - 1) / G;
+  for (int i = threadIdx.x; i < N; i += blockDim.x) s_wy[i] = p.wys[i];
+  const long long nbatch = (long long)p.nframes * BPF;
+  const Tin* frames = (const Tin*)p.frames;
+  const bool masked = p.smask != nullptr;
+  auto issue = [&](long long b, int st) {
+    const long long f = b / BPF, r = b % BPF;
+    mbar_arrive_expect_tx(&bar[st], BATCH_BYTES + (masked ? BATCH_ELEMS : 0u));
+    bulk_g2s(ring + st * BATCH_ELEMS, frames + f * p.frame_stride + r * (long long)BATCH_ELEMS, BATCH_BYTES,
+             &bar[st]);
+    if (masked) bulk_g2s(mring + st * BATCH_ELEMS, p.smask + r * BATCH_ELEMS, BATCH_ELEMS, &bar[st]);
+  };
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < ROW_STAGES; s++) mbar_init(&bar[s], 1);
+    fence_barrier_init();
+    for (int s = 0; s < ROW_STAGES; s++) {
+      const long long b = blockIdx.x + (long long)s * gridDim.x;
+      if (b < nbatch) issue(b, s);
+    }
+  }
+  float wxs[8];  // w(x) at this thread's columns, fixed for the whole kernel
+#pragma unroll
+  for (int q = 0; q < 8; q++) wxs[q] = __ldg(&p.win[t + q * NT]);
+  // reference pixels of the first batch's frame (raw loads, used next iteration)
+  float cpx[4];
+  {
+    const long long f = blockIdx.x < nbatch ? blockIdx.x / BPF : 0;
+#pragma unroll
+    for (int i = 0; i < 4; i++) cpx[i] = ld_pix(frames + f * p.frame_stride + cref_offset<N>(i));
+  }
   // pixel sums: exact integers for u8/u16 (warp totals < 2^31), FP64 for f32
   constexpr bool INT = !std::is_floating_point<Tin>::value;
   using acc_t = typename std::conditional<INT, int, double>::type;
-  RowInput<N, Tin> cur, nxt;
-  long long b = blockIdx.x;
-  cur.load(p, b * G + g, t);
   __syncthreads();
-  for (; b < nbatch; b += gridDim.x) {
-    if (b + gridDim.x < nbatch) nxt.load(p, (b + gridDim.x) * G + g, t);
-    const long long pair = b * G + g;
-    const bool valid = pair < npairs;
-    const int f = (int)((b * G) / (N / 2));  // all G pairs of a batch share the frame
-    const int y0 = valid ? 2 * (int)(pair % (N / 2)) : 0;
-    const uint8_t* m0p = p.smask ? p.smask + (size_t)y0 * N : nullptr;
-    const float wy0 = p.wys[y0], wy1 = p.wys[y0 + 1];
+  int it = 0;
+  for (long long b = blockIdx.x; b < nbatch; b += gridDim.x, it++) {
+    const int st = it % ROW_STAGES;
+    const int f = (int)(b / BPF);
+    const int r = (int)(b % BPF);
+    const float cf = 0.25f * ((cpx[0] + cpx[1]) + (cpx[2] + cpx[3]));
+    {  // next batch's reference pixels
+      const long long bn = b + gridDim.x;
+      const long long fn = bn < nbatch ? bn / BPF : f;
+#pragma unroll
+      for (int i = 0; i < 4; i++) cpx[i] = ld_pix(frames + fn * p.frame_stride + cref_offset<N>(i));
+    }
+    if (!mbar_wait(&bar[st], (uint32_t)(it / ROW_STAGES) & 1u, p.err, 2)) {
+      // give up: let this CTA's other copies in flight land (bounded), then stop
+      if (threadIdx.x == 0)
+        for (int k = 1; k < ROW_STAGES; k++)
+          if (b + (long long)k * gridDim.x < nbatch)
+            mbar_wait(&bar[(it + k) % ROW_STAGES], (uint32_t)((it + k) / ROW_STAGES) & 1u, nullptr, 0);
+      return;
+    }
+    const int y0 = r * 2 * G + 2 * g;
+    const Tin* r0 = ring + st * BATCH_ELEMS + 2 * g * N;
+    const Tin* r1 = r0 + N;
+    const uint8_t* m0p = mring + st * BATCH_ELEMS + 2 * g * N;
+    const float wy0 = s_wy[y0], wy1 = s_wy[y0 + 1];
     float2 v[8];
     acc_t s = 0;
 #pragma unroll
     for (int q = 0; q < 8; q++) {
       const int x = t + q * NT;
-      float m0 = 1.f, m1 = 1.f;
-      if (m0p) {
-        m0 = (float)m0p[x];
-        m1 = (float)m0p[N + x];
-      }
-      const float a0 = cur.a0[q] * m0, a1 = cur.a1[q] * m1;
+      const float m0 = masked ? (float)m0p[x] : 1.f;
+      const float m1 = masked ? (float)m0p[N + x] : 1.f;
+      const float a0 = (float)r0[x] * m0, a1 = (float)r1[x] * m1;
       if constexpr (INT)
         s += (int)a0 + (int)a1;
       else
         s += (double)a0 + (double)a1;
-      const float wx = __ldg(&p.win[x]);
-      v[q] = make_float2((cur.a0[q] - cur.c0) * (wx * m0 * wy0), (cur.a1[q] - cur.c1) * (wx * m1 * wy1));
+      const float wx = wxs[q];
+      v[q] = make_float2((a0 - cf * m0) * (wx * wy0), (a1 - cf * m1) * (wx * wy1));
     }
+    fence_proxy_async_smem();  // this thread's reads of the stage before the next bulk write
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = (double)s;
     const float2* Z = fft<N, false, true, SYNC>(v, t, buf0, buf1, s_tw, 1 + g);
-    __syncthreads();  // red[] complete; every group done with its buffers' reads below
+    __syncthreads();  // red[] complete; every thread is done with stage st
     if (threadIdx.x == 0) {
+      const long long bn = b + (long long)ROW_STAGES * gridDim.x;
+      if (bn < nbatch) issue(bn, st);
       double tot = 0.0;
 #pragma unroll
       for (int w = 0; w < WARPS; w++) tot += red[w];
       atomicAdd(&p.framesum[f], tot);
+      if (r == 0) p.framec[f] = cf;
     }
-    if (valid) {
-      float2* out = p.rows + (size_t)f * NHB * N * KB;
-      for (int kx = t; kx <= N / 2; kx += NT) {
-        const float2 zk = Z[pad(kx)];
-        const float2 zn = Z[pad((N - kx) & (N - 1))];
-        const float2 R0 = make_float2(0.5f * (zk.x + zn.x), 0.5f * (zk.y - zn.y));
-        const float2 R1 = make_float2(0.5f * (zk.y + zn.y), -0.5f * (zk.x - zn.x));
-        float2* o = out + ((size_t)(kx / KB) * N + y0) * KB + (kx % KB);
-        o[0] = R0;
-        o[KB] = R1;
-      }
-      if (t == 0) {
-        p.rowc[(size_t)f * N + y0] = cur.c0;
-        p.rowc[(size_t)f * N + y0 + 1] = cur.c1;
-      }
+    float2* out = p.rows + (size_t)f * NHB * N * KB;
+    for (int kx = t; kx <= N / 2; kx += NT) {
+      const float2 zk = Z[pad(kx)];
+      const float2 zn = Z[pad((N - kx) & (N - 1))];
+      const float2 R0 = make_float2(0.5f * (zk.x + zn.x), 0.5f * (zk.y - zn.y));
+      const float2 R1 = make_float2(0.5f * (zk.y + zn.y), -0.5f * (zk.x - zn.x));
+      float2* o = out + ((size_t)(kx / KB) * N + y0) * KB + (kx % KB);
+      o[0] = R0;
+      o[KB] = R1;
     }
-    cur = nxt;
     __syncthreads();  // buffers and red[] are reused by the next batch
   }
 }
 
-// Inputs of one column-pair tile for this thread's group: both columns at the
-// group's 8 rows (one float4 per row) and the correction coefficients.
+// Persistent: each CTA walks tiles (column pair kb, group of G frames). The
+// tile's G row-spectrum blocks ([y][KB] float2, contiguous per frame) are
+// staged into shared memory by bulk copies; the next tile's copies are
+// issued as soon as every thread has read the current one, so they overlap
+// the second column's transform and the history stores. Group g transforms
+// frame f0 + g; the CTA then writes frame sf = tid % G of each mode, so G
+// consecutive ring slots of a mode leave together (one 32 B sector at G = 4),
+// adding the mean correction (c_f - mu) FFT2(w m)(ky, kx) on the way.
 template <int N>
-struct ColInput {
-  float4 col[8];
-  float dy[8];
-  __device__ __forceinline__ void load(const ColParams& p, int kb, int f, bool fvalid, int t) {
-    constexpr int NT = N / 8;
-    const double mu = fvalid ? p.framesum[f] * p.inv_total[0] : 0.0;
-    const float4* src = (const float4*)(p.rows + ((size_t)f * p.NHB + kb) * N * KB);
-#pragma unroll
-    for (int q = 0; q < 8; q++) {
-      const int y = t + q * NT;
-      col[q] = fvalid ? __ldg(&src[y]) : make_float4(0.f, 0.f, 0.f, 0.f);
-      dy[q] = fvalid ? (float)(((double)p.rowc[(size_t)f * N + y] - mu) * (double)p.wys[y]) : 0.f;
-    }
-  }
-};
-
-// Persistent: each CTA walks tiles (column pair kb, group of G frames) and
-// prefetches the next tile's inputs while it transforms the current one.
-template <int N>
-__global__ void __launch_bounds__(256, 2) cols_kernel(ColParams p) {
+__global__ void __launch_bounds__(256) cols_kernel(ColParams p) {
   constexpr int NT = N / 8;
-  constexpr int G = 256 / NT >= 1 ? 256 / NT : 1;  // frames per tile, one per group
+  constexpr int G = row_groups<N>();  // frames per tile, one per group
   constexpr int PN = padded(N);
   constexpr int SYNC = sync_kind(N, G);
-  extern __shared__ float2 sm[];
+  constexpr uint32_t FRAME_ELEMS = N * KB;  // float2 of one frame's block
+  constexpr uint32_t FRAME_BYTES = FRAME_ELEMS * sizeof(float2);
+  extern __shared__ __align__(16) float2 sm[];
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ float s_dc[G];  // (c_f - mu) scale / N per frame of the tile
   const int g = threadIdx.x / NT, t = threadIdx.x % NT;
   float2* buf0 = sm + (size_t)g * 2 * PN;
   float2* buf1 = buf0 + PN;
   float2* s_tw = sm + (size_t)G * 2 * PN;
+  float2* stage = s_tw + tw_size(N);  // [G][N][KB]
   for (int i = threadIdx.x; i < tw_size(N); i += blockDim.x) s_tw[i] = p.tw[i];
   const int nfg = (p.nframes + G - 1) / G;
   const int ntiles = p.NHB * nfg;
   const float invN = 1.f / N;
   const int sf = threadIdx.x % G;  // frame of the tile this thread stores
-  ColInput<N> cur, nxt;
-  int tile = blockIdx.x;
-  {
+  const double inv_total = p.inv_total[0];
+  auto issue = [&](int tile) {
     const int kb = tile % p.NHB, f0 = (tile / p.NHB) * G;
-    cur.load(p, kb, f0 + g, tile < ntiles && f0 + g < p.nframes, t);
+    const int nf = min(G, p.nframes - f0);
+    mbar_arrive_expect_tx(&bar, nf * FRAME_BYTES);
+    for (int i = 0; i < nf; i++)
+      bulk_g2s(stage + i * FRAME_ELEMS, p.rows + ((size_t)(f0 + i) * p.NHB + kb) * FRAME_ELEMS, FRAME_BYTES,
+               &bar);
+  };
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    fence_barrier_init();
+    if (blockIdx.x < ntiles) issue(blockIdx.x);
   }
   __syncthreads();
-  for (; tile < ntiles; tile += gridDim.x) {
+  uint32_t phase = 0;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int kb = tile % p.NHB;
     const int f0 = (tile / p.NHB) * G;
     const int nf = min(G, p.nframes - f0);
-    {
-      const int tn = tile + gridDim.x;
-      const int kbn = tn % p.NHB, f0n = (tn / p.NHB) * G;
-      if (tn < ntiles) nxt.load(p, kbn, f0n + g, f0n + g < p.nframes, t);
+    if (threadIdx.x < nf) {
+      const int f = f0 + threadIdx.x;
+      const double mu = p.framesum[f] * inv_total;
+      s_dc[threadIdx.x] = (float)(((double)p.framec[f] - mu) * (double)p.scale / N);
+      if (kb == 0) p.means[f] = mu * (double)p.scale;
     }
-    if (kb == 0 && t == 0 && g < nf) p.means[f0 + g] = p.framesum[f0 + g] * p.inv_total[0] * (double)p.scale;
+    if (!mbar_wait(&bar, phase, p.err, 3)) return;  // nothing else is in flight
+    phase ^= 1u;
     const int slot = sf < nf ? p.slots[f0 + sf] : 0;
+    const bool fvalid = g < nf;
+    const float2* blk = stage + g * FRAME_ELEMS;
 #pragma unroll 1
     for (int c = 0; c < KB; c++) {
       const int kx = kb * KB + c;
       if (kx >= p.NH) break;  // uniform over the CTA
       float2 v[8];
-      const bool sep = !p.wcorr_full && kx < 4;
-      const float2 wc = sep ? p.wcorr[kx] : make_float2(0.f, 0.f);
 #pragma unroll
-      for (int q = 0; q < 8; q++) {
-        float2 a = c == 0 ? make_float2(cur.col[q].x, cur.col[q].y) : make_float2(cur.col[q].z, cur.col[q].w);
-        float2 w = wc;
-        if (p.wcorr_full) w = p.wcorr[(size_t)(t + q * NT) * p.NH + kx];
-        if (sep || p.wcorr_full) {
-          a.x = fmaf(cur.dy[q], w.x, a.x);
-          a.y = fmaf(cur.dy[q], w.y, a.y);
-        }
-        v[q] = a;
+      for (int q = 0; q < 8; q++) v[q] = fvalid ? blk[(t + q * NT) * KB + c] : make_float2(0.f, 0.f);
+      if (c == KB - 1 || kx + 1 >= p.NH) {
+        // every thread has read the stage: the next tile's copies may land
+        fence_proxy_async_smem();
+        __syncthreads();
+        if (threadIdx.x == 0 && tile + (int)gridDim.x < ntiles) issue(tile + gridDim.x);
       }
       const float2* Y = fft<N, false, true, SYNC>(v, t, buf0, buf1, s_tw, 1 + g);
-      __syncthreads();  // every group's column is in shared memory
+      __syncthreads();  // every group's column (and s_dc) is in shared memory
       // Y of group g sits at the same offset in every group's buffer pair; the
       // CTA writes frame sf = tid % G of each mode: G consecutive ring slots
       if (sf < nf) {
@@ -233,14 +265,23 @@ __global__ void __launch_bounds__(256, 2) cols_kernel(ColParams p) {
         const float2* ys = sm + (size_t)sf * 2 * PN + yoff;
         float2* hs = p.hist + (size_t)kx * p.T + slot;
         const size_t mstride = (size_t)p.NH * p.T;
+        const float dc = s_dc[sf];
+        const float2 wkx = kx < 4 ? p.wc4[kx] : make_float2(0.f, 0.f);
         for (int ky = threadIdx.x / G; ky < N; ky += 256 / G) {
           const float2 y = ys[pad(ky)];
-          hs[(size_t)ky * mstride] = make_float2(y.x * invN, y.y * invN);
+          float2 w = make_float2(0.f, 0.f);
+          if (p.w2d) {
+            w = __ldg(&p.w2d[(size_t)kx * N + ky]);
+          } else if (kx < 4 && (ky < 4 || ky > N - 4)) {
+            // separable window: W(kx) W(ky), W(N - k) = conj W(k)
+            const float2 wk = ky < 4 ? p.wc4[ky] : make_float2(p.wc4[N - ky].x, -p.wc4[N - ky].y);
+            w = cmul(wkx, wk);
+          }
+          hs[(size_t)ky * mstride] = make_float2(fmaf(dc, w.x, y.x * invN), fmaf(dc, w.y, y.y * invN));
         }
       }
       __syncthreads();
     }
-    cur = nxt;
   }
 }
 
@@ -271,7 +312,7 @@ static cudaError_t rows_n(const RowParams& p, cudaStream_t s) {
   constexpr int G = groups<N>();
   const long long npairs = (long long)p.nframes * (N / 2);
   auto k = rows_kernel<N, Tin>;
-  const size_t sm = fft_smem<N>();
+  const size_t sm = fft_smem<N>() + N * sizeof(float) + (size_t)ROW_STAGES * 2 * G * N * (sizeof(Tin) + 1);
   cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   const int grid = persistent_grid(k, G * (N / 8), sm, (npairs + G - 1) / G);
   k<<<grid, G * (N / 8), sm, s>>>(p);
@@ -304,7 +345,7 @@ template <int N>
 static cudaError_t cols_n(const ColParams& p, cudaStream_t s) {
   constexpr int G = groups<N>();
   auto k = cols_kernel<N>;
-  const size_t sm = fft_smem<N>();
+  const size_t sm = fft_smem<N>() + (size_t)G * N * KB * sizeof(float2);
   cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   const int grid = persistent_grid(k, G * (N / 8), sm, (long long)p.NHB * ((p.nframes + G - 1) / G));
   k<<<grid, G * (N / 8), sm, s>>>(p);

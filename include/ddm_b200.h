@@ -97,8 +97,9 @@ int ddm_ingest_luma(ddm_engine *h, const float *luma, int32_t slot,
  * been copied off the caller's buffer. */
 int ddm_ingest_frames(ddm_engine *h, const void *frames, int32_t dtype,
                       int32_t n, const int32_t *slots, float scale);
-/* Same, with `frames` already in device memory (cudaMalloc / torch). Work is
- * queued on the engine's stream; the buffer must stay valid until it runs. */
+/* Same, with `frames` already in device memory (cudaMalloc / torch; 16-byte
+ * aligned, else DDM_ERR_ARG). Work is queued on the engine's stream; the
+ * buffer must stay valid until it runs. */
 int ddm_ingest_frames_device(ddm_engine *h, const void *frames, int32_t dtype,
                              int32_t n, const int32_t *slots, float scale);
 
@@ -181,7 +182,7 @@ int ddm_fit_lm(int32_t nfit, int32_t nt_max, int32_t K, const int32_t *nt, const
  * loop that must not enter cudaMalloc, which can stall on device-wide
  * synchronisation. Needs no engine.
  *
- * Transforms n frames (DEVICE memory, N*N pixels of `dtype` each, luma =
+ * Transforms n frames (DEVICE memory, 16-byte aligned, N*N pixels of `dtype` each, luma =
  * value * scale) exactly as ddm_ingest_frames_device does and writes frame i
  * into ring slot slots[i] % T of the caller's DEVICE history `hist`
  * (float2 [N*(N/2+1)][T], the readHistory layout), on `stream`

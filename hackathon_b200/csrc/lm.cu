@@ -33,26 +33,39 @@ constexpr int LM_MAX_LAGS = 128;   // 4 per lane
 constexpr int LM_MAX_NODES = 8;
 constexpr int LM_WARPS = 8;        // fits per 256-thread CTA
 
-// g(x; Z) and its log-derivatives x dg/dx, Z dg/dZ (FP32).
-__device__ __forceinline__ void isf3d_d(float x, float Z, float& g, float& gx, float& gz) {
-  const float Z1 = Z + 1.f;
-  const float L = x / Z1;
-  if (L < 1e-4f) {
-    const float x2 = x * x;
-    g = 1.f - x2 * (Z + 2.f) / (6.f * Z1);
-    gx = -2.f * x2 * (Z + 2.f) / (6.f * Z1);
-    gz = x2 * Z / (6.f * Z1 * Z1);
+// Precision-generic math for the model: FP32 for the bulk of the
+// iterations, FP64 for the final refinement.
+__device__ __forceinline__ float m_atan(float x) { return atanf(x); }
+__device__ __forceinline__ double m_atan(double x) { return atan(x); }
+__device__ __forceinline__ float m_log1p(float x) { return log1pf(x); }
+__device__ __forceinline__ double m_log1p(double x) { return log1p(x); }
+__device__ __forceinline__ float m_exp(float x) { return expf(x); }
+__device__ __forceinline__ double m_exp(double x) { return exp(x); }
+__device__ __forceinline__ void m_sincos(float x, float* s, float* c) { sincosf(x, s, c); }
+__device__ __forceinline__ void m_sincos(double x, double* s, double* c) { sincos(x, s, c); }
+
+// g(x; Z) (isf3d, motility_fit.js:140-144) and its log-derivatives
+// x dg/dx, Z dg/dZ.
+template <typename R>
+__device__ __forceinline__ void isf3d_d(R x, R Z, R& g, R& gx, R& gz) {
+  const R Z1 = Z + R(1);
+  const R L = x / Z1;
+  if (L < R(1e-4)) {
+    const R x2 = x * x;
+    g = R(1) - x2 * (Z + R(2)) / (R(6) * Z1);
+    gx = R(-2) * x2 * (Z + R(2)) / (R(6) * Z1);
+    gz = x2 * Z / (R(6) * Z1 * Z1);
     return;
   }
-  const float a = atanf(L), u = 1.f + L * L, lu = log1pf(L * L);
-  const float U = expf(0.5f * Z * lu);
-  float s, c;
-  sincosf(Z * a, &s, &c);
-  const float G = s / (Z * L * U);
-  const float LgL = c / (u * U) - G * (1.f + Z * L * L / u);
+  const R a = m_atan(L), u = R(1) + L * L, lu = m_log1p(L * L);
+  const R U = m_exp(R(0.5) * Z * lu);
+  R s, c;
+  m_sincos(Z * a, &s, &c);
+  const R G = s / (Z * L * U);
+  const R LgL = c / (u * U) - G * (R(1) + Z * L * L / u);
   g = G;
   gx = LgL;
-  gz = a * c / (L * U) - G - 0.5f * Z * G * lu - (Z / Z1) * LgL;
+  gz = a * c / (L * U) - G - R(0.5) * Z * G * lu - (Z / Z1) * LgL;
 }
 
 struct LmProblem {
@@ -143,41 +156,44 @@ __device__ __forceinline__ double varpro(const LmProblem& P, int lane, double al
 }
 
 // Normal equations at theta: H (upper triangle, 21), g (6), cost; warp-reduced.
+// The model and Jacobian are evaluated in R; the sums are FP64.
+template <typename R>
 __device__ __forceinline__ void lm_normal(const LmProblem& P, const double (&th)[LM_NP], int lane,
                                           double (&H)[21], double (&gr)[LM_NP], double& cost) {
-  const float A = (float)th[0], B = (float)th[1], al = (float)th[2];
-  const float v = (float)exp(th[3]), Z = (float)exp(th[4]), D = (float)exp(th[5]);
+  const R A = (R)th[0], B = (R)th[1], al = (R)th[2];
+  const R v = (R)exp(th[3]), Z = (R)exp(th[4]), D = (R)exp(th[5]);
   for (int i = 0; i < 21; i++) H[i] = 0.0;
   for (int i = 0; i < LM_NP; i++) gr[i] = 0.0;
   cost = 0.0;
-  const float iK = 1.f / P.K;
+  const R iK = R(1) / R(P.K);
+  const R w = (R)P.w;
 #pragma unroll
   for (int r = 0; r < 4; r++) {
     const int j = lane + 32 * r;
     if (j >= P.nt) break;
-    const float t = P.tau[r];
-    float sE = 0.f, sEg = 0.f, sdD = 0.f, sgx = 0.f, sgz = 0.f;
+    const R t = (R)P.tau[r];
+    R sE = 0, sEg = 0, sdD = 0, sgx = 0, sgz = 0;
     for (int n = 0; n < P.K; n++) {
-      const float q = P.qn[n];
-      const float E = expf(-D * q * q * t);
-      float g, gx, gz;
-      isf3d_d(q * v * t, Z, g, gx, gz);
-      const float mix = 1.f - al + al * g;
+      const R q = (R)P.qn[n];
+      const R E = m_exp(-D * q * q * t);
+      R g, gx, gz;
+      isf3d_d<R>(q * v * t, Z, g, gx, gz);
+      const R mix = R(1) - al + al * g;
       sE += E * mix;
-      sEg += E * (g - 1.f);
+      sEg += E * (g - R(1));
       sdD += E * D * q * q * t * mix;
       sgx += E * al * gx;
       sgz += E * al * gz;
     }
-    const float c = 1.f - sE * iK;
-    const double rr = (double)P.w * ((double)A * c + (double)B - (double)P.d[r]);
+    const R c = R(1) - sE * iK;
+    const double rr = (double)w * ((double)A * (double)c + (double)B - (double)P.d[r]);
     double J[LM_NP];
-    J[0] = (double)P.w * c;
-    J[1] = (double)P.w;
-    J[2] = (double)(-P.w * A * sEg * iK);
-    J[3] = (double)(-P.w * A * sgx * iK);
-    J[4] = (double)(-P.w * A * sgz * iK);
-    J[5] = (double)(P.w * A * sdD * iK);
+    J[0] = (double)(w * c);
+    J[1] = (double)w;
+    J[2] = (double)(-w * A * sEg * iK);
+    J[3] = (double)(-w * A * sgx * iK);
+    J[4] = (double)(-w * A * sgz * iK);
+    J[5] = (double)(w * A * sdD * iK);
     cost += rr * rr;
     int k = 0;
 #pragma unroll
@@ -239,12 +255,13 @@ __device__ __forceinline__ bool lm_solve(const double (&H)[21], const double (&g
   return true;
 }
 
-// Marquardt iteration from th (projected, amplitudes set); returns iterations.
-__device__ int lm_run(const LmProblem& P, int lane, double (&th)[LM_NP], double& cost, int max_iter,
-                      double tol) {
+// Marquardt iterations with the model in R from th (projected, amplitudes
+// set), continuing from lambda; returns the iterations taken.
+template <typename R>
+__device__ int lm_phase(const LmProblem& P, int lane, double (&th)[LM_NP], double& cost, double& lambda,
+                        int max_iter, double tol) {
   double H[21], gr[LM_NP];
-  lm_normal(P, th, lane, H, gr, cost);
-  double lambda = 1e-3;
+  lm_normal<R>(P, th, lane, H, gr, cost);
   int small = 0, it = 0;
   for (it = 0; it < max_iter; it++) {
     double delta[LM_NP];
@@ -257,7 +274,7 @@ __device__ int lm_run(const LmProblem& P, int lane, double (&th)[LM_NP], double&
 #pragma unroll
     for (int a = 0; a < LM_NP; a++) th2[a] = fmin(P.hi[a], fmax(P.lo[a], th[a] + delta[a]));
     double H2[21], g2[LM_NP], c2;
-    lm_normal(P, th2, lane, H2, g2, c2);
+    lm_normal<R>(P, th2, lane, H2, g2, c2);
     if (c2 < cost) {
       const double rel = (cost - c2) / (cost > 0 ? cost : 1e-300);
 #pragma unroll
@@ -280,6 +297,21 @@ __device__ int lm_run(const LmProblem& P, int lane, double (&th)[LM_NP], double&
     }
   }
   return it;
+}
+
+// Marquardt's method (the iteration of oracle/lm.c): FP32 model until the
+// FP32 cost stops resolving progress, then FP64 model iterations from there
+// (the FP32 cost carries ~1e-7 relative noise, which would otherwise stop
+// the walk early along flat valleys). Returns the iterations taken.
+__device__ int lm_run(const LmProblem& P, int lane, double (&th)[LM_NP], double& cost, int max_iter,
+                      double tol) {
+  double lambda = 1e-3;
+  const int it32 = lm_phase<float>(P, lane, th, cost, lambda, max_iter, tol);
+  // the FP32 phase often ends on a run of rejected steps (lambda > 1e12)
+  // that only the FP32 noise caused: restart the damping
+  lambda = 1e-3;
+  const int it64 = lm_phase<double>(P, lane, th, cost, lambda, max_iter - it32 > 8 ? max_iter - it32 : 8, tol);
+  return it32 + it64;
 }
 
 __global__ void __launch_bounds__(32 * LM_WARPS) lm_kernel(LmParams p) {

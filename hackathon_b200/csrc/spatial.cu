@@ -27,7 +27,10 @@
 // cancellation the reference avoids with its (hi, lo) mean,
 // ddm.wgsl:129-150); the correction term is the small (c_f - mu).
 #include <cstdint>
+#include <map>
+#include <mutex>
 #include <type_traits>
+#include <utility>
 
 #include "async_copy.cuh"
 #include "fft_block.cuh"
@@ -103,12 +106,13 @@ __global__ void __launch_bounds__(256) rows_kernel(RowParams p) {
   float wxs[8];  // w(x) at this thread's columns, fixed for the whole kernel
 #pragma unroll
   for (int q = 0; q < 8; q++) wxs[q] = __ldg(&p.win[t + q * NT]);
-  // reference pixels of the first batch's frame (raw loads, used next iteration)
-  float cpx[4];
+  // reference pixels of the first batch's frame (raw loads, converted at use
+  // so that the prefetch never waits on them)
+  Tin cpx[4];
   {
     const long long f = blockIdx.x < nbatch ? blockIdx.x / BPF : 0;
 #pragma unroll
-    for (int i = 0; i < 4; i++) cpx[i] = ld_pix(frames + f * p.frame_stride + cref_offset<N>(i));
+    for (int i = 0; i < 4; i++) cpx[i] = __ldg(frames + f * p.frame_stride + cref_offset<N>(i));
   }
   // pixel sums: exact integers for u8/u16 (warp totals < 2^31), FP64 for f32
   constexpr bool INT = !std::is_floating_point<Tin>::value;
@@ -119,12 +123,12 @@ __global__ void __launch_bounds__(256) rows_kernel(RowParams p) {
     const int st = it % ROW_STAGES;
     const int f = (int)(b / BPF);
     const int r = (int)(b % BPF);
-    const float cf = 0.25f * ((cpx[0] + cpx[1]) + (cpx[2] + cpx[3]));
+    const float cf = 0.25f * (((float)cpx[0] + (float)cpx[1]) + ((float)cpx[2] + (float)cpx[3]));
     {  // next batch's reference pixels
       const long long bn = b + gridDim.x;
       const long long fn = bn < nbatch ? bn / BPF : f;
 #pragma unroll
-      for (int i = 0; i < 4; i++) cpx[i] = ld_pix(frames + fn * p.frame_stride + cref_offset<N>(i));
+      for (int i = 0; i < 4; i++) cpx[i] = __ldg(frames + fn * p.frame_stride + cref_offset<N>(i));
     }
     if (!mbar_wait(&bar[st], (uint32_t)(it / ROW_STAGES) & 1u, p.err, 2)) {
       // give up: let this CTA's other copies in flight land (bounded), then stop
@@ -202,12 +206,14 @@ __global__ void __launch_bounds__(256) cols_kernel(ColParams p) {
   extern __shared__ __align__(16) float2 sm[];
   __shared__ __align__(8) uint64_t bar;
   __shared__ float s_dc[G];  // (c_f - mu) scale / N per frame of the tile
+  __shared__ float2 s_wc4[4];
   const int g = threadIdx.x / NT, t = threadIdx.x % NT;
   float2* buf0 = sm + (size_t)g * 2 * PN;
   float2* buf1 = buf0 + PN;
   float2* s_tw = sm + (size_t)G * 2 * PN;
   float2* stage = s_tw + tw_size(N);  // [G][N][KB]
   for (int i = threadIdx.x; i < tw_size(N); i += blockDim.x) s_tw[i] = p.tw[i];
+  if (threadIdx.x < 4) s_wc4[threadIdx.x] = p.wc4[threadIdx.x];
   const int nfg = (p.nframes + G - 1) / G;
   const int ntiles = p.NHB * nfg;
   const float invN = 1.f / N;
@@ -256,6 +262,14 @@ __global__ void __launch_bounds__(256) cols_kernel(ColParams p) {
         __syncthreads();
         if (threadIdx.x == 0 && tile + (int)gridDim.x < ntiles) issue(tile + gridDim.x);
       }
+      // this thread's 8 output modes of the correction table, loaded now so
+      // the column transform hides their latency
+      constexpr int KYS = 256 / G;  // ky stride of the store loop
+      float2 wreg[N / KYS];
+      if (p.w2d) {
+#pragma unroll
+        for (int i = 0; i < N / KYS; i++) wreg[i] = __ldg(&p.w2d[(size_t)kx * N + threadIdx.x / G + i * KYS]);
+      }
       const float2* Y = fft<N, false, true, SYNC>(v, t, buf0, buf1, s_tw, 1 + g);
       __syncthreads();  // every group's column (and s_dc) is in shared memory
       // Y of group g sits at the same offset in every group's buffer pair; the
@@ -266,15 +280,17 @@ __global__ void __launch_bounds__(256) cols_kernel(ColParams p) {
         float2* hs = p.hist + (size_t)kx * p.T + slot;
         const size_t mstride = (size_t)p.NH * p.T;
         const float dc = s_dc[sf];
-        const float2 wkx = kx < 4 ? p.wc4[kx] : make_float2(0.f, 0.f);
-        for (int ky = threadIdx.x / G; ky < N; ky += 256 / G) {
+        const float2 wkx = kx < 4 ? s_wc4[kx] : make_float2(0.f, 0.f);
+#pragma unroll
+        for (int i = 0; i < N / KYS; i++) {
+          const int ky = threadIdx.x / G + i * KYS;
           const float2 y = ys[pad(ky)];
           float2 w = make_float2(0.f, 0.f);
           if (p.w2d) {
-            w = __ldg(&p.w2d[(size_t)kx * N + ky]);
+            w = wreg[i];
           } else if (kx < 4 && (ky < 4 || ky > N - 4)) {
             // separable window: W(kx) W(ky), W(N - k) = conj W(k)
-            const float2 wk = ky < 4 ? p.wc4[ky] : make_float2(p.wc4[N - ky].x, -p.wc4[N - ky].y);
+            const float2 wk = ky < 4 ? s_wc4[ky] : make_float2(s_wc4[N - ky].x, -s_wc4[N - ky].y);
             w = cmul(wkx, wk);
           }
           hs[(size_t)ky * mstride] = make_float2(fmaf(dc, w.x, y.x * invN), fmaf(dc, w.y, y.y * invN));
@@ -297,13 +313,31 @@ static size_t fft_smem() {
   return ((size_t)groups<N>() * 2 * padded(N) + tw_size(N)) * sizeof(float2);
 }
 
+// One wave of persistent CTAs. The occupancy query and the shared-memory
+// opt-in are made once per kernel and device (they cost more host time than
+// the launch itself).
 template <typename K>
 static int persistent_grid(K k, int threads, size_t smem, long long work) {
-  int dev = 0, sms = 0, per = 0;
+  static std::mutex mu;
+  static std::map<std::pair<const void*, int>, int> waves;
+  int dev = 0;
   cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, threads, smem);
-  const long long g = (long long)sms * (per > 0 ? per : 1);
+  const auto key = std::make_pair((const void*)k, dev);
+  int g = 0;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = waves.find(key);
+    if (it != waves.end()) g = it->second;
+  }
+  if (g <= 0) {
+    int sms = 0, per = 0;
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, threads, smem);
+    g = sms * (per > 0 ? per : 1);
+    std::lock_guard<std::mutex> lk(mu);
+    waves[key] = g;
+  }
   return (int)(work < g ? (work > 0 ? work : 1) : g);
 }
 
@@ -313,7 +347,6 @@ static cudaError_t rows_n(const RowParams& p, cudaStream_t s) {
   const long long npairs = (long long)p.nframes * (N / 2);
   auto k = rows_kernel<N, Tin>;
   const size_t sm = fft_smem<N>() + N * sizeof(float) + (size_t)ROW_STAGES * 2 * G * N * (sizeof(Tin) + 1);
-  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   const int grid = persistent_grid(k, G * (N / 8), sm, (npairs + G - 1) / G);
   k<<<grid, G * (N / 8), sm, s>>>(p);
   return cudaGetLastError();
@@ -346,7 +379,6 @@ static cudaError_t cols_n(const ColParams& p, cudaStream_t s) {
   constexpr int G = groups<N>();
   auto k = cols_kernel<N>;
   const size_t sm = fft_smem<N>() + (size_t)G * N * KB * sizeof(float2);
-  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   const int grid = persistent_grid(k, G * (N / 8), sm, (long long)p.NHB * ((p.nframes + G - 1) / G));
   k<<<grid, G * (N / 8), sm, s>>>(p);
   return cudaGetLastError();

@@ -11,7 +11,10 @@ Where a bin's cost surface has two basins of nearly equal cost, the FP32
 model and the FP64 oracle can step into different ones from the same start;
 such bins (some parameter further apart than 5 %) may be at most 1 in 12 and
 must still agree in cost, and every bin where both land in the same basin
-must agree to 1e-3."""
+must agree to 1e-3. Bins on which the oracle itself does not converge within
+its iteration budget (a valley it is still walking down, e.g. D -> 0 when the
+data do not determine D) are left out: their end point is set by the budget.
+"""
 import numpy as np
 import pytest
 
@@ -39,10 +42,16 @@ def _same_basin(a, b):
     return abs(a[2] - b[2]) <= 0.05 and all(abs(np.exp(a[k] - b[k]) - 1) <= 0.05 for k in (3, 4, 5))
 
 
-def _judge(pairs):
-    """pairs of (theta_gpu, cost_gpu, theta_oracle, cost_oracle)."""
+MAX_ITER = 200
+
+
+def _judge(pairs, cap=MAX_ITER):
+    """pairs of (theta_gpu, cost_gpu, theta_oracle, cost_oracle, oracle
+    iterations); `cap` = the oracle's iteration budget for one fit."""
     other_basin, bad = 0, []
-    for i, (tg, cg, to, co) in enumerate(pairs):
+    pairs = [p for p in pairs if p[4] < cap]
+    assert len(pairs) >= 40
+    for i, (tg, cg, to, co, _) in enumerate(pairs):
         if not _same_basin(tg, to):
             other_basin += 1
             if not abs(cg - co) <= 1e-3 * co + 1e-12:
@@ -72,7 +81,8 @@ def test_lm_seeded_matches_oracle(noise):
     d, tau, qn, w = _arrays(cases)
     start = _starts(cases)
     res = fit.fit_lm(d, tau, qn, w, b6, mode="seeded", start=start)
-    pairs = [(res.theta[i], res.cost[i]) + O.lm_fit_start(c["d"], tau, c["qn"], c["w"], b6, start[i])[:2]
+    pairs = [(res.theta[i], res.cost[i]) + O.lm_fit_start(c["d"], tau, c["qn"], c["w"], b6, start[i],
+                                                          max_iter=MAX_ITER)
              for i, c in enumerate(cases)]
     _judge(pairs)
 
@@ -83,9 +93,9 @@ def test_lm_plain_matches_oracle(noise):
     b6 = bounds6(cases)
     d, tau, qn, w = _arrays(cases)
     res = fit.fit_lm(d, tau, qn, w, b6, mode="plain")
-    pairs = [(res.theta[i], res.cost[i]) + O.lm_fit_plain(c["d"], tau, c["qn"], c["w"], b6)[:2]
+    pairs = [(res.theta[i], res.cost[i]) + O.lm_fit_plain(c["d"], tau, c["qn"], c["w"], b6, max_iter=MAX_ITER)[:3]
              for i, c in enumerate(cases)]
-    _judge(pairs)
+    _judge(pairs, cap=3 * MAX_ITER)  # three refined starts
     assert (res.iters > 0).all() and (res.evals > 100).all()
 
 

@@ -47,6 +47,16 @@ _SIGS = {
     "ddm_kernel_launches": (C.c_int64, [_vp]),
     "ddm_fit_lm": (C.c_int, [_i32, _i32, _i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i32, _i32,
                              C.c_double, _i32, _vp, _vp, _vp, _vp, _i32, _vp]),
+    "ddm_mlp_create": (C.c_int, [_i32, C.c_uint64, C.POINTER(_vp)]),
+    "ddm_mlp_destroy": (None, [_vp]),
+    "ddm_mlp_last_error": (C.c_char_p, [_vp]),
+    "ddm_mlp_param_count": (_i32, []),
+    "ddm_mlp_get_params": (C.c_int, [_vp, _vp]),
+    "ddm_mlp_set_params": (C.c_int, [_vp, _vp]),
+    "ddm_mlp_forward": (C.c_int, [_vp, _vp, _i32, _vp, _vp]),
+    "ddm_mlp_gradients": (C.c_int, [_vp, _vp, _vp, _i32, _vp, _vp]),
+    "ddm_mlp_train_step": (C.c_int, [_vp, _vp, _vp, _i32, C.c_float, _vp]),
+    "ddm_mlp_sync": (C.c_int, [_vp]),
     "ddm_spectra_noalloc": (C.c_int, [_vp, _i32, _i32, _i32, _i32, _vp, C.c_float, _vp, _vp]),
 }
 

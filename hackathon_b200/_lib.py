@@ -54,9 +54,9 @@ _SIGS = {
     "ddm_mlp_get_params": (C.c_int, [_vp, _vp]),
     "ddm_mlp_set_params": (C.c_int, [_vp, _vp]),
     "ddm_mlp_forward": (C.c_int, [_vp, _vp, _i32, _vp, _vp]),
-    "ddm_mlp_gradients": (C.c_int, [_vp, _vp, _vp, _i32, _vp, _vp]),
-    "ddm_mlp_train_step": (C.c_int, [_vp, _vp, _vp, _i32, C.c_float, _vp]),
-    "ddm_mlp_sync": (C.c_int, [_vp]),
+    "ddm_mlp_gradients": (C.c_int, [_vp, _vp, _vp, _i32, _vp, _vp, _vp]),
+    "ddm_mlp_train_step": (C.c_int, [_vp, _vp, _vp, _i32, C.c_float, _vp, _vp]),
+    "ddm_mlp_sync": (C.c_int, [_vp, _vp]),
     "ddm_spectra_noalloc": (C.c_int, [_vp, _i32, _i32, _i32, _i32, _vp, C.c_float, _vp, _vp]),
 }
 

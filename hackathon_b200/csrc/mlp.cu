@@ -453,7 +453,6 @@ void release(ddm_mlp* h) {
   }
   f(h->xh); f(h->xt); f(h->out); f(h->dA); f(h->dAt); f(h->dB); f(h->dBt); f(h->dO); f(h->dOt);
   f(h->loss); f(h->d_err);
-  if (h->stream) cudaStreamDestroy(h->stream);
 }
 
 int refresh_bf16(ddm_mlp* h) {
@@ -597,8 +596,8 @@ extern "C" int ddm_mlp_create(int32_t batch_max, uint64_t seed, ddm_mlp** out) {
   h->dev = dev;
   h->bmax = batch_max;
   const size_t B = batch_max;
-  bool ok = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) == cudaSuccess;
-  ok = ok && zalloc(&h->d_err, 1) == cudaSuccess && zalloc(&h->loss, 1) == cudaSuccess;
+  h->stream = nullptr;  // set-up work on the legacy default stream; calls name their stream
+  bool ok = zalloc(&h->d_err, 1) == cudaSuccess && zalloc(&h->loss, 1) == cudaSuccess;
   for (int l = 0; l < NL && ok; l++) {
     const size_t nw = (size_t)OUT_P[l] * IN_P[l];
     ok = zalloc(&h->W[l], nw) == cudaSuccess && zalloc(&h->b[l], OUT_P[l]) == cudaSuccess &&
@@ -647,7 +646,7 @@ extern "C" int ddm_mlp_create(int32_t batch_max, uint64_t seed, ddm_mlp** out) {
 extern "C" void ddm_mlp_destroy(ddm_mlp* h) {
   if (!h) return;
   cudaSetDevice(h->dev);
-  cudaStreamSynchronize(h->stream);
+  cudaDeviceSynchronize();
   release(h);
   delete h;
 }
@@ -682,14 +681,15 @@ static int copy_params(ddm_mlp* h, float* const* src_dev, float* const* bsrc_dev
 extern "C" int ddm_mlp_get_params(ddm_mlp* h, float* params) {
   if (!h || !params) return mlp_fail(h, DDM_ERR_ARG, "null argument");
   cudaSetDevice(h->dev);
-  MCK(cudaStreamSynchronize(h->stream));
+  MCK(cudaDeviceSynchronize());
   return copy_params(h, h->W, h->b, params, true);
 }
 
 extern "C" int ddm_mlp_set_params(ddm_mlp* h, const float* params) {
   if (!h || !params) return mlp_fail(h, DDM_ERR_ARG, "null argument");
   cudaSetDevice(h->dev);
-  MCK(cudaStreamSynchronize(h->stream));
+  MCK(cudaDeviceSynchronize());
+  h->stream = nullptr;
   int rc = copy_params(h, h->W, h->b, const_cast<float*>(params), false);
   if (rc) return rc;
   for (int l = 0; l < NL; l++) {
@@ -709,18 +709,15 @@ extern "C" int ddm_mlp_forward(ddm_mlp* h, const float* x, int32_t n, float* out
   int rc = check_rows(h, n);
   if (rc) return rc;
   cudaSetDevice(h->dev);
-  cudaStream_t s = stream ? (cudaStream_t)stream : h->stream;
-  cudaStream_t own = h->stream;
-  h->stream = s;
-  cast_input_kernel<<<(n * KIN + 255) / 256, 256, 0, s>>>(x, n, h->xh, nullptr);
+  h->stream = (cudaStream_t)stream;
+  cast_input_kernel<<<(n * KIN + 255) / 256, 256, 0, h->stream>>>(x, n, h->xh, nullptr);
   rc = forward(h, n, false);
   if (!rc) {
     // [n][16] -> [n][5]
     cudaError_t e = cudaMemcpy2DAsync(out, sizeof(float) * NOUT, h->out, sizeof(float) * NOP, sizeof(float) * NOUT,
-                                      n, cudaMemcpyDeviceToDevice, s);
+                                      n, cudaMemcpyDeviceToDevice, h->stream);
     if (e != cudaSuccess) rc = mlp_fail(h, DDM_ERR_CUDA, "output copy: %s", cudaGetErrorString(e));
   }
-  h->stream = own;
   return rc;
 }
 
@@ -737,11 +734,12 @@ static int grads(ddm_mlp* h, const float* x, const float* y, int n) {
 }
 
 extern "C" int ddm_mlp_gradients(ddm_mlp* h, const float* x, const float* y, int32_t n, float* grads_host,
-                                 float* loss_host) {
+                                 float* loss_host, void* stream) {
   if (!h || !x || !y || !grads_host) return mlp_fail(h, DDM_ERR_ARG, "null argument");
   int rc = check_rows(h, n);
   if (rc) return rc;
   cudaSetDevice(h->dev);
+  h->stream = (cudaStream_t)stream;
   if ((rc = grads(h, x, y, n))) return rc;
   MCK(cudaStreamSynchronize(h->stream));
   if ((rc = device_error(h))) return rc;
@@ -750,12 +748,13 @@ extern "C" int ddm_mlp_gradients(ddm_mlp* h, const float* x, const float* y, int
 }
 
 extern "C" int ddm_mlp_train_step(ddm_mlp* h, const float* x, const float* y, int32_t n, float lr,
-                                  float* loss_host) {
+                                  float* loss_host, void* stream) {
   if (!h || !x || !y) return mlp_fail(h, DDM_ERR_ARG, "null argument");
   int rc = check_rows(h, n);
   if (rc) return rc;
   if (!(lr > 0)) return mlp_fail(h, DDM_ERR_ARG, "lr must be > 0");
   cudaSetDevice(h->dev);
+  h->stream = (cudaStream_t)stream;
   if ((rc = grads(h, x, y, n))) return rc;
   h->step++;
   const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
@@ -778,9 +777,9 @@ extern "C" int ddm_mlp_train_step(ddm_mlp* h, const float* x, const float* y, in
   return DDM_OK;
 }
 
-extern "C" int ddm_mlp_sync(ddm_mlp* h) {
+extern "C" int ddm_mlp_sync(ddm_mlp* h, void* stream) {
   if (!h) return DDM_ERR_ARG;
   cudaSetDevice(h->dev);
-  MCK(cudaStreamSynchronize(h->stream));
+  MCK(cudaStreamSynchronize((cudaStream_t)stream));
   return device_error(h);
 }

@@ -103,14 +103,22 @@ class Surrogate:
         assert p.size == self.nparams
         self._check(self._lib.ddm_mlp_set_params(self._h, C.c_void_p(p.ctypes.data)))
 
+    @staticmethod
+    def _stream(stream):
+        """The caller's stream, default torch's current one (ordered with torch work)."""
+        import torch
+        s = torch.cuda.current_stream().cuda_stream if stream is None else stream
+        return C.c_void_p(s) if s else None
+
     def forward(self, x, out=None, stream=None):
-        """x: torch CUDA tensor [n, 65] FP32 -> [n, 5] FP32 (device)."""
+        """x: torch CUDA tensor [n, 65] FP32 -> [n, 5] FP32 (device), queued
+        on `stream` (default torch's current stream)."""
         import torch
         n = x.shape[0]
         if out is None:
             out = torch.empty((n, NOUT), dtype=torch.float32, device=x.device)
         self._check(self._lib.ddm_mlp_forward(self._h, C.c_void_p(x.data_ptr()), n, C.c_void_p(out.data_ptr()),
-                                              C.c_void_p(stream) if stream else None))
+                                              self._stream(stream)))
         return out
 
     def predict(self, feats, chunk=None):
@@ -125,21 +133,23 @@ class Surrogate:
             xt = torch.zeros((m, NFEAT), dtype=torch.float32, device="cuda")
             xt[: b - a] = torch.from_numpy(np.ascontiguousarray(feats[a:b], np.float32)).cuda()
             out[a:b] = self.forward(xt)[: b - a].cpu().numpy()
-        self._check(self._lib.ddm_mlp_sync(self._h))
+        self.sync()
         return out
 
-    def gradients(self, x, y):
+    def gradients(self, x, y, stream=None):
         g = np.zeros(self.nparams, np.float32)
         loss = C.c_float()
         self._check(self._lib.ddm_mlp_gradients(self._h, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()),
-                                                x.shape[0], C.c_void_p(g.ctypes.data), C.byref(loss)))
+                                                x.shape[0], C.c_void_p(g.ctypes.data), C.byref(loss),
+                                                self._stream(stream)))
         return loss.value, g
 
-    def train_step(self, x, y, lr, want_loss=False):
+    def train_step(self, x, y, lr, want_loss=False, stream=None):
         loss = C.c_float()
         self._check(self._lib.ddm_mlp_train_step(self._h, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()),
-                                                 x.shape[0], float(lr), C.byref(loss) if want_loss else None))
+                                                 x.shape[0], float(lr), C.byref(loss) if want_loss else None,
+                                                 self._stream(stream)))
         return loss.value if want_loss else None
 
-    def sync(self):
-        self._check(self._lib.ddm_mlp_sync(self._h))
+    def sync(self, stream=None):
+        self._check(self._lib.ddm_mlp_sync(self._h, self._stream(stream)))

@@ -184,7 +184,10 @@ int ddm_fit_lm(int32_t nfit, int32_t nt_max, int32_t K, const int32_t *nt, const
  * tensor cores (BF16 operands, FP32 accumulators in tensor memory); FP32
  * master weights with Adam. Its prediction only seeds ddm_fit_lm (mode 1).
  * x, y and out are DEVICE arrays (row-major [n][65], [n][5], [n][5]); n is a
- * multiple of 8 and at most batch_max. Errors via ddm_mlp_last_error(h)
+ * multiple of 8 and at most batch_max. Work is queued on the caller's
+ * `stream` (cudaStream_t as void*, NULL = the legacy default stream), in
+ * order with the caller's other work there; one model serves one stream at
+ * a time. Errors via ddm_mlp_last_error(h)
  * (or with h = NULL after a failed create). Parameters travel as one flat
  * FP32 array: per layer W [out][in] row-major, then b [out]. */
 typedef struct ddm_mlp ddm_mlp;
@@ -194,17 +197,17 @@ const char *ddm_mlp_last_error(const ddm_mlp *h);
 int32_t ddm_mlp_param_count(void);
 int ddm_mlp_get_params(ddm_mlp *h, float *params);
 int ddm_mlp_set_params(ddm_mlp *h, const float *params);
-/* Inference, queued on `stream` (NULL = the model's stream). */
+/* Inference. */
 int ddm_mlp_forward(ddm_mlp *h, const float *x, int32_t n, float *out, void *stream);
 /* Forward + backward of the mean-squared error; host grads in the parameter
  * layout and the loss (may be NULL). Blocks. */
 int ddm_mlp_gradients(ddm_mlp *h, const float *x, const float *y, int32_t n, float *grads,
-                      float *loss);
+                      float *loss, void *stream);
 /* One Adam step (lr; beta 0.9, 0.999). loss != NULL blocks and returns it. */
 int ddm_mlp_train_step(ddm_mlp *h, const float *x, const float *y, int32_t n, float lr,
-                       float *loss);
-/* Waits for the model's queued work; surfaces device-side error words. */
-int ddm_mlp_sync(ddm_mlp *h);
+                       float *loss, void *stream);
+/* Waits for `stream`; surfaces the model's device-side error words. */
+int ddm_mlp_sync(ddm_mlp *h, void *stream);
 
 /* Allocation-free spatial stage. No counterpart in the reference (its WebGPU
  * engine allocates all buffers at create time); this is for callers that may

@@ -46,7 +46,8 @@ _SIGS = {
     "ddm_set_stream": (C.c_int, [_vp, _vp]),
     "ddm_kernel_launches": (C.c_int64, [_vp]),
     "ddm_fit_lm": (C.c_int, [_i32, _i32, _i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i32, _i32,
-                             C.c_double, _i32, _vp, _vp, _vp, _vp, _i32, _vp]),
+                             C.c_double, _i32, _vp, _vp, _vp, _vp, _vp, _i32, _vp]),
+    "ddm_model_curves": (C.c_int, [_i32, _i32, _vp, _vp, _i32, _vp, C.c_float, C.c_uint64, _vp, _vp, _vp]),
     "ddm_mlp_create": (C.c_int, [_i32, C.c_uint64, C.POINTER(_vp)]),
     "ddm_mlp_destroy": (None, [_vp]),
     "ddm_mlp_last_error": (C.c_char_p, [_vp]),

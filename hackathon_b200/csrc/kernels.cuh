@@ -82,7 +82,7 @@ struct RadialFullParams {
   double* odrift;
 };
 
-enum { LM_PLAIN = 0, LM_SEEDED = 1 };
+enum { LM_PLAIN = 0, LM_SEEDED = 1, LM_SEEDED_FALLBACK = 2 };
 
 struct LmParams {
   int nfit, nt_max, K;
@@ -97,6 +97,7 @@ struct LmParams {
   double* cost;            // [nfit] out
   int* iters;              // [nfit] out (or nullptr)
   int* evals;              // [nfit] out (or nullptr)
+  int* status;             // [nfit] out (or nullptr): bit 0 converged, bit 1 fell back to mode 0
   int mode, max_iter, nrefine;
   double tol;
 };

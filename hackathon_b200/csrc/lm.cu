@@ -259,10 +259,11 @@ __device__ __forceinline__ bool lm_solve(const double (&H)[21], const double (&g
 // set), continuing from lambda; returns the iterations taken.
 template <typename R>
 __device__ int lm_phase(const LmProblem& P, int lane, double (&th)[LM_NP], double& cost, double& lambda,
-                        int max_iter, double tol) {
+                        int max_iter, double tol, bool& converged) {
   double H[21], gr[LM_NP];
   lm_normal<R>(P, th, lane, H, gr, cost);
   int small = 0, it = 0;
+  converged = false;
   for (it = 0; it < max_iter; it++) {
     double delta[LM_NP];
     if (!lm_solve(H, gr, lambda, delta)) {
@@ -289,6 +290,7 @@ __device__ int lm_phase(const LmProblem& P, int lane, double (&th)[LM_NP], doubl
       small = rel < tol ? small + 1 : 0;
       if (small >= 2) {
         it++;
+        converged = true;
         break;
       }
     } else {
@@ -302,16 +304,108 @@ __device__ int lm_phase(const LmProblem& P, int lane, double (&th)[LM_NP], doubl
 // Marquardt's method (the iteration of oracle/lm.c): FP32 model until the
 // FP32 cost stops resolving progress, then FP64 model iterations from there
 // (the FP32 cost carries ~1e-7 relative noise, which would otherwise stop
-// the walk early along flat valleys). Returns the iterations taken.
+// the walk early along flat valleys). Returns the iterations taken;
+// `converged` = the FP64 phase met the relative-decrease test.
 __device__ int lm_run(const LmProblem& P, int lane, double (&th)[LM_NP], double& cost, int max_iter,
-                      double tol) {
+                      double tol, bool& converged) {
   double lambda = 1e-3;
-  const int it32 = lm_phase<float>(P, lane, th, cost, lambda, max_iter, tol);
+  bool c32;
+  const int it32 = lm_phase<float>(P, lane, th, cost, lambda, max_iter, tol, c32);
   // the FP32 phase often ends on a run of rejected steps (lambda > 1e12)
   // that only the FP32 noise caused: restart the damping
   lambda = 1e-3;
-  const int it64 = lm_phase<double>(P, lane, th, cost, lambda, max_iter - it32 > 8 ? max_iter - it32 : 8, tol);
+  const int it64 =
+      lm_phase<double>(P, lane, th, cost, lambda, max_iter - it32 > 8 ? max_iter - it32 : 8, tol, converged);
   return it32 + it64;
+}
+
+// The reference's start strategy (fitBrownian, motility_fit.js:500-536;
+// fitSwimmer :577-611) per bin, LM from the best `nrefine` of 64 starts
+// (oracle/lm.c or_lm_fit_plain). Accumulates iterations and evaluations.
+__device__ void plain_fit(const LmProblem& P, int lane, int nrefine, int max_iter, double tol,
+                          double (&th)[LM_NP], double& cost, int& iters, int& evals, bool& converged) {
+  double A, B;
+  const double lo = P.lo[5], hi = P.hi[5];
+  int bi = 0;
+  double bf = 1e308;
+  for (int i = 0; i <= 48; i++) {
+    const double x = lo + ((hi - lo) * i) / 48;
+    const double v = varpro(P, lane, 0.0, P.lo[3], 0.0, x, A, B);
+    if (v < bf) bf = v, bi = i;
+  }
+  evals += 49;
+  double a = lo + ((hi - lo) * (bi > 0 ? bi - 1 : 0)) / 48;
+  double b = lo + ((hi - lo) * (bi < 48 ? bi + 1 : 48)) / 48;
+  const double gr = (sqrt(5.0) - 1) / 2;
+  double c = b - gr * (b - a), dd = a + gr * (b - a);
+  double fc = varpro(P, lane, 0.0, P.lo[3], 0.0, c, A, B);
+  double fd = varpro(P, lane, 0.0, P.lo[3], 0.0, dd, A, B);
+  evals += 2;
+  for (int it = 0; it < 60 && b - a > 1e-6; it++) {
+    if (fc < fd) {
+      b = dd;
+      dd = c;
+      fd = fc;
+      c = b - gr * (b - a);
+      fc = varpro(P, lane, 0.0, P.lo[3], 0.0, c, A, B);
+    } else {
+      a = c;
+      c = dd;
+      fc = fd;
+      dd = a + gr * (b - a);
+      fd = varpro(P, lane, 0.0, P.lo[3], 0.0, dd, A, B);
+    }
+    evals++;
+  }
+  const double lD0 = fc < fd ? c : dd;
+  // 64 starts: lane l holds starts 2l and 2l+1 (index = 4 iv + 2 iz + ia)
+  const double lZs0 = fmin(P.hi[4], fmax(P.lo[4], log(1.5)));
+  const double lZs1 = fmin(P.hi[4], fmax(P.lo[4], log(8.0)));
+  double sc[2];
+  for (int s = 0; s < 64; s++) {
+    const int iv = s >> 2, iz = (s >> 1) & 1, ia = s & 1;
+    const double lv = P.lo[3] + ((P.hi[3] - P.lo[3]) * (iv + 0.5)) / 16;
+    const double f = varpro(P, lane, ia ? 0.8 : 0.3, lv, iz ? lZs1 : lZs0, lD0, A, B);
+    if ((s >> 1) == lane) sc[s & 1] = f;
+  }
+  evals += 64;
+  double best = 1e308;
+  double bth[LM_NP] = {0, 0, 0, 0, 0, 0};
+  bool bconv = false;
+  for (int k = 0; k < nrefine && k < 64; k++) {
+    // k-th smallest cost, lowest index on ties (a stable sort's order)
+    double m = sc[0] <= sc[1] ? sc[0] : sc[1];
+    int mi = sc[0] <= sc[1] ? 2 * lane : 2 * lane + 1;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const double m2 = __shfl_xor_sync(0xffffffffu, m, o);
+      const int i2 = __shfl_xor_sync(0xffffffffu, mi, o);
+      if (m2 < m || (m2 == m && i2 < mi)) m = m2, mi = i2;
+    }
+    if ((mi >> 1) == lane) sc[mi & 1] = 1e308;  // taken
+    const int iv = mi >> 2, iz = (mi >> 1) & 1, ia = mi & 1;
+    double t2[LM_NP];
+    t2[2] = ia ? 0.8 : 0.3;
+    t2[3] = P.lo[3] + ((P.hi[3] - P.lo[3]) * (iv + 0.5)) / 16;
+    t2[4] = iz ? lZs1 : lZs0;
+    t2[5] = lD0;
+    varpro(P, lane, t2[2], t2[3], t2[4], t2[5], t2[0], t2[1]);
+    double cst;
+    bool cv;
+    const int it = lm_run(P, lane, t2, cst, max_iter, tol, cv);
+    iters += it;
+    evals += 2 + it;
+    if (cst < best) {
+      best = cst;
+      bconv = cv;
+#pragma unroll
+      for (int q = 0; q < LM_NP; q++) bth[q] = t2[q];
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < LM_NP; q++) th[q] = bth[q];
+  cost = best;
+  converged = bconv;
 }
 
 __global__ void __launch_bounds__(32 * LM_WARPS) lm_kernel(LmParams p) {
@@ -344,8 +438,9 @@ __global__ void __launch_bounds__(32 * LM_WARPS) lm_kernel(LmParams p) {
     P.hi[3 + a] = log((double)bd[2 * a + 1]);
   }
   double th[LM_NP], cost = 0;
-  int iters = 0, evals = 0;
-  if (p.mode == LM_SEEDED) {
+  int iters = 0, evals = 0, status = 0;
+  bool conv = false;
+  if (p.mode == LM_SEEDED || p.mode == LM_SEEDED_FALLBACK) {
     const float* s = p.start + (size_t)fit * 4;
     th[2] = (double)s[0];
     th[3] = log((double)s[1]);
@@ -354,90 +449,26 @@ __global__ void __launch_bounds__(32 * LM_WARPS) lm_kernel(LmParams p) {
 #pragma unroll
     for (int a = 2; a < LM_NP; a++) th[a] = fmin(P.hi[a], fmax(P.lo[a], th[a]));
     varpro(P, lane, th[2], th[3], th[4], th[5], th[0], th[1]);
-    iters = lm_run(P, lane, th, cost, p.max_iter, p.tol);
+    iters = lm_run(P, lane, th, cost, p.max_iter, p.tol, conv);
     evals = 2 + iters;
+    if (p.mode == LM_SEEDED_FALLBACK && !conv) {
+      // the seed did not lead to a converged fit: the reference's start
+      // strategy decides, and the lower cost wins
+      double t2[LM_NP], c2;
+      bool cv2;
+      plain_fit(P, lane, p.nrefine, p.max_iter, p.tol, t2, c2, iters, evals, cv2);
+      status |= 2;
+      if (c2 < cost) {
+        cost = c2;
+        conv = cv2;
+#pragma unroll
+        for (int q = 0; q < LM_NP; q++) th[q] = t2[q];
+      }
+    }
   } else {
-    // the reference's start strategy (fitBrownian, motility_fit.js:500-536;
-    // fitSwimmer :577-611), per bin; oracle/lm.c or_lm_fit_plain
-    double A, B;
-    const double lo = P.lo[5], hi = P.hi[5];
-    int bi = 0;
-    double bf = 1e308;
-    for (int i = 0; i <= 48; i++) {
-      const double x = lo + ((hi - lo) * i) / 48;
-      const double v = varpro(P, lane, 0.0, P.lo[3], 0.0, x, A, B);
-      if (v < bf) bf = v, bi = i;
-    }
-    evals += 49;
-    double a = lo + ((hi - lo) * (bi > 0 ? bi - 1 : 0)) / 48;
-    double b = lo + ((hi - lo) * (bi < 48 ? bi + 1 : 48)) / 48;
-    const double gr = (sqrt(5.0) - 1) / 2;
-    double c = b - gr * (b - a), dd = a + gr * (b - a);
-    double fc = varpro(P, lane, 0.0, P.lo[3], 0.0, c, A, B);
-    double fd = varpro(P, lane, 0.0, P.lo[3], 0.0, dd, A, B);
-    evals += 2;
-    for (int it = 0; it < 60 && b - a > 1e-6; it++) {
-      if (fc < fd) {
-        b = dd;
-        dd = c;
-        fd = fc;
-        c = b - gr * (b - a);
-        fc = varpro(P, lane, 0.0, P.lo[3], 0.0, c, A, B);
-      } else {
-        a = c;
-        c = dd;
-        fc = fd;
-        dd = a + gr * (b - a);
-        fd = varpro(P, lane, 0.0, P.lo[3], 0.0, dd, A, B);
-      }
-      evals++;
-    }
-    const double lD0 = fc < fd ? c : dd;
-    // 64 starts: lane l holds starts 2l and 2l+1 (index = 4 iv + 2 iz + ia)
-    const double lZs0 = fmin(P.hi[4], fmax(P.lo[4], log(1.5)));
-    const double lZs1 = fmin(P.hi[4], fmax(P.lo[4], log(8.0)));
-    double sc[2];
-    for (int s = 0; s < 64; s++) {
-      const int iv = s >> 2, iz = (s >> 1) & 1, ia = s & 1;
-      const double lv = P.lo[3] + ((P.hi[3] - P.lo[3]) * (iv + 0.5)) / 16;
-      const double f = varpro(P, lane, ia ? 0.8 : 0.3, lv, iz ? lZs1 : lZs0, lD0, A, B);
-      if ((s >> 1) == lane) sc[s & 1] = f;
-    }
-    evals += 64;
-    double best = 1e308;
-    double bth[LM_NP] = {0, 0, 0, 0, 0, 0};
-    for (int k = 0; k < p.nrefine && k < 64; k++) {
-      // k-th smallest cost, lowest index on ties (a stable sort's order)
-      double m = sc[0] <= sc[1] ? sc[0] : sc[1];
-      int mi = sc[0] <= sc[1] ? 2 * lane : 2 * lane + 1;
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        const double m2 = __shfl_xor_sync(0xffffffffu, m, o);
-        const int i2 = __shfl_xor_sync(0xffffffffu, mi, o);
-        if (m2 < m || (m2 == m && i2 < mi)) m = m2, mi = i2;
-      }
-      if ((mi >> 1) == lane) sc[mi & 1] = 1e308;  // taken
-      const int iv = mi >> 2, iz = (mi >> 1) & 1, ia = mi & 1;
-      double t2[LM_NP];
-      t2[2] = ia ? 0.8 : 0.3;
-      t2[3] = P.lo[3] + ((P.hi[3] - P.lo[3]) * (iv + 0.5)) / 16;
-      t2[4] = iz ? lZs1 : lZs0;
-      t2[5] = lD0;
-      varpro(P, lane, t2[2], t2[3], t2[4], t2[5], t2[0], t2[1]);
-      double cst;
-      const int it = lm_run(P, lane, t2, cst, p.max_iter, p.tol);
-      iters += it;
-      evals += 2 + it;
-      if (cst < best) {
-        best = cst;
-#pragma unroll
-        for (int q = 0; q < LM_NP; q++) bth[q] = t2[q];
-      }
-    }
-#pragma unroll
-    for (int q = 0; q < LM_NP; q++) th[q] = bth[q];
-    cost = best;
+    plain_fit(P, lane, p.nrefine, p.max_iter, p.tol, th, cost, iters, evals, conv);
   }
+  status |= conv ? 1 : 0;
 #pragma unroll
   for (int a = 0; a < LM_NP; a++)
     if (lane == a) p.theta[(size_t)fit * LM_NP + a] = th[a];
@@ -445,6 +476,7 @@ __global__ void __launch_bounds__(32 * LM_WARPS) lm_kernel(LmParams p) {
     p.cost[fit] = cost;
     if (p.iters) p.iters[fit] = iters;
     if (p.evals) p.evals[fit] = evals;
+    if (p.status) p.status[fit] = status;
   }
 }
 
@@ -489,17 +521,17 @@ extern "C" int ddm_fit_lm(int32_t nfit, int32_t nt_max, int32_t K, const int32_t
                           const float* tau, const float* qn, const float* w, const float* bounds,
                           const float* start, int32_t mode, int32_t max_iter, double tol,
                           int32_t nrefine, double* theta, double* cost, int32_t* iters, int32_t* evals,
-                          int32_t on_device, void* stream) {
+                          int32_t* status, int32_t on_device, void* stream) {
   ddm_detached_error().clear();
   if (nfit < 0 || nt_max < 1 || nt_max > ddm::LM_MAX_LAGS || K < 1 || K > ddm::LM_MAX_NODES)
     return lm_fail(DDM_ERR_ARG, "ddm_fit_lm: need nfit >= 0, 1 <= nt_max <= %d, 1 <= K <= %d",
                    ddm::LM_MAX_LAGS, ddm::LM_MAX_NODES);
-  if (mode != ddm::LM_PLAIN && mode != ddm::LM_SEEDED)
-    return lm_fail(DDM_ERR_ARG, "ddm_fit_lm: mode must be 0 (reference starts) or 1 (seeded)");
+  if (mode != ddm::LM_PLAIN && mode != ddm::LM_SEEDED && mode != ddm::LM_SEEDED_FALLBACK)
+    return lm_fail(DDM_ERR_ARG, "ddm_fit_lm: mode must be 0 (reference starts), 1 (seeded) or 2 (seeded, fallback)");
   if (max_iter < 1 || nrefine < 1 || nrefine > 64 || !(tol >= 0))
     return lm_fail(DDM_ERR_ARG, "ddm_fit_lm: need max_iter >= 1, 1 <= nrefine <= 64, tol >= 0");
   if (nfit == 0) return DDM_OK;
-  if (!nt || !d || !tau || !qn || !w || !bounds || !theta || !cost || (mode == ddm::LM_SEEDED && !start))
+  if (!nt || !d || !tau || !qn || !w || !bounds || !theta || !cost || (mode != ddm::LM_PLAIN && !start))
     return lm_fail(DDM_ERR_ARG, "ddm_fit_lm: null array");
   cudaStream_t s = (cudaStream_t)stream;
   ddm::LmParams p{};
@@ -512,13 +544,13 @@ extern "C" int ddm_fit_lm(int32_t nfit, int32_t nt_max, int32_t K, const int32_t
   p.tol = tol;
   if (on_device) {
     p.nt = nt; p.d = d; p.tau = tau; p.qn = qn; p.w = w; p.bounds = bounds; p.start = start;
-    p.theta = theta; p.cost = cost; p.iters = iters; p.evals = evals;
+    p.theta = theta; p.cost = cost; p.iters = iters; p.evals = evals; p.status = status;
     cudaError_t e = ddm::launch_lm(p, s);
     if (e != cudaSuccess) return lm_fail(DDM_ERR_CUDA, "ddm_fit_lm: %s", cudaGetErrorString(e));
     return DDM_OK;
   }
   const size_t nf = (size_t)nfit, nd = nf * nt_max;
-  int *dnt = nullptr, *dit = nullptr, *dev = nullptr;
+  int *dnt = nullptr, *dit = nullptr, *dev = nullptr, *dst = nullptr;
   float *dd = nullptr, *dtau = nullptr, *dqn = nullptr, *dw = nullptr, *db = nullptr, *ds = nullptr;
   double *dth = nullptr, *dc = nullptr;
   cudaError_t e = cudaSuccess;
@@ -529,24 +561,125 @@ extern "C" int ddm_fit_lm(int32_t nfit, int32_t nt_max, int32_t K, const int32_t
   step(stage_in(&dqn, qn, nf * K, s));
   step(stage_in(&dw, w, nf, s));
   step(stage_in(&db, bounds, nf * 6, s));
-  if (mode == ddm::LM_SEEDED) step(stage_in(&ds, start, nf * 4, s));
+  if (mode != ddm::LM_PLAIN) step(stage_in(&ds, start, nf * 4, s));
   step(stage_in<double>(&dth, nullptr, nf * 6, s));
   step(stage_in<double>(&dc, nullptr, nf, s));
   step(stage_in<int>(&dit, nullptr, nf, s));
   step(stage_in<int>(&dev, nullptr, nf, s));
+  step(stage_in<int>(&dst, nullptr, nf, s));
   if (e == cudaSuccess) {
     p.nt = dnt; p.d = dd; p.tau = dtau; p.qn = dqn; p.w = dw; p.bounds = db; p.start = ds;
-    p.theta = dth; p.cost = dc; p.iters = dit; p.evals = dev;
+    p.theta = dth; p.cost = dc; p.iters = dit; p.evals = dev; p.status = dst;
     step(ddm::launch_lm(p, s));
     step(cudaMemcpyAsync(theta, dth, sizeof(double) * nf * 6, cudaMemcpyDeviceToHost, s));
     step(cudaMemcpyAsync(cost, dc, sizeof(double) * nf, cudaMemcpyDeviceToHost, s));
     if (iters) step(cudaMemcpyAsync(iters, dit, sizeof(int) * nf, cudaMemcpyDeviceToHost, s));
     if (evals) step(cudaMemcpyAsync(evals, dev, sizeof(int) * nf, cudaMemcpyDeviceToHost, s));
+    if (status) step(cudaMemcpyAsync(status, dst, sizeof(int) * nf, cudaMemcpyDeviceToHost, s));
   }
   for (void* ptr : {(void*)dnt, (void*)dd, (void*)dtau, (void*)dqn, (void*)dw, (void*)db, (void*)ds,
-                    (void*)dth, (void*)dc, (void*)dit, (void*)dev})
+                    (void*)dth, (void*)dc, (void*)dit, (void*)dev, (void*)dst})
     if (ptr) cudaFreeAsync(ptr, s);
   step(cudaStreamSynchronize(s));
   if (e != cudaSuccess) return lm_fail(DDM_ERR_CUDA, "ddm_fit_lm: %s", cudaGetErrorString(e));
+  return DDM_OK;
+}
+
+// ------------------------------------------------------------------ model curves
+
+namespace ddm {
+
+// counter-based standard normal (splitmix64 hash -> Box-Muller)
+__device__ __forceinline__ uint64_t mix64(uint64_t z) {
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+__device__ __forceinline__ float normal01(uint64_t seed, uint64_t i, uint64_t j) {
+  const uint64_t h = mix64(seed ^ mix64(i * 0x100000001B3ull + j));
+  const float u1 = ((float)(h >> 40) + 0.5f) * (1.f / 16777216.f);
+  const float u2 = ((float)((h >> 16) & 0xFFFFFFull) + 0.5f) * (1.f / 16777216.f);
+  return sqrtf(-2.f * logf(u1)) * cospif(2.f * u2);
+}
+
+// c(tau) of one curve (FP32), the model column of lm_normal
+__device__ __forceinline__ float model_at(const float* qn, int K, float al, float v, float Z, float D, float t) {
+  float sE = 0.f;
+  for (int n = 0; n < K; n++) {
+    const float q = qn[n];
+    const float E = expf(-D * q * q * t);
+    float g = 1.f, gx, gz;
+    if (al > 0.f) isf3d_d<float>(q * v * t, Z, g, gx, gz);
+    sE += E * (1.f - al + al * g);
+  }
+  return 1.f - sE / K;
+}
+
+__global__ void curves_kernel(int n, int K, const float* __restrict__ qn, const float* __restrict__ th, int nt,
+                              const float* __restrict__ tau, float noise, uint64_t seed, float* __restrict__ y) {
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long long)n * nt) return;
+  const int i = (int)(idx / nt), j = (int)(idx % nt);
+  const float* t6 = th + (size_t)i * 6;
+  const float c = model_at(qn + (size_t)i * K, K, t6[2], t6[3], t6[4], t6[5], tau[j]);
+  float v = t6[0] * c + t6[1];
+  if (noise > 0.f) v *= 1.f + noise * normal01(seed, (uint64_t)i, (uint64_t)j);
+  y[idx] = v;
+}
+
+// first lag where c reaches 1 - 1/e: a 256-point log scan over [1e-3, 1e7]
+// brackets it, 40 bisection steps refine it; 1e7 if never reached
+__global__ void tau_e_kernel(int n, int K, const float* __restrict__ qn, const float* __restrict__ th,
+                             float* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float* t6 = th + (size_t)i * 6;
+  const float* q = qn + (size_t)i * K;
+  const float target = 1.f - 0.36787944117144233f;
+  const float l0 = logf(1e-3f), l1 = logf(1e7f);
+  float lo = l0, hi = l1;
+  bool found = false;
+  float prev = l0;
+  for (int s = 1; s <= 256 && !found; s++) {
+    const float x = l0 + (l1 - l0) * s / 256.f;
+    if (model_at(q, K, t6[2], t6[3], t6[4], t6[5], expf(x)) >= target) {
+      lo = prev;
+      hi = x;
+      found = true;
+    }
+    prev = x;
+  }
+  if (!found) {
+    out[i] = 1e7f;
+    return;
+  }
+  for (int it = 0; it < 40; it++) {
+    const float mid = 0.5f * (lo + hi);
+    if (model_at(q, K, t6[2], t6[3], t6[4], t6[5], expf(mid)) >= target)
+      hi = mid;
+    else
+      lo = mid;
+  }
+  out[i] = expf(0.5f * (lo + hi));
+}
+
+}  // namespace ddm
+
+extern "C" int ddm_model_curves(int32_t n, int32_t K, const float* qn, const float* theta, int32_t nt,
+                                const float* tau, float noise, uint64_t seed, float* y, float* tau_e,
+                                void* stream) {
+  ddm_detached_error().clear();
+  if (n < 0 || K < 1 || K > ddm::LM_MAX_NODES || nt < 0 || !(noise >= 0))
+    return lm_fail(DDM_ERR_ARG, "ddm_model_curves: need n >= 0, 1 <= K <= %d, nt >= 0, noise >= 0",
+                   ddm::LM_MAX_NODES);
+  if (n == 0) return DDM_OK;
+  if (!qn || !theta || (nt > 0 && (!tau || !y))) return lm_fail(DDM_ERR_ARG, "ddm_model_curves: null array");
+  cudaStream_t s = (cudaStream_t)stream;
+  const long long tot = (long long)n * nt;
+  if (tot > 0) ddm::curves_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(n, K, qn, theta, nt, tau, noise, seed, y);
+  if (tau_e) ddm::tau_e_kernel<<<(n + 127) / 128, 128, 0, s>>>(n, K, qn, theta, tau_e);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return lm_fail(DDM_ERR_CUDA, "ddm_model_curves: %s", cudaGetErrorString(e));
   return DDM_OK;
 }

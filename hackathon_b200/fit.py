@@ -21,7 +21,7 @@ import numpy as np
 from . import _lib
 
 SWIM_MIN_UM_S = 2.0  # GATES.SWIM_MIN_UM_S, motility_fit.js:28-38
-MODES = {"plain": 0, "seeded": 1}
+MODES = {"plain": 0, "seeded": 1, "seeded_fallback": 2}
 MAX_LAGS = 128
 MAX_NODES = 8
 
@@ -97,6 +97,7 @@ class FitResult:
     cost: np.ndarray    # [nfit] weighted RSS
     iters: np.ndarray   # [nfit] LM iterations
     evals: np.ndarray   # [nfit] model evaluations
+    status: np.ndarray = None  # [nfit] bit 0 converged, bit 1 fell back to the reference's starts
 
     @property
     def alpha(self):
@@ -141,19 +142,20 @@ def fit_lm(d, tau, qn, w, bnds, mode="plain", start=None, nt=None, max_iter=200,
     ntv = np.ascontiguousarray(np.full(nfit, nt_max) if nt is None else nt, np.int32)
     m = MODES[mode]
     st = None
-    if m == 1:
+    if m != 0:
         st = np.ascontiguousarray(start, np.float32).reshape(nfit, 4)
     theta = np.zeros((nfit, 6))
     cost = np.zeros(nfit)
     iters = np.zeros(nfit, np.int32)
     evals = np.zeros(nfit, np.int32)
+    status = np.zeros(nfit, np.int32)
     p = lambda a: C.c_void_p(a.ctypes.data) if a is not None else None  # noqa: E731
     _check(lib.ddm_fit_lm(nfit, nt_max, K, p(ntv), p(d), p(tau), p(qn), p(w), p(bnds), p(st), m,
-                          max_iter, tol, nrefine, p(theta), p(cost), p(iters), p(evals), 0, None))
-    return FitResult(theta, cost, iters, evals)
+                          max_iter, tol, nrefine, p(theta), p(cost), p(iters), p(evals), p(status), 0, None))
+    return FitResult(theta, cost, iters, evals, status)
 
 
-def fit_lm_device(d, tau, qn, w, bnds, nt, theta, cost, iters=None, evals=None, mode="plain",
+def fit_lm_device(d, tau, qn, w, bnds, nt, theta, cost, iters=None, evals=None, status=None, mode="plain",
                   start=None, max_iter=200, tol=1e-10, nrefine=3, stream=None):
     """Same on device tensors (torch, contiguous): queued on `stream`."""
     lib = _lib.load()
@@ -163,7 +165,26 @@ def fit_lm_device(d, tau, qn, w, bnds, nt, theta, cost, iters=None, evals=None, 
     s = C.c_void_p(stream) if stream else None
     _check(lib.ddm_fit_lm(nfit, nt_max, K, a(nt), a(d), a(tau), a(qn), a(w), a(bnds), a(start),
                           MODES[mode], max_iter, tol, nrefine, a(theta), a(cost), a(iters), a(evals),
-                          1, s))
+                          a(status), 1, s))
+
+
+def model_curves(theta, qn, tau, noise=0.0, seed=0, want_tau_e=False, stream=None):
+    """Model curves on the GPU (ddm_model_curves): theta [n, 6] = (A, B,
+    alpha, vbar, Z, D), qn [n, K], tau [nt] -> torch CUDA y [n, nt] (and
+    tau_e [n])."""
+    import torch
+    lib = _lib.load()
+    th = torch.as_tensor(np.ascontiguousarray(theta, np.float32)).cuda()
+    q = torch.as_tensor(np.ascontiguousarray(qn, np.float32)).cuda()
+    t = torch.as_tensor(np.ascontiguousarray(tau, np.float32)).cuda()
+    n, K = q.shape
+    y = torch.empty((n, t.numel()), dtype=torch.float32, device="cuda")
+    te = torch.empty(n, dtype=torch.float32, device="cuda") if want_tau_e else None
+    a = lambda x: C.c_void_p(x.data_ptr()) if x is not None else None  # noqa: E731
+    s = torch.cuda.current_stream().cuda_stream if stream is None else stream
+    _check(lib.ddm_model_curves(n, K, a(q), a(th), t.numel(), a(t), float(noise), int(seed), a(y), a(te),
+                                C.c_void_p(s) if s else None))
+    return (y, te) if want_tau_e else y
 
 
 def fit_bins(radial, dxUm=1.0, fps=1.0, mode="plain", start=None, swim_min=SWIM_MIN_UM_S, **kw):

@@ -164,16 +164,29 @@ int64_t ddm_kernel_launches(const ddm_engine *h);
  *           :589-601) ranked by VarPro cost, LM from the best `nrefine`.
  *   mode 1: LM from start[4*i..] = (alpha, vbar, Z, D) (e.g. the surrogate's
  *           prediction), amplitudes from VarPro.
+ *   mode 2: as mode 1; a fit whose LM did not converge also runs mode 0 and
+ *           keeps the lower cost (the reference's starts as the fallback).
  * Arrays: nt[nfit] lags per fit (<= nt_max <= 128), d and tau [nfit][nt_max],
  * qn [nfit][K] (K <= 8), w[nfit], bounds [nfit][6], start [nfit][4];
- * out theta [nfit][6], cost[nfit], iters/evals [nfit] (may be NULL).
+ * out theta [nfit][6], cost[nfit], iters/evals/status [nfit] (may be NULL;
+ * status bit 0 = converged, bit 1 = fell back to mode 0).
  * on_device = 0: host arrays, blocks until done; 1: device arrays, queued on
  * `stream` (cudaStream_t as void*). Errors via ddm_create_error(). */
 int ddm_fit_lm(int32_t nfit, int32_t nt_max, int32_t K, const int32_t *nt, const float *d,
                const float *tau, const float *qn, const float *w, const float *bounds,
                const float *start, int32_t mode, int32_t max_iter, double tol, int32_t nrefine,
-               double *theta, double *cost, int32_t *iters, int32_t *evals, int32_t on_device,
-               void *stream);
+               double *theta, double *cost, int32_t *iters, int32_t *evals, int32_t *status,
+               int32_t on_device, void *stream);
+
+/* Model curves for training and evaluation data (no reference counterpart):
+ * y[i][j] = (A c(tau_j) + B) (1 + noise * n_ij), c the model column above
+ * (FP32), n_ij standard normal from a counter-based generator keyed by
+ * (seed, i, j). theta [n][6] = (A, B, alpha, vbar, Z, D) (linear units),
+ * qn [n][K], tau [nt] shared; tau_e[i] (may be NULL) = the first lag where
+ * c reaches 1 - 1/e (noise-free). DEVICE arrays, queued on `stream`. */
+int ddm_model_curves(int32_t n, int32_t K, const float *qn, const float *theta, int32_t nt,
+                     const float *tau, float noise, uint64_t seed, float *y, float *tau_e,
+                     void *stream);
 
 /* ---------------------------------------------------------------------------
  * Learned seed for the fit: a BF16 tensor-core MLP (no counterpart in the

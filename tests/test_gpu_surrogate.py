@@ -1,0 +1,64 @@
+"""The learned seed end to end on the GPU: the model-curve generator against
+the FP64 model (oracle/lm.c), the seeded-with-fallback LM mode, and what a
+trained surrogate gains over the method without it (the reference's start
+strategy) on held-out curves at equal fit error."""
+import numpy as np
+import pytest
+
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+F = pytest.importorskip("hackathon_b200.fit")
+ST = pytest.importorskip("hackathon_b200.surrogate_train")
+
+
+def test_model_curves_match_fp64_model():
+    th, qn = ST.sample_params(64, seed=1)
+    tau = ST.lm_tau()
+    y = F.model_curves(th, qn, tau).cpu().numpy()
+    for i in range(64):
+        t = th[i].astype(np.float64)
+        ref = O.lm_model(tau.astype(np.float64), qn[i].astype(np.float64),
+                         [t[0], t[1], t[2], np.log(t[3]), np.log(t[4]), np.log(t[5])])
+        assert np.abs(y[i] - ref).max() <= 2e-5 * np.abs(ref).max()
+
+
+def test_model_curve_noise_and_tau_e():
+    th, qn = ST.sample_params(2048, seed=2)
+    tau = ST.lm_tau()
+    clean = F.model_curves(th, qn, tau).cpu().numpy()
+    noisy, te = F.model_curves(th, qn, tau, noise=0.01, seed=7, want_tau_e=True)
+    r = noisy.cpu().numpy() / clean - 1
+    assert abs(r.mean()) < 2e-4 and abs(r.std() - 0.01) < 3e-4
+    te = te.cpu().numpy()
+    for i in range(0, 2048, 97):  # c(tau_e) = 1 - 1/e on the FP64 model (A = 1, B = 0)
+        t = th[i].astype(np.float64)
+        c = O.lm_model(np.array([te[i]], np.float64), qn[i].astype(np.float64),
+                       [1.0, 0.0, t[2], np.log(t[3]), np.log(t[4]), np.log(t[5])])[0]
+        assert abs(c - (1 - np.exp(-1))) < 1e-4
+
+
+def test_seeded_fallback_recovers_from_bad_seeds():
+    data = ST.analytic_set(256, seed=3)
+    bnds = ST.swim_bounds(data["qn"])
+    d = data["d"].cpu().numpy()
+    tau = ST.lm_tau()
+    w = 1 / d.max(1)
+    plain = F.fit_lm(d, tau, data["qn"], w, bnds, mode="plain")
+    bad = np.tile([0.5, bnds[1] * 0.99, 90.0, bnds[4] * 1.01], (256, 1))  # far from every truth
+    fb = F.fit_lm(d, tau, data["qn"], w, bnds, mode="seeded_fallback", start=bad)
+    assert ((fb.status >> 1) & 1).mean() > 0.2  # many seeds did not converge and fell back
+    assert (fb.cost <= plain.cost * (1 + 1e-3) + 1e-30).mean() >= 0.95
+
+
+def test_trained_surrogate_gains_over_plain_lm():
+    net = ST.build_and_train(n_analytic=1 << 16, epochs=6, seed=0, batch_max=8192)
+    held = ST.analytic_set(4096, seed=99)
+    summary, _ = ST.compare_fits(net, held, ST.swim_bounds(held["qn"]))
+    print(summary)
+    assert summary["frac_equal_or_better"] >= 0.9, summary
+    assert summary["speedup"] >= 2.0, summary
+    assert summary["surrogate_mean_evals"] < 0.5 * summary["plain_mean_evals"], summary
+    net.close()

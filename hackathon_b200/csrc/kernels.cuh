@@ -98,6 +98,7 @@ struct LmParams {
   int* iters;              // [nfit] out (or nullptr)
   int* evals;              // [nfit] out (or nullptr)
   int* status;             // [nfit] out (or nullptr): bit 0 converged, bit 1 fell back to mode 0
+  int* counter;            // work counter, 0 at launch (warps fetch fits)
   int mode, max_iter, nrefine;
   double tol;
 };

@@ -257,18 +257,23 @@ __device__ __forceinline__ bool lm_solve(const double (&H)[21], const double (&g
 
 // Marquardt iterations with the model in R from th (projected, amplitudes
 // set), continuing from lambda; returns the iterations taken.
+// max_reject > 0 ends the phase after that many consecutive rejected steps
+// (used by the FP32 phase, whose cost cannot resolve the last decreases).
 template <typename R>
 __device__ int lm_phase(const LmProblem& P, int lane, double (&th)[LM_NP], double& cost, double& lambda,
-                        int max_iter, double tol, bool& converged) {
+                        int max_iter, double tol, bool& converged, int max_reject = 0) {
   double H[21], gr[LM_NP];
   lm_normal<R>(P, th, lane, H, gr, cost);
-  int small = 0, it = 0;
+  int small = 0, it = 0, rejected = 0;
   converged = false;
   for (it = 0; it < max_iter; it++) {
     double delta[LM_NP];
     if (!lm_solve(H, gr, lambda, delta)) {
       lambda *= 4;
-      if (lambda > 1e12) break;
+      if (lambda > 1e12 || (max_reject && ++rejected >= max_reject)) {
+        converged = lambda > 1e12;  // no step lowers the cost: a numerical minimum
+        break;
+      }
       continue;
     }
     double th2[LM_NP];
@@ -287,6 +292,7 @@ __device__ int lm_phase(const LmProblem& P, int lane, double (&th)[LM_NP], doubl
       for (int i = 0; i < 21; i++) H[i] = H2[i];
       cost = c2;
       lambda = fmax(lambda / 3, 1e-12);
+      rejected = 0;
       small = rel < tol ? small + 1 : 0;
       if (small >= 2) {
         it++;
@@ -295,7 +301,10 @@ __device__ int lm_phase(const LmProblem& P, int lane, double (&th)[LM_NP], doubl
       }
     } else {
       lambda *= 4;
-      if (lambda > 1e12) break;
+      if (lambda > 1e12 || (max_reject && ++rejected >= max_reject)) {
+        converged = lambda > 1e12;  // no step lowers the cost: a numerical minimum
+        break;
+      }
     }
   }
   return it;
@@ -305,14 +314,16 @@ __device__ int lm_phase(const LmProblem& P, int lane, double (&th)[LM_NP], doubl
 // FP32 cost stops resolving progress, then FP64 model iterations from there
 // (the FP32 cost carries ~1e-7 relative noise, which would otherwise stop
 // the walk early along flat valleys). Returns the iterations taken;
-// `converged` = the FP64 phase met the relative-decrease test.
+// `converged` = the FP64 phase stopped at a minimum (the relative-decrease
+// test, or no step lowering the cost any more) rather than at the cap.
 __device__ int lm_run(const LmProblem& P, int lane, double (&th)[LM_NP], double& cost, int max_iter,
                       double tol, bool& converged) {
   double lambda = 1e-3;
   bool c32;
-  const int it32 = lm_phase<float>(P, lane, th, cost, lambda, max_iter, tol, c32);
-  // the FP32 phase often ends on a run of rejected steps (lambda > 1e12)
-  // that only the FP32 noise caused: restart the damping
+  // FP32 phase: ends when two accepted steps gain < 1e-6 (the FP32 cost's
+  // resolution) or after 4 rejected steps in a row
+  const int it32 = lm_phase<float>(P, lane, th, cost, lambda, max_iter, fmax(tol, 1e-6), c32, 4);
+  // FP64 phase with the caller's tolerance; restart the damping
   lambda = 1e-3;
   const int it64 =
       lm_phase<double>(P, lane, th, cost, lambda, max_iter - it32 > 8 ? max_iter - it32 : 8, tol, converged);
@@ -408,10 +419,7 @@ __device__ void plain_fit(const LmProblem& P, int lane, int nrefine, int max_ite
   converged = bconv;
 }
 
-__global__ void __launch_bounds__(32 * LM_WARPS) lm_kernel(LmParams p) {
-  const int lane = threadIdx.x & 31;
-  const int fit = blockIdx.x * LM_WARPS + (threadIdx.x >> 5);
-  if (fit >= p.nfit) return;  // whole warp
+__device__ __noinline__ void lm_one(const LmParams& p, int fit, int lane) {
   LmProblem P;
   P.nt = min(p.nt[fit], min(p.nt_max, LM_MAX_LAGS));
   P.K = min(p.K, LM_MAX_NODES);
@@ -480,10 +488,30 @@ __global__ void __launch_bounds__(32 * LM_WARPS) lm_kernel(LmParams p) {
   }
 }
 
+// Persistent: each warp takes the next fit from an atomic counter until all
+// are done, so fits of very different cost (a fallback, a slow valley) do
+// not hold a CTA's other warps.
+__global__ void __launch_bounds__(32 * LM_WARPS) lm_kernel(LmParams p) {
+  const int lane = threadIdx.x & 31;
+  for (;;) {
+    int fit = 0;
+    if (lane == 0) fit = atomicAdd(p.counter, 1);
+    fit = __shfl_sync(0xffffffffu, fit, 0);
+    if (fit >= p.nfit) return;  // whole warp
+    lm_one(p, fit, lane);
+  }
+}
+
+// p.counter: a device int set to 0 before the launch (stream-ordered).
 cudaError_t launch_lm(const LmParams& p, cudaStream_t s) {
   if (p.nfit <= 0) return cudaSuccess;
-  const int grid = (p.nfit + LM_WARPS - 1) / LM_WARPS;
-  lm_kernel<<<grid, 32 * LM_WARPS, 0, s>>>(p);
+  int dev = 0, sms = 0, per = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, lm_kernel, 32 * LM_WARPS, 0);
+  const int need = (p.nfit + LM_WARPS - 1) / LM_WARPS;
+  const int wave = sms * (per > 0 ? per : 1);
+  lm_kernel<<<need < wave ? need : wave, 32 * LM_WARPS, 0, s>>>(p);
   return cudaGetLastError();
 }
 
@@ -545,7 +573,12 @@ extern "C" int ddm_fit_lm(int32_t nfit, int32_t nt_max, int32_t K, const int32_t
   if (on_device) {
     p.nt = nt; p.d = d; p.tau = tau; p.qn = qn; p.w = w; p.bounds = bounds; p.start = start;
     p.theta = theta; p.cost = cost; p.iters = iters; p.evals = evals; p.status = status;
-    cudaError_t e = ddm::launch_lm(p, s);
+    int* ctr = nullptr;
+    cudaError_t e = cudaMallocAsync((void**)&ctr, sizeof(int), s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(ctr, 0, sizeof(int), s);
+    p.counter = ctr;
+    if (e == cudaSuccess) e = ddm::launch_lm(p, s);
+    if (ctr) cudaFreeAsync(ctr, s);
     if (e != cudaSuccess) return lm_fail(DDM_ERR_CUDA, "ddm_fit_lm: %s", cudaGetErrorString(e));
     return DDM_OK;
   }
@@ -567,9 +600,12 @@ extern "C" int ddm_fit_lm(int32_t nfit, int32_t nt_max, int32_t K, const int32_t
   step(stage_in<int>(&dit, nullptr, nf, s));
   step(stage_in<int>(&dev, nullptr, nf, s));
   step(stage_in<int>(&dst, nullptr, nf, s));
+  int* ctr = nullptr;
+  step(stage_in<int>(&ctr, nullptr, 1, s));
+  step(cudaMemsetAsync(ctr, 0, sizeof(int), s));
   if (e == cudaSuccess) {
     p.nt = dnt; p.d = dd; p.tau = dtau; p.qn = dqn; p.w = dw; p.bounds = db; p.start = ds;
-    p.theta = dth; p.cost = dc; p.iters = dit; p.evals = dev; p.status = dst;
+    p.theta = dth; p.cost = dc; p.iters = dit; p.evals = dev; p.status = dst; p.counter = ctr;
     step(ddm::launch_lm(p, s));
     step(cudaMemcpyAsync(theta, dth, sizeof(double) * nf * 6, cudaMemcpyDeviceToHost, s));
     step(cudaMemcpyAsync(cost, dc, sizeof(double) * nf, cudaMemcpyDeviceToHost, s));
@@ -578,7 +614,7 @@ extern "C" int ddm_fit_lm(int32_t nfit, int32_t nt_max, int32_t K, const int32_t
     if (status) step(cudaMemcpyAsync(status, dst, sizeof(int) * nf, cudaMemcpyDeviceToHost, s));
   }
   for (void* ptr : {(void*)dnt, (void*)dd, (void*)dtau, (void*)dqn, (void*)dw, (void*)db, (void*)ds,
-                    (void*)dth, (void*)dc, (void*)dit, (void*)dev, (void*)dst})
+                    (void*)dth, (void*)dc, (void*)dit, (void*)dev, (void*)dst, (void*)ctr})
     if (ptr) cudaFreeAsync(ptr, s);
   step(cudaStreamSynchronize(s));
   if (e != cudaSuccess) return lm_fail(DDM_ERR_CUDA, "ddm_fit_lm: %s", cudaGetErrorString(e));

@@ -178,8 +178,10 @@ def predict_starts(net, x, bnds):
 
 
 def compare_fits(net, data, bnds, max_iter=200, tol=1e-10, nrefine=3):
-    """Plain LM (reference starts) vs surrogate-seeded LM with fallback on the
-    same curves; device-timed with CUDA events on one stream."""
+    """Plain LM (reference starts), surrogate-seeded LM, and surrogate-seeded
+    LM with the plain strategy as fallback, on the same curves; each
+    device-timed with CUDA events on one stream (the seeded timings include
+    the surrogate's inference)."""
     import torch
     d = data["d"].contiguous()
     n, nt = d.shape
@@ -188,8 +190,9 @@ def compare_fits(net, data, bnds, max_iter=200, tol=1e-10, nrefine=3):
     w = (1.0 / d.max(1).values).contiguous()
     b6 = torch.from_numpy(np.tile(bnds, (n, 1))).cuda()
     ntv = torch.full((n,), nt, dtype=torch.int32, device="cuda")
+    predict_starts(net, data["x"][:8], bnds)  # first-call set-up outside the timed region
     res = {}
-    for name in ("plain", "surrogate"):
+    for name, mode in (("plain", "plain"), ("seeded", "seeded"), ("fallback", "seeded_fallback")):
         theta = torch.empty((n, 6), dtype=torch.float64, device="cuda")
         cost = torch.empty(n, dtype=torch.float64, device="cuda")
         iters = torch.empty(n, dtype=torch.int32, device="cuda")
@@ -199,27 +202,26 @@ def compare_fits(net, data, bnds, max_iter=200, tol=1e-10, nrefine=3):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
         e0.record(stream)
-        if name == "plain":
-            F.fit_lm_device(d, tau, qn, w, b6, ntv, theta, cost, iters, evals, status, mode="plain",
-                            max_iter=max_iter, tol=tol, nrefine=nrefine, stream=stream.cuda_stream)
-        else:
-            start = predict_starts(net, data["x"], bnds)
-            F.fit_lm_device(d, tau, qn, w, b6, ntv, theta, cost, iters, evals, status, mode="seeded_fallback",
-                            start=start, max_iter=max_iter, tol=tol, nrefine=nrefine, stream=stream.cuda_stream)
+        start = None if mode == "plain" else predict_starts(net, data["x"], bnds)
+        F.fit_lm_device(d, tau, qn, w, b6, ntv, theta, cost, iters, evals, status, mode=mode, start=start,
+                        max_iter=max_iter, tol=tol, nrefine=nrefine, stream=stream.cuda_stream)
         e1.record(stream)
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1)
         res[name] = dict(ms=ms, qfits_per_s=n / (ms / 1e3), theta=theta.cpu().numpy(), cost=cost.cpu().numpy(),
                          iters=iters.cpu().numpy(), evals=evals.cpu().numpy(), status=status.cpu().numpy())
-    p, s = res["plain"], res["surrogate"]
-    equal = s["cost"] <= p["cost"] * (1 + 1e-3) + 1e-30
-    summary = dict(n=n, plain_qfits_per_s=p["qfits_per_s"], surrogate_qfits_per_s=s["qfits_per_s"],
-                   speedup=s["qfits_per_s"] / p["qfits_per_s"],
-                   plain_mean_iters=float(p["iters"].mean()), surrogate_mean_iters=float(s["iters"].mean()),
-                   plain_mean_evals=float(p["evals"].mean()), surrogate_mean_evals=float(s["evals"].mean()),
-                   frac_equal_or_better=float(equal.mean()),
-                   frac_fallback=float(((s["status"] >> 1) & 1).mean()),
-                   median_cost_ratio=float(np.median(s["cost"] / np.maximum(p["cost"], 1e-300))))
+    p = res["plain"]
+    summary = dict(n=n, plain_qfits_per_s=p["qfits_per_s"], plain_mean_iters=float(p["iters"].mean()),
+                   plain_mean_evals=float(p["evals"].mean()))
+    for name in ("seeded", "fallback"):
+        r = res[name]
+        equal = r["cost"] <= p["cost"] * (1 + 1e-3) + 1e-30
+        summary.update({f"{name}_qfits_per_s": r["qfits_per_s"],
+                        f"{name}_speedup": r["qfits_per_s"] / p["qfits_per_s"],
+                        f"{name}_mean_iters": float(r["iters"].mean()),
+                        f"{name}_mean_evals": float(r["evals"].mean()),
+                        f"{name}_frac_equal_or_better": float(equal.mean()),
+                        f"{name}_frac_fallback": float(((r["status"] >> 1) & 1).mean())})
     return summary, res
 
 

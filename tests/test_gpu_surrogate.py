@@ -49,16 +49,21 @@ def test_seeded_fallback_recovers_from_bad_seeds():
     plain = F.fit_lm(d, tau, data["qn"], w, bnds, mode="plain")
     bad = np.tile([0.5, bnds[1] * 0.99, 90.0, bnds[4] * 1.01], (256, 1))  # far from every truth
     fb = F.fit_lm(d, tau, data["qn"], w, bnds, mode="seeded_fallback", start=bad)
-    assert ((fb.status >> 1) & 1).mean() > 0.2  # many seeds did not converge and fell back
+    assert ((fb.status >> 1) & 1).mean() > 0.05  # seeds whose LM hit the cap fell back
     assert (fb.cost <= plain.cost * (1 + 1e-3) + 1e-30).mean() >= 0.95
 
 
 def test_trained_surrogate_gains_over_plain_lm():
-    net = ST.build_and_train(n_analytic=1 << 16, epochs=6, seed=0, batch_max=8192)
-    held = ST.analytic_set(4096, seed=99)
-    summary, _ = ST.compare_fits(net, held, ST.swim_bounds(held["qn"]))
-    print(summary)
-    assert summary["frac_equal_or_better"] >= 0.9, summary
-    assert summary["speedup"] >= 2.0, summary
-    assert summary["surrogate_mean_evals"] < 0.5 * summary["plain_mean_evals"], summary
+    """Equal fit error = final cost within 1e-3 of the plain LM's (or lower)."""
+    net = ST.build_and_train(n_analytic=1 << 18, epochs=16, seed=0, batch_max=4096)
+    held = ST.analytic_set(8192, seed=99)
+    s, _ = ST.compare_fits(net, held, ST.swim_bounds(held["qn"]))
+    print(s)
+    # seeded alone: far fewer model evaluations and a large q-fits/s gain
+    assert s["seeded_frac_equal_or_better"] >= 0.98, s
+    assert s["seeded_mean_evals"] < 0.2 * s["plain_mean_evals"], s
+    assert s["seeded_speedup"] >= 4.0, s
+    # with the reference's starts as fallback: equal fit error on >= 99.5 %
+    assert s["fallback_frac_equal_or_better"] >= 0.995, s
+    assert s["fallback_speedup"] >= 1.5, s
     net.close()

@@ -459,7 +459,21 @@ __device__ __noinline__ void lm_one(const LmParams& p, int fit, int lane) {
     varpro(P, lane, th[2], th[3], th[4], th[5], th[0], th[1]);
     iters = lm_run(P, lane, th, cost, p.max_iter, p.tol, conv);
     evals = 2 + iters;
-    if (p.mode == LM_SEEDED_FALLBACK && !conv) {
+    bool bad = !conv;
+    if (p.mode == LM_SEEDED_FALLBACK && !bad) {
+      // The Brownian null (alpha = 0) is nested in the model, so no optimum
+      // costs more than the best Brownian fit: a seeded fit above a coarse
+      // 17-point Brownian scan (itself an upper bound of the Brownian
+      // optimum) sits in a wrong basin.
+      double A, B, bmin = 1e308;
+      for (int i = 0; i <= 16; i++) {
+        const double x = P.lo[5] + ((P.hi[5] - P.lo[5]) * i) / 16;
+        bmin = fmin(bmin, varpro(P, lane, 0.0, P.lo[3], 0.0, x, A, B));
+      }
+      evals += 17;
+      bad = cost > bmin;
+    }
+    if (p.mode == LM_SEEDED_FALLBACK && bad) {
       // the seed did not lead to a converged fit: the reference's start
       // strategy decides, and the lower cost wins
       double t2[LM_NP], c2;

@@ -165,8 +165,10 @@ int64_t ddm_kernel_launches(const ddm_engine *h);
  *   mode 1: LM from start[4*i..] = (alpha, vbar, Z, D) (e.g. the surrogate's
  *           prediction), amplitudes from VarPro.
  *   mode 2: as mode 1; a fit whose LM did not converge (stopped at
- *           max_iter) also runs mode 0 and keeps the lower cost (the
- *           reference's starts as the fallback).
+ *           max_iter) or whose cost exceeds a coarse 17-point Brownian
+ *           (alpha = 0) scan -- impossible at a global optimum, since the
+ *           Brownian model is nested -- also runs mode 0 and keeps the lower
+ *           cost (the reference's starts as the fallback).
  * Arrays: nt[nfit] lags per fit (<= nt_max <= 128), d and tau [nfit][nt_max],
  * qn [nfit][K] (K <= 8), w[nfit], bounds [nfit][6], start [nfit][4];
  * out theta [nfit][6], cost[nfit], iters/evals/status [nfit] (may be NULL;

@@ -13,6 +13,14 @@ analyzeRadial, motility-ddm/src/ddm_ref.js:196-206, 425-437).
 Under torchrun each rank analyses its own video (weak scaling, no collective
 on the data path).
 
+  fit    (rank 0) q-fits/s of the batched GPU LM on 10^5 held-out q-curves:
+         plain (the reference's start strategy), seeded by the tensor-core
+         surrogate (trained in the run on 2^19 analytic curves + the engine's
+         own radial curves of 48 seeded videos), and seeded with the plain
+         strategy as fallback; fit error as the share of curves whose cost is
+         within 1e-3 of the plain LM's, and agreement with the FP64 LM oracle
+         on a bounded sample.
+
 --impl reference times the reference's CPU algorithm on the host cores: the
 reference is JavaScript with no runtime on this machine, so its FP64 C
 restatement (oracle/, test infrastructure) stands in, on a bounded sample.
@@ -67,7 +75,7 @@ class ClockSampler:
     def start(self):
         try:
             self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits", "-lms", "200",
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits", "-lms", "20",
                  "-i", str(self.index)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -76,7 +84,12 @@ class ClockSampler:
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.perf_counter(), line.strip()))
+
+    def mark(self, t0, t1):
+        """Host-time window of the timed region (samples outside are dropped
+        unless none fall inside)."""
+        self.window = (t0, t1)
 
     def stop(self):
         if not self.proc:
@@ -88,7 +101,9 @@ class ClockSampler:
             self.proc.kill()
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        w = getattr(self, "window", None)
+        inside = [ln for t, ln in self.lines if w and w[0] <= t <= w[1]]
+        for ln in inside or [ln for _, ln in self.lines]:
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 9:
                 continue
@@ -103,7 +118,7 @@ class ClockSampler:
         if not sm:
             return None
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "samples_inside_timed_region": len(inside)}
 
 
 def _profile_traffic():
@@ -154,6 +169,46 @@ def cpu_baseline(frames_u16, valid, sample_frames=24, sample_modes=6144, threads
                       f"modes of the TPAD={TPAD} masked WK, FP64, scaled to the {T}-frame video"}
 
 
+def fit_benchmark(n_eval=100000, n_train=1 << 19, n_videos=48, epochs=8, oracle_sample=256):
+    """q-fits/s of the batched LM on held-out q-curves: plain (the reference's
+    start strategy), surrogate-seeded, and surrogate-seeded with the plain
+    strategy as fallback; the surrogate trained here on the GPU (analytic
+    curves + the engine's own radial curves of seeded videos). Fit error:
+    share of curves whose cost is within 1e-3 of the plain LM's (or lower),
+    and, on a bounded sample, cost and parameter agreement with the FP64 LM
+    oracle (reference start strategy, on the host)."""
+    import torch
+    from hackathon_b200 import surrogate_train as ST
+    t0 = time.perf_counter()
+    net = ST.build_and_train(n_analytic=n_train, n_videos=n_videos, epochs=epochs, seed=0, batch_max=8192)
+    t_train = time.perf_counter() - t0
+    held = ST.analytic_set(n_eval, seed=12345)
+    bnds = ST.swim_bounds(held["qn"])
+    summary, res = ST.compare_fits(net, held, bnds)
+    # FP64 oracle on a bounded sample (host)
+    import oracle as O
+    d = held["d"].cpu().numpy().astype(np.float64)
+    tau = ST.lm_tau().astype(np.float64)
+    idx = np.arange(0, n_eval, n_eval // oracle_sample)[:oracle_sample]
+    t1 = time.perf_counter()
+    oc = np.array([O.lm_fit_plain(d[i], tau, held["qn"][i].astype(np.float64), 1 / d[i].max(),
+                                  bnds.astype(np.float64))[1] for i in idx])
+    t_or = time.perf_counter() - t1
+    fb = res["fallback"]
+    summary.update({
+        "train_curves": int(n_train), "train_videos": int(n_videos), "train_s": t_train,
+        "oracle_sample": int(len(idx)), "oracle_qfits_per_s_1core": len(idx) / t_or,
+        # equal fit error: cost within 1e-3 of the FP64 oracle's, or lower
+        "fallback_frac_equal_or_better_than_fp64_oracle": float((fb["cost"][idx] <= oc * (1 + 1e-3)).mean()),
+        "seeded_frac_equal_or_better_than_fp64_oracle": float(
+            (res["seeded"]["cost"][idx] <= oc * (1 + 1e-3)).mean()),
+        "plain_frac_cost_within_1e-3_of_fp64_oracle": float(
+            (np.abs(res["plain"]["cost"][idx] - oc) <= 1e-3 * oc).mean())})
+    net.close()
+    torch.cuda.synchronize()
+    return summary
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -185,11 +240,12 @@ def run_reference(args, rank, world):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-fit", action="store_true", help="skip the q-fits/s (surrogate + LM) section")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", 0))
@@ -241,12 +297,14 @@ def main():
         dist.barrier()
     clocks = ClockSampler(local)
     clocks.start()
+    time.sleep(0.3)  # sampler running before the timed region
     l0 = eng.kernel_launches
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
            torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     torch.cuda.synchronize()
     start = torch.cuda.Event(enable_timing=True)
     end = torch.cuda.Event(enable_timing=True)
+    h0 = time.perf_counter()
     start.record(stream)
     for i in range(args.steps):
         ev[i][0].record(stream)
@@ -256,6 +314,7 @@ def main():
         ev[i][2].record(stream)
     end.record(stream)
     torch.cuda.synchronize()
+    clocks.mark(h0, time.perf_counter())
     if dist:
         dist.barrier()
     launches = eng.kernel_launches - l0
@@ -328,6 +387,10 @@ def main():
             "pipeline_frac": (sp_bytes + tm_bytes) / (ms_step * 1e6) / peak,
             "stages": stages}
 
+    fit = None
+    if rank == 0 and not args.no_fit:
+        fit = fit_benchmark()
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         fr = frames.view(torch.int16).cpu().numpy().view(np.uint16)
@@ -347,7 +410,8 @@ def main():
                 "roofline": roof,
                 "clocks": clk,
                 "cpu_baseline": cpu,
-                "binned_modes": nbinned}
+                "binned_modes": nbinned,
+                "fit": fit}
         print(json.dumps(line), flush=True)
     eng.destroy()
     if dist:

@@ -268,8 +268,9 @@ def main():
     import hackathon_b200 as H
     from hackathon_b200 import synth
 
+    from hackathon_b200 import replicas as R
     torch.cuda.set_device(local)
-    spec = synth.config2(seed=1 + rank)
+    spec = synth.config2(seed=R.rank_seed(1, rank))
     frames, valid, truth = synth.generate(spec)
     mask_roi = synth.roi_mask(spec)
     slots = np.arange(T, dtype=np.int32)
@@ -322,12 +323,9 @@ def main():
     ms = start.elapsed_time(end)
     t_sp = statistics.mean(a.elapsed_time(b) for a, b, _ in ev)
     t_tm = statistics.mean(b.elapsed_time(c) for _, b, c in ev)
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = R.max_over_ranks(ms, dist, device="cuda")
     ms_step = ms / args.steps
-    value = world * T / (ms_step / 1e3)
+    value = R.weak_scaling_throughput(T, ms_step, world)
 
     # ---------------- e2e: pinned host frames through the C ABI
     host = frames.view(torch.int16).cpu().pin_memory()
@@ -350,11 +348,8 @@ def main():
     e1.record(stream)
     torch.cuda.synchronize()
     ms_e2e = e0.elapsed_time(e1)
-    if dist:
-        t = torch.tensor([ms_e2e], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_e2e = float(t.item())
-    e2e = world * T * args.e2e_steps / (ms_e2e / 1e3)
+    ms_e2e = R.max_over_ranks(ms_e2e, dist, device="cuda")
+    e2e = R.weak_scaling_throughput(T * args.e2e_steps, ms_e2e, world)
 
     # ---------------- roofline of the dominant stage
     peak, peak_kind = _peaks()

@@ -48,6 +48,16 @@ _SIGS = {
     "ddm_fit_lm": (C.c_int, [_i32, _i32, _i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i32, _i32,
                              C.c_double, _i32, _vp, _vp, _vp, _vp, _vp, _i32, _vp]),
     "ddm_model_curves": (C.c_int, [_i32, _i32, _vp, _vp, _i32, _vp, C.c_float, C.c_uint64, _vp, _vp, _vp]),
+    "ddm_batch_create": (C.c_int, [_vp, _i32, C.POINTER(_vp)]),
+    "ddm_batch_destroy": (None, [_vp]),
+    "ddm_batch_last_error": (C.c_char_p, [_vp]),
+    "ddm_batch_set_stream": (C.c_int, [_vp, _vp]),
+    "ddm_batch_ingest": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
+    "ddm_batch_compute_temporal": (C.c_int, [_vp, _vp, _vp]),
+    "ddm_batch_enqueue_temporal": (C.c_int, [_vp]),
+    "ddm_batch_sync": (C.c_int, [_vp]),
+    "ddm_batch_capture": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
+    "ddm_batch_launch_graph": (C.c_int, [_vp]),
     "ddm_mlp_create": (C.c_int, [_i32, C.c_uint64, C.POINTER(_vp)]),
     "ddm_mlp_destroy": (None, [_vp]),
     "ddm_mlp_last_error": (C.c_char_p, [_vp]),

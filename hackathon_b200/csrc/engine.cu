@@ -53,6 +53,7 @@ struct ddm_engine {
   void *d_stage[NSTAGE]{};             // device staging for host frames
   size_t stage_bytes = 0;
   double scale_last = 1.0;
+  bool wys_ready = false;              // d_wys holds w(y) * scale_last
   int last_mean_index = -1;
   bool have_frames = false;
 
@@ -64,6 +65,7 @@ struct ddm_engine {
   size_t meta_bytes = 0;
   int4 *d_items = nullptr;             // bin-sorted (mode, kx, ky, bin)
   int4 *d_units = nullptr;             // fused-path units
+  std::vector<int4> h_units;           // host copy (batched launches concatenate them)
   int nunits = 0;
   int *d_bin_units = nullptr;          // [NB+1]
   uint32_t *d_offsets = nullptr, *d_nmodes = nullptr;
@@ -158,6 +160,7 @@ static int build_units(ddm_engine *h) {
   }
   bin_units[NB] = (int)units.size();
   h->nunits = (int)units.size();
+  h->h_units = units;
   std::vector<int4> items(std::max(total, 1));
   for (int i = 0; i < total; i++) {
     const int32_t *m = &h->bins.modes[4 * (size_t)i];
@@ -458,7 +461,7 @@ static int launch_chunk(ddm_engine *h, const void *dframes, int dtype, int n, co
 
 static int set_scale(ddm_engine *h, float scale) {
   if (!(scale > 0) || !std::isfinite(scale)) return fail(h, DDM_ERR_ARG, "scale must be finite and > 0");
-  if ((double)scale == h->scale_last && h->have_frames) return DDM_OK;
+  if ((double)scale == h->scale_last && h->wys_ready) return DDM_OK;
   const int N = h->g.N;
   const std::vector<double> w = blackman_harris(N);
   std::vector<float> wys(N);
@@ -467,6 +470,7 @@ static int set_scale(ddm_engine *h, float scale) {
   CK(cudaStreamSynchronize(h->stream));
   CK(cudaMemcpy(h->d_wys, wys.data(), sizeof(float) * N, cudaMemcpyHostToDevice));
   h->scale_last = scale;
+  h->wys_ready = true;
   return DDM_OK;
 }
 
@@ -752,4 +756,331 @@ extern "C" int ddm_idle(ddm_engine *h) {
   CK(cudaStreamSynchronize(h->stream));
   prune_inflight(h);
   return check_device_error(h);
+}
+
+// ================================================================== batches
+//
+// Many videos (engines of any geometry on one device) analysed together:
+// every engine's spatial chunks are queued on the batch stream without host
+// synchronisation, and the temporal analysis of ALL videos is one persistent
+// launch over the concatenated units of every engine (units carry their
+// video index; per-video descriptors hold the history, order, mask, N(tau),
+// mask spectrum and partials). The launch uses the largest TPAD of the
+// batch: zero padding beyond T + L - 1 leaves every lag < L exact, so each
+// video's radial record equals its own engine's. Each video's unit partials
+// are then reduced by its engine's reduce kernel. The whole step can be
+// captured once into a CUDA graph and replayed.
+
+struct ddm_batch {
+  std::vector<ddm_engine *> e;
+  int device = 0;
+  int TPAD = 0, Tmax = 0, Lmax = 0, nunits = 0;
+  cudaStream_t own = nullptr, stream = nullptr;
+  VideoDesc *d_videos = nullptr;
+  int4 *d_units = nullptr;
+  float2 *d_tw = nullptr;
+  float2 *d_mspec = nullptr;           // [n][TPAD]
+  float *d_npairs = nullptr;           // [n][Lmax]
+  uint32_t *d_order = nullptr;         // [n][Tmax]
+  float *d_mask = nullptr;             // [n][Tmax]
+  char *h_meta = nullptr;              // pinned: order, mask, npairs, mspec of every video
+  size_t meta_bytes = 0;
+  int *d_counter = nullptr, *d_err = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  std::string err;
+};
+
+static int bfail(ddm_batch *b, int code, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  if (b)
+    b->err = buf;
+  else
+    g_create_error = buf;
+  return code;
+}
+
+#define BCK(x)                                                                                \
+  do {                                                                                        \
+    cudaError_t e_ = (x);                                                                     \
+    if (e_ != cudaSuccess) return bfail(b, DDM_ERR_CUDA, "%s: %s", #x, cudaGetErrorString(e_)); \
+  } while (0)
+
+static void batch_release(ddm_batch *b) {
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  for (void *p : {(void *)b->d_videos, (void *)b->d_units, (void *)b->d_tw, (void *)b->d_mspec,
+                  (void *)b->d_npairs, (void *)b->d_order, (void *)b->d_mask, (void *)b->d_counter,
+                  (void *)b->d_err})
+    if (p) cudaFree(p);
+  if (b->h_meta) cudaFreeHost(b->h_meta);
+  if (b->own) cudaStreamDestroy(b->own);
+}
+
+extern "C" const char *ddm_batch_last_error(const ddm_batch *b) { return b ? b->err.c_str() : g_create_error.c_str(); }
+
+extern "C" int ddm_batch_create(ddm_engine *const *engines, int32_t n, ddm_batch **out) {
+  g_create_error.clear();
+  if (!out || !engines || n < 1) return bfail(nullptr, DDM_ERR_ARG, "ddm_batch_create: need n >= 1 engines");
+  *out = nullptr;
+  for (int i = 0; i < n; i++)
+    if (!engines[i]) return bfail(nullptr, DDM_ERR_ARG, "ddm_batch_create: engine %d is NULL", i);
+  ddm_batch *b = new ddm_batch();
+  b->e.assign(engines, engines + n);
+  b->device = engines[0]->device;
+  for (auto *h : b->e) {
+    if (h->device != b->device) {
+      delete b;
+      return bfail(nullptr, DDM_ERR_ARG, "ddm_batch_create: engines on different devices");
+    }
+    b->TPAD = std::max(b->TPAD, h->g.TPAD);
+    b->Tmax = std::max(b->Tmax, h->g.T);
+    b->Lmax = std::max(b->Lmax, h->g.L);
+  }
+  cudaSetDevice(b->device);
+  std::vector<VideoDesc> vids(n);
+  std::vector<int4> units;
+  for (int i = 0; i < n; i++) {
+    ddm_engine *h = b->e[i];
+    VideoDesc &v = vids[i];
+    v.hist = h->d_hist;
+    v.items = h->d_items;
+    v.partials = h->d_partials;
+    v.T = h->g.T;
+    v.L = h->g.L;
+    v.unit0 = (int)units.size();
+    v.nunits = h->nunits;
+    for (int4 u : h->h_units) units.push_back(make_int4(u.x, u.y, u.z, i));
+  }
+  b->nunits = (int)units.size();
+  b->meta_bytes = (size_t)n * (sizeof(uint32_t) * b->Tmax + sizeof(float) * b->Tmax + sizeof(float) * b->Lmax +
+                               sizeof(float2) * b->TPAD);
+  const std::vector<float> tw = twiddle_table(b->TPAD);
+  bool ok = cudaStreamCreateWithFlags(&b->own, cudaStreamNonBlocking) == cudaSuccess;
+  b->stream = b->own;
+  auto al = [&](void **p, size_t bytes) { ok = ok && cudaMalloc(p, bytes ? bytes : 1) == cudaSuccess; };
+  al((void **)&b->d_videos, sizeof(VideoDesc) * n);
+  al((void **)&b->d_units, sizeof(int4) * units.size());
+  al((void **)&b->d_tw, sizeof(float) * tw.size());
+  al((void **)&b->d_mspec, sizeof(float2) * n * (size_t)b->TPAD);
+  al((void **)&b->d_npairs, sizeof(float) * n * (size_t)b->Lmax);
+  al((void **)&b->d_order, sizeof(uint32_t) * n * (size_t)b->Tmax);
+  al((void **)&b->d_mask, sizeof(float) * n * (size_t)b->Tmax);
+  al((void **)&b->d_counter, sizeof(int));
+  al((void **)&b->d_err, sizeof(int));
+  ok = ok && cudaHostAlloc((void **)&b->h_meta, b->meta_bytes, cudaHostAllocDefault) == cudaSuccess;
+  if (ok) {
+    for (int i = 0; i < n; i++) {
+      vids[i].order = b->d_order + (size_t)i * b->Tmax;
+      vids[i].mask = b->d_mask + (size_t)i * b->Tmax;
+      vids[i].npairs = b->d_npairs + (size_t)i * b->Lmax;
+      vids[i].mspec = b->d_mspec + (size_t)i * b->TPAD;
+    }
+    ok = cudaMemcpy(b->d_videos, vids.data(), sizeof(VideoDesc) * n, cudaMemcpyHostToDevice) == cudaSuccess &&
+         (units.empty() ||
+          cudaMemcpy(b->d_units, units.data(), sizeof(int4) * units.size(), cudaMemcpyHostToDevice) == cudaSuccess) &&
+         cudaMemcpy(b->d_tw, tw.data(), sizeof(float) * tw.size(), cudaMemcpyHostToDevice) == cudaSuccess &&
+         cudaMemset(b->d_err, 0, sizeof(int)) == cudaSuccess;
+  }
+  if (!ok) {
+    batch_release(b);
+    delete b;
+    return bfail(nullptr, DDM_ERR_NOMEM, "ddm_batch_create: device allocation or upload failed");
+  }
+  *out = b;
+  return DDM_OK;
+}
+
+extern "C" void ddm_batch_destroy(ddm_batch *b) {
+  if (!b) return;
+  cudaSetDevice(b->device);
+  cudaStreamSynchronize(b->stream);
+  batch_release(b);
+  delete b;
+}
+
+extern "C" int ddm_batch_set_stream(ddm_batch *b, void *stream) {
+  if (!b) return DDM_ERR_ARG;
+  b->stream = stream ? (cudaStream_t)stream : b->own;
+  return DDM_OK;
+}
+
+// Spatial stage of every video from DEVICE frames, queued on the batch
+// stream with no host synchronisation (capturable). frames[i]: n[i] frames of
+// engine i's N*N pixels of dtypes[i] (16-byte aligned), slots[i][n[i]], scale
+// per video. A scale differing from the engine's last one is uploaded first
+// (a host synchronisation: set scales before capturing).
+extern "C" int ddm_batch_ingest(ddm_batch *b, const void *const *frames, const int32_t *dtypes,
+                                const int32_t *n, const int32_t *const *slots, const float *scales) {
+  if (!b || !frames || !dtypes || !n || !slots || !scales) return bfail(b, DDM_ERR_ARG, "null argument");
+  cudaSetDevice(b->device);
+  for (size_t i = 0; i < b->e.size(); i++) {
+    ddm_engine *h = b->e[i];
+    if (n[i] == 0) continue;
+    int rc = check_frames_args(h, frames[i], dtypes[i], n[i], slots[i]);
+    if (rc) return bfail(b, rc, "video %zu: %s", i, h->err.c_str());
+    if ((uintptr_t)frames[i] & 15) return bfail(b, DDM_ERR_ARG, "video %zu: frames must be 16-byte aligned", i);
+    if ((rc = set_scale(h, scales[i]))) return bfail(b, rc, "video %zu: %s", i, h->err.c_str());
+    cudaStream_t keep = h->stream;
+    h->stream = b->stream;
+    const size_t fbytes = (size_t)h->g.N * h->g.N * dtype_size(dtypes[i]);
+    for (int c0 = 0; c0 < n[i] && !rc; c0 += h->chunk) {
+      const int m = std::min(h->chunk, n[i] - c0);
+      rc = launch_chunk(h, (const char *)frames[i] + (size_t)c0 * fbytes, dtypes[i], m, slots[i] + c0, scales[i]);
+    }
+    h->stream = keep;
+    if (rc) return bfail(b, rc, "video %zu: %s", i, h->err.c_str());
+    h->radial_valid = false;
+  }
+  return DDM_OK;
+}
+
+extern "C" int ddm_batch_enqueue_temporal(ddm_batch *b);
+
+// Temporal analysis of every video in ONE launch; orders[i], masks[i] of
+// length T_i. Queued on the batch stream (no host synchronisation; the meta
+// tables are computed on the host and copied from pinned memory in order).
+extern "C" int ddm_batch_compute_temporal(ddm_batch *b, const uint32_t *const *orders, const float *const *masks) {
+  if (!b || !orders || !masks) return bfail(b, DDM_ERR_ARG, "null argument");
+  cudaSetDevice(b->device);
+  const int nv = (int)b->e.size();
+  uint32_t *ho = (uint32_t *)b->h_meta;
+  float *hm = (float *)(ho + (size_t)nv * b->Tmax);
+  float *hn = hm + (size_t)nv * b->Tmax;
+  float *hs = hn + (size_t)nv * b->Lmax;
+  // the pinned tables may still be read by the previous call's copies
+  BCK(cudaStreamSynchronize(b->stream));
+  for (int i = 0; i < nv; i++) {
+    ddm_engine *h = b->e[i];
+    const int T = h->g.T, L = h->g.L;
+    if (!orders[i] || !masks[i]) return bfail(b, DDM_ERR_ARG, "video %d: order/mask is NULL", i);
+    for (int j = 0; j < T; j++)
+      if (orders[i][j] >= (uint32_t)T) return bfail(b, DDM_ERR_ARG, "video %d: order[%d] >= T", i, j);
+    std::vector<float> npairs, mspec;
+    temporal_meta(masks[i], T, b->TPAD, L, npairs, mspec);
+    memcpy(ho + (size_t)i * b->Tmax, orders[i], sizeof(uint32_t) * T);
+    for (int j = 0; j < T; j++) hm[(size_t)i * b->Tmax + j] = masks[i][j] != 0.f ? 1.f : 0.f;
+    memcpy(hn + (size_t)i * b->Lmax, npairs.data(), sizeof(float) * L);
+    memcpy(hs + (size_t)i * 2 * b->TPAD, mspec.data(), sizeof(float) * 2 * b->TPAD);
+  }
+  return ddm_batch_enqueue_temporal(b);
+}
+
+// The device part of ddm_batch_compute_temporal, from the pinned tables as
+// they are when it runs (a graph replay re-reads them).
+extern "C" int ddm_batch_enqueue_temporal(ddm_batch *b) {
+  if (!b) return DDM_ERR_ARG;
+  const int nv = (int)b->e.size();
+  // pinned layout: order [n][Tmax], mask [n][Tmax], npairs [n][Lmax], mspec [n][TPAD]
+  const char *hp = b->h_meta;
+  BCK(cudaMemcpyAsync(b->d_order, hp, sizeof(uint32_t) * nv * (size_t)b->Tmax, cudaMemcpyHostToDevice, b->stream));
+  BCK(cudaMemcpyAsync(b->d_mask, hp + sizeof(uint32_t) * nv * (size_t)b->Tmax, sizeof(float) * nv * (size_t)b->Tmax,
+                      cudaMemcpyHostToDevice, b->stream));
+  hp += (sizeof(uint32_t) + sizeof(float)) * nv * (size_t)b->Tmax;
+  BCK(cudaMemcpyAsync(b->d_npairs, hp, sizeof(float) * nv * (size_t)b->Lmax, cudaMemcpyHostToDevice, b->stream));
+  hp += sizeof(float) * nv * (size_t)b->Lmax;
+  BCK(cudaMemcpyAsync(b->d_mspec, hp, sizeof(float2) * nv * (size_t)b->TPAD, cudaMemcpyHostToDevice, b->stream));
+  TemporalParams tp{};
+  tp.tw = b->d_tw;
+  tp.units = b->d_units;
+  tp.nunits = b->nunits;
+  tp.unit_counter = b->d_counter;
+  tp.err = b->d_err;
+  tp.T = b->Tmax;
+  tp.L = b->Lmax;
+  tp.videos = b->d_videos;
+  BCK(cudaMemsetAsync(b->d_counter, 0, sizeof(int), b->stream));
+  if (b->nunits > 0) {
+    const int grid = std::min(temporal_max_grid(b->TPAD, b->Tmax, b->Lmax, false), b->nunits);
+    BCK(launch_temporal(b->TPAD, b->Lmax, false, tp, std::max(grid, 1), b->stream));
+  }
+  for (ddm_engine *h : b->e) {
+    ReduceParams rp{};
+    rp.partials = h->d_partials;
+    rp.bin_units = h->d_bin_units;
+    rp.nmodes = h->d_nmodes;
+    rp.nunits = h->nunits;
+    rp.NB = h->g.NB;
+    rp.L = h->g.L;
+    rp.D = h->d_radD;
+    rp.P = h->d_radP;
+    rp.drift = h->d_radDrift;
+    BCK(launch_reduce(rp, b->stream));
+    h->radial_valid = true;
+    h->full_valid = false;
+  }
+  return DDM_OK;
+}
+
+// Waits for the batch stream and surfaces device-side error words.
+extern "C" int ddm_batch_sync(ddm_batch *b) {
+  if (!b) return DDM_ERR_ARG;
+  cudaSetDevice(b->device);
+  BCK(cudaStreamSynchronize(b->stream));
+  int e = 0;
+  BCK(cudaMemcpy(&e, b->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  for (ddm_engine *h : b->e) {
+    int he = 0;
+    BCK(cudaMemcpy(&he, h->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (he) cudaMemset(h->d_err, 0, sizeof(int));
+    e |= he;
+  }
+  if (e) {
+    cudaMemset(b->d_err, 0, sizeof(int));
+    return bfail(b, DDM_ERR_CUDA, "a staged copy did not complete in time (code %d)", e);
+  }
+  return DDM_OK;
+}
+
+// Captures one full step -- ddm_batch_ingest of the given device frames and
+// the temporal launch -- into a CUDA graph (replaces any earlier one). The
+// meta tables are read from the pinned buffer at replay time: call
+// ddm_batch_compute_temporal once before capturing (it fills them), and
+// again with new orders/masks to refresh them before a replay.
+extern "C" int ddm_batch_capture(ddm_batch *b, const void *const *frames, const int32_t *dtypes,
+                                 const int32_t *n, const int32_t *const *slots, const float *scales) {
+  if (!b) return DDM_ERR_ARG;
+  cudaSetDevice(b->device);
+  // scales must be in place before capture (their upload synchronises)
+  for (size_t i = 0; i < b->e.size(); i++) {
+    int rc = set_scale(b->e[i], scales[i]);
+    if (rc) return bfail(b, rc, "video %zu: %s", i, b->e[i]->err.c_str());
+  }
+  BCK(cudaStreamSynchronize(b->stream));
+  if (b->exec) {
+    cudaGraphExecDestroy(b->exec);
+    b->exec = nullptr;
+  }
+  if (b->graph) {
+    cudaGraphDestroy(b->graph);
+    b->graph = nullptr;
+  }
+  BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+  int rc = ddm_batch_ingest(b, frames, dtypes, n, slots, scales);
+  if (!rc) rc = ddm_batch_enqueue_temporal(b);
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+  if (rc) {
+    if (g) cudaGraphDestroy(g);
+    return rc;
+  }
+  if (e != cudaSuccess) return bfail(b, DDM_ERR_CUDA, "stream capture: %s", cudaGetErrorString(e));
+  b->graph = g;
+  BCK(cudaGraphInstantiate(&b->exec, g, 0));
+  return DDM_OK;
+}
+
+extern "C" int ddm_batch_launch_graph(ddm_batch *b) {
+  if (!b || !b->exec) return bfail(b, DDM_ERR_STATE, "no captured graph");
+  cudaSetDevice(b->device);
+  BCK(cudaGraphLaunch(b->exec, b->stream));
+  for (ddm_engine *h : b->e) {
+    h->radial_valid = true;
+    h->full_valid = false;
+  }
+  return DDM_OK;
 }

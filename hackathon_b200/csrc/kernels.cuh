@@ -41,6 +41,18 @@ struct ColParams {
   int* err;                // error word (bounded waits that timed out), or nullptr
 };
 
+// One video of a batched temporal launch (units carry the video index in .w).
+struct VideoDesc {
+  const float2* hist;      // [modes][T]
+  const uint32_t* order;   // [T]
+  const float* mask;       // [T]
+  const float* npairs;     // [L]
+  const float2* mspec;     // [TPAD of the launch]
+  const int4* items;       // bin-sorted (mode, kx, ky, bin)
+  double* partials;        // [nunits][PFIELDS][L] + P at [nunits*PFIELDS*L + u]
+  int T, L, unit0, nunits; // unit0: first global unit of this video
+};
+
 struct TemporalParams {
   const float2* hist;      // [modes][T]
   const uint32_t* order;   // [T]
@@ -57,7 +69,8 @@ struct TemporalParams {
   float2* outC;            // [modes][L]
   float* outP;             // [modes]
   int* err;                // error word (bounded waits that timed out)
-  int T, L;
+  int T, L;                // single video; batched: the largest T and L
+  const VideoDesc* videos; // nullptr: one video (the fields above); else units[u].w indexes it
 };
 
 struct ReduceParams {

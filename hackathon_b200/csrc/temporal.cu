@@ -94,18 +94,38 @@ struct TemporalBounds {
   static constexpr int MIN_BLOCKS = NT >= 512 ? 1 : 512 / NT;
 };
 
-// Thread 0: stage the time series of pair k of `unit` into staging buffer b.
-__device__ __forceinline__ void issue_pair(const TemporalParams& p, int unit, int k, float2* stage,
+// The video a unit belongs to (batched launches) or the single video.
+__device__ __forceinline__ VideoDesc video_of(const TemporalParams& p, int vi) {
+  if (p.videos) return p.videos[vi];
+  VideoDesc v;
+  v.hist = p.hist;
+  v.order = p.order;
+  v.mask = p.mask;
+  v.npairs = p.npairs;
+  v.mspec = p.mspec;
+  v.items = p.items;
+  v.partials = p.partials;
+  v.T = p.T;
+  v.L = p.L;
+  v.unit0 = 0;
+  v.nunits = p.nunits;
+  return v;
+}
+
+// Thread 0: stage the time series of pair k of `unit` into staging buffer
+// `stage` (rows Tstride apart).
+__device__ __forceinline__ void issue_pair(const TemporalParams& p, int unit, int k, float2* stage, int Tstride,
                                            uint64_t* bar) {
   const int4 U = p.units[unit];
+  const VideoDesc v = video_of(p, p.videos ? U.w : 0);
   const bool hasb = k + 1 < U.y;
-  const int ma = load_item(p.items, U.x + k).x;
-  const uint32_t bytes = (uint32_t)p.T * sizeof(float2);
+  const int ma = load_item(v.items, U.x + k).x;
+  const uint32_t bytes = (uint32_t)v.T * sizeof(float2);
   mbar_arrive_expect_tx(bar, hasb ? 2 * bytes : bytes);
-  bulk_g2s(stage, p.hist + (size_t)ma * p.T, bytes, bar);
+  bulk_g2s(stage, v.hist + (size_t)ma * v.T, bytes, bar);
   if (hasb) {
-    const int mb = load_item(p.items, U.x + k + 1).x;
-    bulk_g2s(stage + p.T, p.hist + (size_t)mb * p.T, bytes, bar);
+    const int mb = load_item(v.items, U.x + k + 1).x;
+    bulk_g2s(stage + Tstride, v.hist + (size_t)mb * v.T, bytes, bar);
   }
 }
 
@@ -122,23 +142,32 @@ __global__ void __launch_bounds__(NP / 8, TemporalBounds<NP>::MIN_BLOCKS)
   __shared__ __align__(8) uint64_t mbar[2];
   __shared__ int s_next;
   const int t = threadIdx.x;
-  const int T = p.T, L = p.L;
-  float2* stage = sm + 3 * PN;        // [2 buffers][2 rows][T]
-  float2* s_tw = stage + 4 * T;       // per-stage twiddle blocks
+  const int TS = p.T;                 // staging stride: the (largest) T
+  float2* stage = sm + 3 * PN;        // [2 buffers][2 rows][TS]
+  float2* s_tw = stage + 4 * TS;      // per-stage twiddle blocks
   float* s_np = (float*)(s_tw + tw_size(NP));  // N(tau), tau < L
-  const float np0 = p.npairs[0];
   const float invn = 0.5f / NP;
   for (int i = t; i < tw_size(NP); i += NT) s_tw[i] = p.tw[i];
-  for (int i = t; i < L; i += NT) s_np[i] = p.npairs[i];
 
+  // per-video state, (re)loaded when a unit of another video comes up
+  VideoDesc vd;
+  int cur_v = -1, L = 0;
+  float np0 = 0.f;
   uint32_t ord[4];
   float msk[4];
+  auto load_video = [&](int vi) {
+    vd = video_of(p, vi);
+    cur_v = vi;
+    L = vd.L;
+    np0 = vd.npairs[0];
+    for (int i = t; i < L; i += NT) s_np[i] = vd.npairs[i];
 #pragma unroll
-  for (int q = 0; q < 4; q++) {
-    const int i = t + q * NT;
-    ord[q] = i < T ? __ldg(&p.order[i]) : 0u;
-    msk[q] = i < T ? __ldg(&p.mask[i]) : 0.f;
-  }
+    for (int q = 0; q < 4; q++) {
+      const int i = t + q * NT;
+      ord[q] = i < vd.T ? __ldg(&vd.order[i]) : 0u;
+      msk[q] = i < vd.T ? __ldg(&vd.mask[i]) : 0.f;
+    }
+  };
   if (t == 0) {
     mbar_init(&mbar[0], 1);
     mbar_init(&mbar[1], 1);
@@ -150,7 +179,7 @@ __global__ void __launch_bounds__(NP / 8, TemporalBounds<NP>::MIN_BLOCKS)
   __syncthreads();
   if (t == 0) {
     s_next = atomicAdd(p.unit_counter, 1);
-    if (u < p.nunits) issue_pair(p, u, 0, stage, &mbar[0]);
+    if (u < p.nunits) issue_pair(p, u, 0, stage, TS, &mbar[0]);
   }
   __syncthreads();
   int unext = s_next;
@@ -165,6 +194,12 @@ __global__ void __launch_bounds__(NP / 8, TemporalBounds<NP>::MIN_BLOCKS)
 
   while (u < p.nunits) {
     const int4 U = p.units[u];
+    const int vi = p.videos ? U.w : 0;
+    if (vi != cur_v) {  // uniform over the CTA (every thread holds the same u)
+      __syncthreads();  // s_np is no longer read
+      load_video(vi);
+      __syncthreads();
+    }
     // prefetch the next pair (this unit's, or the next unit's first) into the
     // other staging buffer; its last readers finished before the loop-end sync
     int nu = u, nk = k + 2;
@@ -173,18 +208,18 @@ __global__ void __launch_bounds__(NP / 8, TemporalBounds<NP>::MIN_BLOCKS)
       nk = 0;
     }
     const bool prefetched = nu < p.nunits;
-    if (t == 0 && prefetched) issue_pair(p, nu, nk, stage + (buf ^ 1) * 2 * T, &mbar[buf ^ 1]);
+    if (t == 0 && prefetched) issue_pair(p, nu, nk, stage + (buf ^ 1) * 2 * TS, TS, &mbar[buf ^ 1]);
     if (!mbar_wait(&mbar[buf], (phase >> buf) & 1u, p.err, 1)) {
       // give up: let the copy in flight land (bounded), then stop
       if (prefetched) mbar_wait(&mbar[buf ^ 1], (phase >> (buf ^ 1)) & 1u, p.err, 1);
       return;
     }
     phase ^= 1u << buf;
-    const float2* rowa = stage + buf * 2 * T;
-    const float2* rowb = rowa + T;
+    const float2* rowa = stage + buf * 2 * TS;
+    const float2* rowb = rowa + TS;
     const bool hasb = k + 1 < U.y;
-    const int4 ea = load_item(p.items, U.x + k);
-    const int4 eb = hasb ? load_item(p.items, U.x + k + 1) : ea;
+    const int4 ea = load_item(vd.items, U.x + k);
+    const int4 eb = hasb ? load_item(vd.items, U.x + k + 1) : ea;
     float2 v[8];
     {
       float2 w[8];
@@ -210,7 +245,7 @@ __global__ void __launch_bounds__(NP / 8, TemporalBounds<NP>::MIN_BLOCKS)
       const int4 e = s ? eb : ea;
       gather<NP>(v, s ? rowb : rowa, ord, msk);
       const float2* Y = fft<NP, false, true>(v, t, bufA, bufB, s_tw);
-      spectrum_v<NP>(v, t, Y, bufZ, p.mspec, s == 1);
+      spectrum_v<NP>(v, t, Y, bufZ, vd.mspec, s == 1);
       __syncthreads();
       const float2* W = fft<NP, true, true>(v, t, bufA, bufB, s_tw);
       const float ps = s ? zsum.y : zsum.x;
@@ -274,17 +309,19 @@ __global__ void __launch_bounds__(NP / 8, TemporalBounds<NP>::MIN_BLOCKS)
     if (k + 2 >= U.y) {
       if (!FULL) {
         // one partial record per unit: [u][field][tau], P after all records
+        // (u local to the unit's video)
+        const int ul = u - vd.unit0;
 #pragma unroll
         for (int r = 0; r < LPT; r++) {
           const int tau = t + r * NT;
           if (tau < L)
 #pragma unroll
             for (int c = 0; c < PFIELDS; c++) {
-              p.partials[((size_t)u * PFIELDS + c) * L + tau] = acc[r][c];
+              vd.partials[((size_t)ul * PFIELDS + c) * L + tau] = acc[r][c];
               acc[r][c] = 0.0;
             }
         }
-        if (t == 0) p.partials[(size_t)p.nunits * PFIELDS * L + u] = accP;
+        if (t == 0) vd.partials[(size_t)vd.nunits * PFIELDS * L + ul] = accP;
         accP = 0.0;
       }
       u = unext;

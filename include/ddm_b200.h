@@ -146,6 +146,50 @@ int ddm_set_stream(ddm_engine *h, void *stream);
 /* Kernels launched by this engine so far (instrumentation). */
 int64_t ddm_kernel_launches(const ddm_engine *h);
 
+/* ---------------------------------------------------------------------------
+ * Batches: many videos of uneven size and frame count analysed together (no
+ * counterpart in the reference, whose engine holds one video). A batch
+ * borrows existing engines (any geometries, one device; the caller keeps
+ * them alive and destroys them after the batch). Every engine's spatial
+ * chunks are queued on the batch stream without host synchronisation, and
+ * the temporal analysis of ALL videos is one persistent launch over the
+ * concatenated work units of every engine, at the batch's largest TPAD (zero
+ * padding beyond T + L - 1 leaves every lag < L exact: each video's radial
+ * record, read with ddm_read_radial on its engine, equals what its own
+ * engine computes). The whole step can be captured once into a CUDA graph
+ * and replayed. Errors via ddm_batch_last_error(b) (NULL after a failed
+ * create). */
+typedef struct ddm_batch ddm_batch;
+int ddm_batch_create(ddm_engine *const *engines, int32_t n, ddm_batch **out);
+void ddm_batch_destroy(ddm_batch *b);
+const char *ddm_batch_last_error(const ddm_batch *b);
+/* The stream the batch queues its work on (NULL = its own stream). */
+int ddm_batch_set_stream(ddm_batch *b, void *stream);
+/* Spatial stage of every video from DEVICE frames (16-byte aligned):
+ * frames[i] holds n[i] frames of engine i (dtype dtypes[i]), slots[i][n[i]],
+ * luma scale scales[i]. Queued, no host synchronisation (a changed scale is
+ * uploaded first, which synchronises). */
+int ddm_batch_ingest(ddm_batch *b, const void *const *frames, const int32_t *dtypes,
+                     const int32_t *n, const int32_t *const *slots, const float *scales);
+/* Temporal analysis of every video in one launch; orders[i] and masks[i] of
+ * length T_i (as ddm_compute_temporal). Computes the per-video tables on the
+ * host, then queues the copies, the launch and the per-video reductions. */
+int ddm_batch_compute_temporal(ddm_batch *b, const uint32_t *const *orders,
+                               const float *const *masks);
+/* The queued part of ddm_batch_compute_temporal alone, from the tables the
+ * last ddm_batch_compute_temporal filled in. */
+int ddm_batch_enqueue_temporal(ddm_batch *b);
+/* Waits for the batch stream; surfaces device-side error words. */
+int ddm_batch_sync(ddm_batch *b);
+/* Captures ddm_batch_ingest(frames...) + ddm_batch_enqueue_temporal into a
+ * CUDA graph (after one ddm_batch_compute_temporal); ddm_batch_launch_graph
+ * replays it on the batch stream (new orders/masks: call
+ * ddm_batch_compute_temporal's table step again first -- it also runs the
+ * step once). */
+int ddm_batch_capture(ddm_batch *b, const void *const *frames, const int32_t *dtypes,
+                      const int32_t *n, const int32_t *const *slots, const float *scales);
+int ddm_batch_launch_graph(ddm_batch *b);
+
 /* Batched per-bin Levenberg-Marquardt fit of the motility model (the fit
  * stage of analyzeMotility, motility-ddm/src/motility_fit.js:577-611, per
  * q-bin). The reference fits (alpha, vbar, Z, D) globally by VarPro +

@@ -94,7 +94,7 @@ def test_batch_matches_individual_engines_and_graph_replay():
 
 
 def test_batch_small_video_against_oracle():
-    N, T, L = 64, 96, 40
+    N, T, L = 64, 128, 40  # the FP64 oracle transforms powers of two (TPAD = 2T)
     sim = dict(O.BASE, N=N, T=T, seed=9, swimmers=dict(n=20, vbar=20.0, sigma=8.0, geometry="3d"),
                passive=dict(n=20), dropExact=6)
     frames, valid, _ = O.simulate(sim)

@@ -29,7 +29,7 @@ thread_local std::string g_create_error;
 
 struct ddm_engine {
   ddm_geometry g{};
-  int NH = 0, NHB = 0, modes = 0, chunk = 0;
+  int NH = 0, NHB = 0, modes = 0, chunk = 0, chunk_cap = 0, unit_size = 0;
   int device = 0;
   std::string err;
   int64_t launches = 0, throttled = 0;
@@ -144,13 +144,28 @@ static void release(ddm_engine *h) {
   delete h;
 }
 
-static int build_units(ddm_engine *h) {
-  // fused path: runs of up to U modes inside one bin, bins in order
+// Work units of the fused temporal path: runs of up to U modes inside one
+// bin, bins in order. U = 0: about three units per persistent CTA.
+static int build_units(ddm_engine *h, int U = 0) {
   const int NB = h->g.NB;
   const int total = (int)h->bins.offsets[NB];
-  const int grid = std::max(1, temporal_max_grid(h->g.TPAD, h->g.T, h->g.L, false));
-  int U = total / (3 * grid);
-  U = std::max(16, std::min(256, U + (U & 1)));
+  if (U <= 0) {
+    const int grid = std::max(1, temporal_max_grid(h->g.TPAD, h->g.T, h->g.L, false));
+    U = total / (3 * grid);
+    U = std::max(16, std::min(256, U + (U & 1)));
+  }
+  h->unit_size = U;
+  for (void *p : {(void *)h->d_items, (void *)h->d_units, (void *)h->d_bin_units, (void *)h->d_offsets,
+                  (void *)h->d_nmodes, (void *)h->d_units_full, (void *)h->d_counter, (void *)h->d_err,
+                  (void *)h->d_partials})
+    if (p) cudaFree(p);
+  h->d_items = nullptr;
+  h->d_units = nullptr;
+  h->d_bin_units = nullptr;
+  h->d_offsets = h->d_nmodes = nullptr;
+  h->d_units_full = nullptr;
+  h->d_counter = h->d_err = nullptr;
+  h->d_partials = nullptr;
   std::vector<int4> units;
   std::vector<int> bin_units(NB + 1, 0);
   for (int b = 0; b < NB; b++) {
@@ -309,6 +324,8 @@ extern "C" int ddm_create(const ddm_geometry *geometry, ddm_engine **out) {
     size_t c = std::max<size_t>(1, target / per);
     c = std::min<size_t>(MAX_CHUNK, std::max<size_t>(c, fg));
     h->chunk = (int)(c / fg * fg);  // whole column-kernel frame groups
+    // buffers hold up to chunk_cap frames, so the autotuner may pick larger chunks
+    h->chunk_cap = std::max(h->chunk, std::min<int>(MAX_CHUNK, (int)std::max<size_t>(fg, (96u << 20) / per)) / fg * fg);
   }
   h->bins = make_bins(g.N, g.NB, g.kmin, g.kmax, g.knodes);
   int rc = DDM_OK;
@@ -329,12 +346,12 @@ extern "C" int ddm_create(const ddm_geometry *geometry, ddm_engine **out) {
   }
   cudaEventCreateWithFlags(&h->meta_ev, cudaEventDisableTiming);
   const int N = g.N;
-  h->stage_bytes = (size_t)h->chunk * N * N * sizeof(float);
+  h->stage_bytes = (size_t)h->chunk_cap * N * N * sizeof(float);
   if ((rc = dalloc(h, &h->d_hist, (size_t)h->modes * g.T)) ||
-      (rc = dalloc(h, &h->d_rows, (size_t)h->chunk * h->NHB * N * KB)) ||
-      (rc = dalloc(h, &h->d_rowc, (size_t)h->chunk * N)) ||
-      (rc = dalloc(h, &h->d_framesum, (size_t)h->chunk)) ||
-      (rc = dalloc(h, &h->d_means, (size_t)h->chunk)) || (rc = dalloc(h, &h->d_win, N)) ||
+      (rc = dalloc(h, &h->d_rows, (size_t)h->chunk_cap * h->NHB * N * KB)) ||
+      (rc = dalloc(h, &h->d_rowc, (size_t)h->chunk_cap * N)) ||
+      (rc = dalloc(h, &h->d_framesum, (size_t)h->chunk_cap)) ||
+      (rc = dalloc(h, &h->d_means, (size_t)h->chunk_cap)) || (rc = dalloc(h, &h->d_win, N)) ||
       (rc = dalloc(h, &h->d_wys, N)) || (rc = dalloc(h, &h->d_ninv, N)) ||
       (rc = dalloc(h, &h->d_invtot, 1)) || (rc = dalloc(h, &h->d_tw_s, N)) ||
       (rc = dalloc(h, &h->d_tw_t, g.TPAD)) || (rc = dalloc(h, &h->d_wcorr4, 4)) ||
@@ -1082,5 +1099,118 @@ extern "C" int ddm_batch_launch_graph(ddm_batch *b) {
     h->radial_valid = true;
     h->full_valid = false;
   }
+  return DDM_OK;
+}
+
+// ================================================================ autotuner
+//
+// Times the engine's own kernels on this device for its geometry and keeps
+// the fastest choices:
+//   spatial chunk  frames per row/column launch pair (multiples of the
+//                  column kernel's frame group, up to the buffers' capacity):
+//                  larger chunks amortise launches and waves, smaller ones
+//                  keep the row-spectrum scratch resident in L2;
+//   temporal unit  modes per work unit of the persistent temporal kernel:
+//                  smaller units balance uneven bins, larger ones write fewer
+//                  partial records.
+// Each candidate is timed with CUDA events on the engine stream (median of 3
+// after a warm-up) over a synthetic u16 video in a temporary device buffer.
+// The runs overwrite the history ring: tune right after ddm_create, before
+// ingesting, and before building batches over the engine.
+extern "C" int ddm_autotune(ddm_engine *h, char *report, int32_t report_len) {
+  if (!h) return DDM_ERR_ARG;
+  cudaSetDevice(h->device);
+  const int N = h->g.N, T = h->g.T;
+  const int fg = frames_per_col_cta(N);
+  const int nfr = std::min(T, std::max(4 * h->chunk_cap, 64) / fg * fg);
+  void *frames = nullptr;
+  int rc;
+  CK(cudaMalloc(&frames, (size_t)nfr * N * N * 2));
+  CK(cudaMemset(frames, 0x5A, (size_t)nfr * N * N * 2));  // any pixels: FFT time is data-independent
+  std::vector<int32_t> slots(nfr);
+  for (int i = 0; i < nfr; i++) slots[i] = i;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  auto med3 = [](float a, float b, float c) { return std::max(std::min(a, b), std::min(std::max(a, b), c)); };
+  std::string rep = "{\"spatial_chunk\": {";
+  // ---- spatial chunk
+  int best_chunk = h->chunk;
+  float best_t = 1e30f;
+  const int keep_chunk = h->chunk;
+  for (int c = fg; c <= h->chunk_cap; c += (c < 8 * fg ? fg : 2 * fg)) {
+    h->chunk = c;
+    float t[3];
+    for (int r = -1; r < 3; r++) {
+      cudaEventRecord(e0, h->stream);
+      if ((rc = ingest_impl(h, frames, 1, nfr, slots.data(), 1.0f / 65535, true))) {
+        h->chunk = keep_chunk;
+        cudaFree(frames);
+        return rc;
+      }
+      cudaEventRecord(e1, h->stream);
+      cudaEventSynchronize(e1);
+      if (r >= 0) cudaEventElapsedTime(&t[r], e0, e1);
+    }
+    const float us = 1e3f * med3(t[0], t[1], t[2]) / nfr;
+    char b[64];
+    snprintf(b, sizeof b, "%s\"%d\": %.4f", c == fg ? "" : ", ", c, us);
+    rep += b;
+    if (us < best_t) best_t = us, best_chunk = c;
+  }
+  h->chunk = best_chunk;
+  {
+    char b[96];
+    snprintf(b, sizeof b, "}, \"best_chunk\": %d, \"us_per_frame\": %.4f, \"temporal_unit\": {", best_chunk, best_t);
+    rep += b;
+  }
+  // ---- temporal unit size
+  std::vector<uint32_t> order(T);
+  std::vector<float> mask(T, 1.f);
+  for (int i = 0; i < T; i++) order[i] = i;
+  int best_u = h->unit_size;
+  float best_tu = 1e30f;
+  bool first = true;
+  for (int U : {8, 16, 32, 64, 128, 256}) {
+    if ((rc = build_units(h, U))) break;
+    float t[3];
+    for (int r = -1; r < 3; r++) {
+      cudaEventRecord(e0, h->stream);
+      if ((rc = temporal_impl(h, order.data(), mask.data(), 0))) break;
+      cudaEventRecord(e1, h->stream);
+      cudaEventSynchronize(e1);
+      if (r >= 0) cudaEventElapsedTime(&t[r], e0, e1);
+    }
+    if (rc) break;
+    const float ms = med3(t[0], t[1], t[2]);
+    char b[64];
+    snprintf(b, sizeof b, "%s\"%d\": %.4f", first ? "" : ", ", U, ms);
+    rep += b;
+    first = false;
+    if (ms < best_tu) best_tu = ms, best_u = U;
+  }
+  if (!rc) rc = build_units(h, best_u);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(frames);
+  h->have_frames = false;
+  h->radial_valid = h->full_valid = false;
+  if (rc) return rc;
+  {
+    char b[96];
+    snprintf(b, sizeof b, "}, \"best_unit\": %d, \"temporal_ms\": %.4f}", best_u, best_tu);
+    rep += b;
+  }
+  if (report && report_len > 0) {
+    strncpy(report, rep.c_str(), report_len - 1);
+    report[report_len - 1] = 0;
+  }
+  return check_device_error(h);
+}
+
+extern "C" int ddm_get_tuning(const ddm_engine *h, int32_t *chunk, int32_t *unit_size) {
+  if (!h) return DDM_ERR_ARG;
+  if (chunk) *chunk = h->chunk;
+  if (unit_size) *unit_size = h->unit_size;
   return DDM_OK;
 }

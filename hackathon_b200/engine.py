@@ -216,6 +216,22 @@ class DdmEngine:
         f = self._lib.ddm_compute_temporal if wait else self._lib.ddm_compute_temporal_async
         self._check(f(self._h, _ptr(o), _ptr(m), 1 if full else 0))
 
+    def autotune(self):
+        """Times chunk and unit-size candidates on this device and keeps the
+        fastest (ddm_autotune; overwrites the history: call before ingest).
+        Returns the timing report."""
+        import json
+        self._alive()
+        buf = C.create_string_buffer(4096)
+        self._check(self._lib.ddm_autotune(self._h, buf, 4096))
+        return json.loads(buf.value.decode())
+
+    @property
+    def tuning(self):
+        c, u = C.c_int32(), C.c_int32()
+        self._check(self._lib.ddm_get_tuning(self._h, C.byref(c), C.byref(u)))
+        return dict(chunk=c.value, unit_size=u.value)
+
     def read_radial(self):
         """readRadial (ddm-engine.ts:391-395) -> Radial (ddm_ref.js:336-348)."""
         self._alive()

@@ -143,6 +143,16 @@ int64_t ddm_throttled(const ddm_engine *h);
  * e.g. to time it with events on that stream. NULL restores the engine's own
  * stream. */
 int ddm_set_stream(ddm_engine *h, void *stream);
+/* Autotuner (no reference counterpart): times the engine's kernels on this
+ * device for its geometry and keeps the fastest spatial chunk (frames per
+ * row/column launch pair) and temporal work-unit size (modes per unit). The
+ * timing runs overwrite the history ring: call it right after ddm_create,
+ * before ingesting and before ddm_batch_create over the engine. `report`
+ * (may be NULL) receives a JSON summary of every candidate's time. */
+int ddm_autotune(ddm_engine *h, char *report, int32_t report_len);
+/* The engine's current chunk and unit size. */
+int ddm_get_tuning(const ddm_engine *h, int32_t *chunk, int32_t *unit_size);
+
 /* Kernels launched by this engine so far (instrumentation). */
 int64_t ddm_kernel_launches(const ddm_engine *h);
 

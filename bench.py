@@ -246,6 +246,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-fit", action="store_true", help="skip the q-fits/s (surrogate + LM) section")
+    ap.add_argument("--tuning", default="", help="chunk,unit: apply instead of autotuning (profiling runs)")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", 0))
@@ -278,7 +279,12 @@ def main():
     tmask = valid.astype(np.float32)
     eng = H.DdmEngine.create(N=N, T=T, TPAD=TPAD, L=L, NB=NB, kmin=KMIN, kmax=KMAX)
     eng.set_spatial_mask(mask_roi)
-    tune = eng.autotune()  # set-up, outside the timed region
+    if args.tuning:  # a cached autotune result "chunk,unit"
+        c, u = (int(x) for x in args.tuning.split(","))
+        eng.set_tuning(c, u)
+        tune = {"best_chunk": c, "best_unit": u}
+    else:
+        tune = eng.autotune()  # set-up, outside the timed region
     # a dedicated stream: the engine queues its kernels there and the CUDA
     # events below are recorded on the same stream
     stream = torch.cuda.Stream()

@@ -1214,3 +1214,25 @@ extern "C" int ddm_get_tuning(const ddm_engine *h, int32_t *chunk, int32_t *unit
   if (unit_size) *unit_size = h->unit_size;
   return DDM_OK;
 }
+
+// Applies a tuning found earlier (e.g. a cached ddm_autotune result) without
+// timing: chunk a multiple of the column kernel's frame group within the
+// buffers' capacity, unit_size >= 1 (0 keeps the current value).
+extern "C" int ddm_set_tuning(ddm_engine *h, int32_t chunk, int32_t unit_size) {
+  if (!h) return DDM_ERR_ARG;
+  cudaSetDevice(h->device);
+  const int fg = frames_per_col_cta(h->g.N);
+  if (chunk) {
+    if (chunk < fg || chunk > h->chunk_cap || chunk % fg)
+      return fail(h, DDM_ERR_ARG, "chunk %d: need a multiple of %d in [%d, %d]", chunk, fg, fg, h->chunk_cap);
+  }
+  if (unit_size < 0) return fail(h, DDM_ERR_ARG, "unit_size must be >= 0");
+  CK(cudaStreamSynchronize(h->stream));
+  if (chunk) h->chunk = chunk;
+  if (unit_size && unit_size != h->unit_size) {
+    int rc = build_units(h, unit_size);
+    if (rc) return rc;
+    h->radial_valid = h->full_valid = false;
+  }
+  return DDM_OK;
+}

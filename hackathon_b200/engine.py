@@ -226,6 +226,10 @@ class DdmEngine:
         self._check(self._lib.ddm_autotune(self._h, buf, 4096))
         return json.loads(buf.value.decode())
 
+    def set_tuning(self, chunk=0, unit_size=0):
+        self._alive()
+        self._check(self._lib.ddm_set_tuning(self._h, int(chunk), int(unit_size)))
+
     @property
     def tuning(self):
         c, u = C.c_int32(), C.c_int32()

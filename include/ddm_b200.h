@@ -150,8 +150,10 @@ int ddm_set_stream(ddm_engine *h, void *stream);
  * before ingesting and before ddm_batch_create over the engine. `report`
  * (may be NULL) receives a JSON summary of every candidate's time. */
 int ddm_autotune(ddm_engine *h, char *report, int32_t report_len);
-/* The engine's current chunk and unit size. */
+/* The engine's current chunk and unit size; set them without timing (e.g.
+ * from a cached autotune report; 0 keeps a value). */
 int ddm_get_tuning(const ddm_engine *h, int32_t *chunk, int32_t *unit_size);
+int ddm_set_tuning(ddm_engine *h, int32_t chunk, int32_t unit_size);
 
 /* Kernels launched by this engine so far (instrumentation). */
 int64_t ddm_kernel_launches(const ddm_engine *h);

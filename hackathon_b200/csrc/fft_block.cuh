@@ -25,13 +25,14 @@
 
 namespace ddm {
 
-// Shared-memory index with one float2 of padding every 16. 64-bit accesses
-// are served per half-warp (16 lanes over 16 bank pairs): this keeps the
-// stage loads and the stride-1, -64 and -512 stage stores conflict-free; the
-// stride-8 stores and reversed reads stay 2-way (checked by simulating every
-// access pattern of the 512- and 2048-point transforms).
-__device__ __forceinline__ int pad(int i) { return i + (i >> 4); }
-__host__ __device__ constexpr int padded(int n) { return n + n / 16; }
+// Shared-memory index: an XOR swizzle inside each aligned block of 16
+// float2, i ^ ((i >> 3) & 15). 64-bit accesses are served per half-warp (16
+// lanes over 16 bank pairs); with this swizzle every Stockham stage store
+// (strides 1, 8, 64, 512 and the radix-4/2 tails) and every stage load is
+// conflict-free, and no padding memory is needed (checked by simulating
+// every access pattern of the 512- and 2048-point transforms).
+__device__ __forceinline__ int pad(int i) { return i ^ ((i >> 3) & 15); }
+__host__ __device__ constexpr int padded(int n) { return n; }
 
 __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
@@ -135,6 +136,8 @@ __device__ __forceinline__ void stage(float2 (&v)[8], int t, float2* __restrict_
 #pragma unroll
     for (int m = 0; m < R; m++) a[m] = v[i + B * m];
     if (Ns > 1) {
+      // every W^m from the FP64-derived table (products of table entries
+      // would save loads but add roundings the accuracy budget cannot take)
       const float2* tws = tw + tw_offset(n, Ns) + k;
 #pragma unroll
       for (int m = 1; m < R; m++) {

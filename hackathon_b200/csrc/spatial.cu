@@ -49,6 +49,15 @@ __host__ __device__ constexpr int row_groups() {
 }
 constexpr int ROW_STAGES = 2;  // depth of the row-batch staging ring
 
+// float2 between the buffer pairs of consecutive FFT groups: two buffers
+// plus a skew of 2 float2, so the column kernel's stores, which read the same
+// index from G groups at once, hit different banks (16-byte aligned: the
+// bulk-copy destinations after the groups stay aligned).
+template <int N>
+__host__ __device__ constexpr int GSTRIDE() {
+  return 2 * padded(N) + 2;
+}
+
 // The pixels whose mean is a frame's reference level c_f.
 template <int N>
 __device__ __forceinline__ int cref_offset(int i) {
@@ -77,9 +86,9 @@ __global__ void __launch_bounds__(256) rows_kernel(RowParams p) {
   __shared__ double red[WARPS];
   __shared__ __align__(8) uint64_t bar[ROW_STAGES];
   const int g = threadIdx.x / NT, t = threadIdx.x % NT;
-  float2* buf0 = sm + (size_t)g * 2 * PN;
+  float2* buf0 = sm + (size_t)g * GSTRIDE<N>();
   float2* buf1 = buf0 + PN;
-  float2* s_tw = sm + (size_t)G * 2 * PN;
+  float2* s_tw = sm + (size_t)G * GSTRIDE<N>();
   float* s_wy = (float*)(s_tw + tw_size(N));                     // [N] w(y) scale
   Tin* ring = (Tin*)(s_wy + N);                                   // [ROW_STAGES][2G][N]
   uint8_t* mring = (uint8_t*)(ring + ROW_STAGES * BATCH_ELEMS);  // [ROW_STAGES][2G][N]
@@ -208,9 +217,9 @@ __global__ void __launch_bounds__(256) cols_kernel(ColParams p) {
   __shared__ float s_dc[G];  // (c_f - mu) scale / N per frame of the tile
   __shared__ float2 s_wc4[4];
   const int g = threadIdx.x / NT, t = threadIdx.x % NT;
-  float2* buf0 = sm + (size_t)g * 2 * PN;
+  float2* buf0 = sm + (size_t)g * GSTRIDE<N>();
   float2* buf1 = buf0 + PN;
-  float2* s_tw = sm + (size_t)G * 2 * PN;
+  float2* s_tw = sm + (size_t)G * GSTRIDE<N>();
   float2* stage = s_tw + tw_size(N);  // [G][N][KB]
   for (int i = threadIdx.x; i < tw_size(N); i += blockDim.x) s_tw[i] = p.tw[i];
   if (threadIdx.x < 4) s_wc4[threadIdx.x] = p.wc4[threadIdx.x];
@@ -275,8 +284,8 @@ __global__ void __launch_bounds__(256) cols_kernel(ColParams p) {
       // Y of group g sits at the same offset in every group's buffer pair; the
       // CTA writes frame sf = tid % G of each mode: G consecutive ring slots
       if (sf < nf) {
-        const int yoff = (int)(Y - (sm + (size_t)g * 2 * PN));
-        const float2* ys = sm + (size_t)sf * 2 * PN + yoff;
+        const int yoff = (int)(Y - (sm + (size_t)g * GSTRIDE<N>()));
+        const float2* ys = sm + (size_t)sf * GSTRIDE<N>() + yoff;
         float2* hs = p.hist + (size_t)kx * p.T + slot;
         const size_t mstride = (size_t)p.NH * p.T;
         const float dc = s_dc[sf];
@@ -310,7 +319,7 @@ static constexpr int groups() {
 
 template <int N>
 static size_t fft_smem() {
-  return ((size_t)groups<N>() * 2 * padded(N) + tw_size(N)) * sizeof(float2);
+  return ((size_t)groups<N>() * GSTRIDE<N>() + tw_size(N)) * sizeof(float2);
 }
 
 // One wave of persistent CTAs. The occupancy query and the shared-memory

@@ -246,7 +246,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-fit", action="store_true", help="skip the q-fits/s (surrogate + LM) section")
-    ap.add_argument("--tuning", default="", help="chunk,unit: apply instead of autotuning (profiling runs)")
+    ap.add_argument("--tuning", default="", help="chunk,unit[,variant]: apply instead of autotuning")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", 0))
@@ -279,10 +279,11 @@ def main():
     tmask = valid.astype(np.float32)
     eng = H.DdmEngine.create(N=N, T=T, TPAD=TPAD, L=L, NB=NB, kmin=KMIN, kmax=KMAX)
     eng.set_spatial_mask(mask_roi)
-    if args.tuning:  # a cached autotune result "chunk,unit"
-        c, u = (int(x) for x in args.tuning.split(","))
-        eng.set_tuning(c, u)
-        tune = {"best_chunk": c, "best_unit": u}
+    if args.tuning:  # a cached autotune result "chunk,unit[,variant]"
+        vals = [int(x) for x in args.tuning.split(",")]
+        c, u, var = (vals + [0])[:3]
+        eng.set_tuning(c, u, var)
+        tune = {"best_chunk": c, "best_unit": u, "best_variant": var}
     else:
         tune = eng.autotune()  # set-up, outside the timed region
     # a dedicated stream: the engine queues its kernels there and the CUDA
@@ -406,7 +407,8 @@ def main():
                 "config": {"workload": WORKLOAD, "N": N, "T": T, "TPAD": TPAD, "L": L, "NB": NB,
                            "frames_dtype": "u16", "parallelism": f"replicas x{world} (one video per GPU)",
                            "l2": "inputs larger than L2 (537 MB frames, 1.08 GB history per video)",
-                           "autotuned": {"chunk": tune["best_chunk"], "unit": tune["best_unit"]}},
+                           "autotuned": {"chunk": tune["best_chunk"], "unit": tune["best_unit"],
+                                         "temporal_variant": tune["best_variant"]}},
                 "e2e": {"value": e2e, "unit": "frames/s", "h2d_bytes_per_step": int(host.numel() * 2),
                         "d2h_bytes_per_step": rad_bytes},
                 "gpu_launches": int(launches),

@@ -49,8 +49,8 @@ _SIGS = {
                              C.c_double, _i32, _vp, _vp, _vp, _vp, _vp, _i32, _vp]),
     "ddm_model_curves": (C.c_int, [_i32, _i32, _vp, _vp, _i32, _vp, C.c_float, C.c_uint64, _vp, _vp, _vp]),
     "ddm_autotune": (C.c_int, [_vp, C.c_char_p, _i32]),
-    "ddm_get_tuning": (C.c_int, [_vp, C.POINTER(_i32), C.POINTER(_i32)]),
-    "ddm_set_tuning": (C.c_int, [_vp, _i32, _i32]),
+    "ddm_get_tuning": (C.c_int, [_vp, C.POINTER(_i32), C.POINTER(_i32), C.POINTER(_i32)]),
+    "ddm_set_tuning": (C.c_int, [_vp, _i32, _i32, _i32]),
     "ddm_batch_create": (C.c_int, [_vp, _i32, C.POINTER(_vp)]),
     "ddm_batch_destroy": (None, [_vp]),
     "ddm_batch_last_error": (C.c_char_p, [_vp]),

@@ -29,7 +29,7 @@ thread_local std::string g_create_error;
 
 struct ddm_engine {
   ddm_geometry g{};
-  int NH = 0, NHB = 0, modes = 0, chunk = 0, chunk_cap = 0, unit_size = 0;
+  int NH = 0, NHB = 0, modes = 0, chunk = 0, chunk_cap = 0, unit_size = 0, variant = 0;
   int device = 0;
   std::string err;
   int64_t launches = 0, throttled = 0;
@@ -47,7 +47,7 @@ struct ddm_engine {
   double *d_means = nullptr;           // [chunk]
   float *d_win = nullptr, *d_wys = nullptr;
   double *d_ninv = nullptr, *d_invtot = nullptr;
-  float2 *d_tw_s = nullptr, *d_tw_t = nullptr;
+  float2 *d_tw_s = nullptr, *d_tw_t = nullptr, *d_tw_t16 = nullptr;
   float2 *d_wcorr4 = nullptr, *d_wcorr_full = nullptr;  // W(k), k < 4; FFT2(w m) [NH][N]
   uint8_t *d_smask = nullptr;
   void *d_stage[NSTAGE]{};             // device staging for host frames
@@ -125,7 +125,7 @@ static void release(ddm_engine *h) {
   if (h->own_stream) cudaStreamSynchronize(h->own_stream);
   if (h->copy_stream) cudaStreamSynchronize(h->copy_stream);
   void *dev[] = {h->d_hist, h->d_rows, h->d_rowc, h->d_framesum, h->d_means, h->d_win, h->d_wys, h->d_ninv,
-                 h->d_invtot, h->d_tw_s, h->d_tw_t, h->d_wcorr4, h->d_wcorr_full, h->d_smask,
+                 h->d_invtot, h->d_tw_s, h->d_tw_t, h->d_tw_t16, h->d_wcorr4, h->d_wcorr_full, h->d_smask,
                  h->d_stage[0], h->d_stage[1], h->d_order, h->d_mask, h->d_npairs,
                  h->d_mspec, h->d_items, h->d_units, h->d_bin_units, h->d_offsets, h->d_nmodes,
                  h->d_units_full, h->d_counter, h->d_err, h->d_partials, h->d_radD, h->d_radP,
@@ -150,7 +150,7 @@ static int build_units(ddm_engine *h, int U = 0) {
   const int NB = h->g.NB;
   const int total = (int)h->bins.offsets[NB];
   if (U <= 0) {
-    const int grid = std::max(1, temporal_max_grid(h->g.TPAD, h->g.T, h->g.L, false));
+    const int grid = std::max(1, temporal_max_grid(h->g.TPAD, h->g.T, h->g.L, false, h->variant));
     U = total / (3 * grid);
     U = std::max(16, std::min(256, U + (U & 1)));
   }
@@ -354,7 +354,8 @@ extern "C" int ddm_create(const ddm_geometry *geometry, ddm_engine **out) {
       (rc = dalloc(h, &h->d_means, (size_t)h->chunk_cap)) || (rc = dalloc(h, &h->d_win, N)) ||
       (rc = dalloc(h, &h->d_wys, N)) || (rc = dalloc(h, &h->d_ninv, N)) ||
       (rc = dalloc(h, &h->d_invtot, 1)) || (rc = dalloc(h, &h->d_tw_s, N)) ||
-      (rc = dalloc(h, &h->d_tw_t, g.TPAD)) || (rc = dalloc(h, &h->d_wcorr4, 4)) ||
+      (rc = dalloc(h, &h->d_tw_t, g.TPAD)) || (rc = dalloc(h, &h->d_tw_t16, g.TPAD)) ||
+      (rc = dalloc(h, &h->d_wcorr4, 4)) ||
       (rc = dalloc(h, (char **)&h->d_stage[0], h->stage_bytes)) ||
       (rc = dalloc(h, (char **)&h->d_stage[1], h->stage_bytes)) ||
       (rc = dalloc(h, &h->d_order, g.T)) || (rc = dalloc(h, &h->d_mask, g.T)) ||
@@ -372,7 +373,7 @@ extern "C" int ddm_create(const ddm_geometry *geometry, ddm_engine **out) {
   const std::vector<double> w = blackman_harris(N);
   std::vector<float> wf(N);
   for (int i = 0; i < N; i++) wf[i] = (float)w[i];
-  std::vector<float> tws = twiddle_table(N), twt = twiddle_table(g.TPAD);
+  std::vector<float> tws = twiddle_table(N), twt = twiddle_table(g.TPAD), twt16 = twiddle_table(g.TPAD, 16);
   // DFT of the window at kx = 0..3 (zero beyond for the 4-term window)
   float wc4[8];
   for (int kx = 0; kx < 4; kx++) {
@@ -388,6 +389,7 @@ extern "C" int ddm_create(const ddm_geometry *geometry, ddm_engine **out) {
   if (cudaMemcpy(h->d_win, wf.data(), sizeof(float) * N, cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(h->d_tw_s, tws.data(), sizeof(float) * tws.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(h->d_tw_t, twt.data(), sizeof(float) * twt.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(h->d_tw_t16, twt16.data(), sizeof(float) * twt16.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(h->d_wcorr4, wc4, sizeof wc4, cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemset(h->d_hist, 0, sizeof(float2) * (size_t)h->modes * g.T) != cudaSuccess) {
     h->err = "table upload failed";
@@ -634,6 +636,8 @@ static int temporal_impl(ddm_engine *h, const uint32_t *order, const float *mask
   tp.npairs = h->d_npairs;
   tp.mspec = h->d_mspec;
   tp.tw = h->d_tw_t;
+  tp.tw16 = h->d_tw_t16;
+  tp.variant = h->variant;
   tp.unit_counter = h->d_counter;
   tp.err = h->d_err;
   tp.T = T;
@@ -672,7 +676,7 @@ static int temporal_impl(ddm_engine *h, const uint32_t *order, const float *mask
     tp.units = h->d_units;
     tp.nunits = h->nunits;
     tp.partials = h->d_partials;
-    const int grid = std::min(temporal_max_grid(TPAD, T, L, false), h->nunits);
+    const int grid = std::min(temporal_max_grid(TPAD, T, L, false, h->variant), h->nunits);
     CK(cudaMemsetAsync(h->d_counter, 0, sizeof(int), h->stream));
     if (h->nunits > 0) CKL(launch_temporal(TPAD, L, false, tp, std::max(grid, 1), h->stream));
     ReduceParams rp{};
@@ -795,7 +799,7 @@ struct ddm_batch {
   cudaStream_t own = nullptr, stream = nullptr;
   VideoDesc *d_videos = nullptr;
   int4 *d_units = nullptr;
-  float2 *d_tw = nullptr;
+  float2 *d_tw = nullptr, *d_tw16 = nullptr;
   float2 *d_mspec = nullptr;           // [n][TPAD]
   float *d_npairs = nullptr;           // [n][Lmax]
   uint32_t *d_order = nullptr;         // [n][Tmax]
@@ -830,7 +834,7 @@ static int bfail(ddm_batch *b, int code, const char *fmt, ...) {
 static void batch_release(ddm_batch *b) {
   if (b->exec) cudaGraphExecDestroy(b->exec);
   if (b->graph) cudaGraphDestroy(b->graph);
-  for (void *p : {(void *)b->d_videos, (void *)b->d_units, (void *)b->d_tw, (void *)b->d_mspec,
+  for (void *p : {(void *)b->d_videos, (void *)b->d_units, (void *)b->d_tw, (void *)b->d_tw16, (void *)b->d_mspec,
                   (void *)b->d_npairs, (void *)b->d_order, (void *)b->d_mask, (void *)b->d_counter,
                   (void *)b->d_err})
     if (p) cudaFree(p);
@@ -876,13 +880,14 @@ extern "C" int ddm_batch_create(ddm_engine *const *engines, int32_t n, ddm_batch
   b->nunits = (int)units.size();
   b->meta_bytes = (size_t)n * (sizeof(uint32_t) * b->Tmax + sizeof(float) * b->Tmax + sizeof(float) * b->Lmax +
                                sizeof(float2) * b->TPAD);
-  const std::vector<float> tw = twiddle_table(b->TPAD);
+  const std::vector<float> tw = twiddle_table(b->TPAD), tw16 = twiddle_table(b->TPAD, 16);
   bool ok = cudaStreamCreateWithFlags(&b->own, cudaStreamNonBlocking) == cudaSuccess;
   b->stream = b->own;
   auto al = [&](void **p, size_t bytes) { ok = ok && cudaMalloc(p, bytes ? bytes : 1) == cudaSuccess; };
   al((void **)&b->d_videos, sizeof(VideoDesc) * n);
   al((void **)&b->d_units, sizeof(int4) * units.size());
   al((void **)&b->d_tw, sizeof(float) * tw.size());
+  al((void **)&b->d_tw16, sizeof(float) * tw16.size());
   al((void **)&b->d_mspec, sizeof(float2) * n * (size_t)b->TPAD);
   al((void **)&b->d_npairs, sizeof(float) * n * (size_t)b->Lmax);
   al((void **)&b->d_order, sizeof(uint32_t) * n * (size_t)b->Tmax);
@@ -901,6 +906,7 @@ extern "C" int ddm_batch_create(ddm_engine *const *engines, int32_t n, ddm_batch
          (units.empty() ||
           cudaMemcpy(b->d_units, units.data(), sizeof(int4) * units.size(), cudaMemcpyHostToDevice) == cudaSuccess) &&
          cudaMemcpy(b->d_tw, tw.data(), sizeof(float) * tw.size(), cudaMemcpyHostToDevice) == cudaSuccess &&
+         cudaMemcpy(b->d_tw16, tw16.data(), sizeof(float) * tw16.size(), cudaMemcpyHostToDevice) == cudaSuccess &&
          cudaMemset(b->d_err, 0, sizeof(int)) == cudaSuccess;
   }
   if (!ok) {
@@ -1003,6 +1009,8 @@ extern "C" int ddm_batch_enqueue_temporal(ddm_batch *b) {
   BCK(cudaMemcpyAsync(b->d_mspec, hp, sizeof(float2) * nv * (size_t)b->TPAD, cudaMemcpyHostToDevice, b->stream));
   TemporalParams tp{};
   tp.tw = b->d_tw;
+  tp.tw16 = b->d_tw16;
+  tp.variant = b->e[0]->variant;
   tp.units = b->d_units;
   tp.nunits = b->nunits;
   tp.unit_counter = b->d_counter;
@@ -1012,7 +1020,7 @@ extern "C" int ddm_batch_enqueue_temporal(ddm_batch *b) {
   tp.videos = b->d_videos;
   BCK(cudaMemsetAsync(b->d_counter, 0, sizeof(int), b->stream));
   if (b->nunits > 0) {
-    const int grid = std::min(temporal_max_grid(b->TPAD, b->Tmax, b->Lmax, false), b->nunits);
+    const int grid = std::min(temporal_max_grid(b->TPAD, b->Tmax, b->Lmax, false, tp.variant), b->nunits);
     BCK(launch_temporal(b->TPAD, b->Lmax, false, tp, std::max(grid, 1), b->stream));
   }
   for (ddm_engine *h : b->e) {
@@ -1124,7 +1132,7 @@ extern "C" int ddm_autotune(ddm_engine *h, char *report, int32_t report_len) {
   const int fg = frames_per_col_cta(N);
   const int nfr = std::min(T, std::max(4 * h->chunk_cap, 64) / fg * fg);
   void *frames = nullptr;
-  int rc;
+  int rc = DDM_OK;
   CK(cudaMalloc(&frames, (size_t)nfr * N * N * 2));
   CK(cudaMemset(frames, 0x5A, (size_t)nfr * N * N * 2));  // any pixels: FFT time is data-independent
   std::vector<int32_t> slots(nfr);
@@ -1149,7 +1157,11 @@ extern "C" int ddm_autotune(ddm_engine *h, char *report, int32_t report_len) {
         return rc;
       }
       cudaEventRecord(e1, h->stream);
-      cudaEventSynchronize(e1);
+      if (cudaEventSynchronize(e1) != cudaSuccess) {
+        h->chunk = keep_chunk;
+        cudaFree(frames);
+        return fail(h, DDM_ERR_CUDA, "autotune: %s", cudaGetErrorString(cudaGetLastError()));
+      }
       if (r >= 0) cudaEventElapsedTime(&t[r], e0, e1);
     }
     const float us = 1e3f * med3(t[0], t[1], t[2]) / nfr;
@@ -1168,27 +1180,34 @@ extern "C" int ddm_autotune(ddm_engine *h, char *report, int32_t report_len) {
   std::vector<uint32_t> order(T);
   std::vector<float> mask(T, 1.f);
   for (int i = 0; i < T; i++) order[i] = i;
-  int best_u = h->unit_size;
+  int best_u = h->unit_size, best_var = h->variant;
   float best_tu = 1e30f;
   bool first = true;
-  for (int U : {8, 16, 32, 64, 128, 256}) {
+  const int nvar = temporal_has_variant16(h->g.TPAD) ? 2 : 1;
+  for (int cand = 0; cand < 6 * nvar && !rc; cand++) {
+    const int U = 8 << (cand % 6), var = cand / 6;
+    h->variant = var;
     if ((rc = build_units(h, U))) break;
     float t[3];
     for (int r = -1; r < 3; r++) {
       cudaEventRecord(e0, h->stream);
       if ((rc = temporal_impl(h, order.data(), mask.data(), 0))) break;
       cudaEventRecord(e1, h->stream);
-      cudaEventSynchronize(e1);
+      if (cudaEventSynchronize(e1) != cudaSuccess) {
+        rc = fail(h, DDM_ERR_CUDA, "autotune: %s", cudaGetErrorString(cudaGetLastError()));
+        break;
+      }
       if (r >= 0) cudaEventElapsedTime(&t[r], e0, e1);
     }
     if (rc) break;
     const float ms = med3(t[0], t[1], t[2]);
     char b[64];
-    snprintf(b, sizeof b, "%s\"%d\": %.4f", first ? "" : ", ", U, ms);
+    snprintf(b, sizeof b, "%s\"%s%d\": %.4f", first ? "" : ", ", var ? "r16:" : "", U, ms);
     rep += b;
     first = false;
-    if (ms < best_tu) best_tu = ms, best_u = U;
+    if (ms < best_tu) best_tu = ms, best_u = U, best_var = var;
   }
+  h->variant = best_var;
   if (!rc) rc = build_units(h, best_u);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
@@ -1198,7 +1217,8 @@ extern "C" int ddm_autotune(ddm_engine *h, char *report, int32_t report_len) {
   if (rc) return rc;
   {
     char b[96];
-    snprintf(b, sizeof b, "}, \"best_unit\": %d, \"temporal_ms\": %.4f}", best_u, best_tu);
+    snprintf(b, sizeof b, "}, \"best_unit\": %d, \"best_variant\": %d, \"temporal_ms\": %.4f}", best_u,
+             best_var, best_tu);
     rep += b;
   }
   if (report && report_len > 0) {
@@ -1208,18 +1228,21 @@ extern "C" int ddm_autotune(ddm_engine *h, char *report, int32_t report_len) {
   return check_device_error(h);
 }
 
-extern "C" int ddm_get_tuning(const ddm_engine *h, int32_t *chunk, int32_t *unit_size) {
+extern "C" int ddm_get_tuning(const ddm_engine *h, int32_t *chunk, int32_t *unit_size, int32_t *variant) {
   if (!h) return DDM_ERR_ARG;
   if (chunk) *chunk = h->chunk;
   if (unit_size) *unit_size = h->unit_size;
+  if (variant) *variant = h->variant;
   return DDM_OK;
 }
 
 // Applies a tuning found earlier (e.g. a cached ddm_autotune result) without
 // timing: chunk a multiple of the column kernel's frame group within the
 // buffers' capacity, unit_size >= 1 (0 keeps the current value).
-extern "C" int ddm_set_tuning(ddm_engine *h, int32_t chunk, int32_t unit_size) {
+extern "C" int ddm_set_tuning(ddm_engine *h, int32_t chunk, int32_t unit_size, int32_t variant) {
   if (!h) return DDM_ERR_ARG;
+  if (variant < -1 || variant > 1 || (variant == 1 && !temporal_has_variant16(h->g.TPAD)))
+    return fail(h, DDM_ERR_ARG, "variant %d: 0 (radix-8), 1 (radix-16, TPAD 1024..4096) or -1 (keep)", variant);
   cudaSetDevice(h->device);
   const int fg = frames_per_col_cta(h->g.N);
   if (chunk) {
@@ -1229,6 +1252,10 @@ extern "C" int ddm_set_tuning(ddm_engine *h, int32_t chunk, int32_t unit_size) {
   if (unit_size < 0) return fail(h, DDM_ERR_ARG, "unit_size must be >= 0");
   CK(cudaStreamSynchronize(h->stream));
   if (chunk) h->chunk = chunk;
+  if (variant >= 0 && variant != h->variant) {
+    h->variant = variant;
+    h->radial_valid = h->full_valid = false;
+  }
   if (unit_size && unit_size != h->unit_size) {
     int rc = build_units(h, unit_size);
     if (rc) return rc;

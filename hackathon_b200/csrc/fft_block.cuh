@@ -34,14 +34,15 @@ namespace ddm {
 __device__ __forceinline__ int pad(int i) { return i ^ ((i >> 3) & 15); }
 __host__ __device__ constexpr int padded(int n) { return n; }
 
-__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
-__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+#define DDM_HD __host__ __device__ __forceinline__
+DDM_HD float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+DDM_HD float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+DDM_HD float2 cmul(float2 a, float2 b) {
   return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
 }
 // multiply by -i (forward) or +i (inverse)
 template <bool INV>
-__device__ __forceinline__ float2 rot(float2 a) {
+DDM_HD float2 rot(float2 a) {
   return INV ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
 }
 
@@ -69,7 +70,7 @@ struct Dft;
 
 template <bool INV>
 struct Dft<2, INV> {
-  static __device__ __forceinline__ void run(float2* a) {
+  static DDM_HD void run(float2* a) {
     const float2 t = a[0];
     a[0] = cadd(t, a[1]);
     a[1] = csub(t, a[1]);
@@ -78,7 +79,7 @@ struct Dft<2, INV> {
 
 template <bool INV>
 struct Dft<4, INV> {
-  static __device__ __forceinline__ void run(float2* a) {
+  static DDM_HD void run(float2* a) {
     const float2 s02 = cadd(a[0], a[2]), d02 = csub(a[0], a[2]);
     const float2 s13 = cadd(a[1], a[3]), d13 = rot<INV>(csub(a[1], a[3]));
     a[0] = cadd(s02, s13);
@@ -90,7 +91,7 @@ struct Dft<4, INV> {
 
 template <bool INV>
 struct Dft<8, INV> {
-  static __device__ __forceinline__ void run(float2* a) {
+  static DDM_HD void run(float2* a) {
     float2 e[4] = {a[0], a[2], a[4], a[6]};
     float2 o[4] = {a[1], a[3], a[5], a[7]};
     Dft<4, INV>::run(e);
@@ -114,6 +115,44 @@ struct Dft<8, INV> {
     a[6] = csub(e[2], w2);
     a[3] = cadd(e[3], w3);
     a[7] = csub(e[3], w3);
+  }
+};
+
+// 16-point DFT as 4 x 4: inner DFT-4 over n1 of x[4 n1 + n2], twiddle
+// W16^(n2 k1), outer DFT-4 over n2; output X[k1 + 4 k2].
+template <bool INV>
+struct Dft<16, INV> {
+  static DDM_HD void run(float2* a) {
+    // W16^p = (cos(2 pi p / 16), -+ sin(2 pi p / 16)), p = n2 * k1
+    const float c1 = 0.92387953251128676f, s1 = 0.38268343236508977f, h = 0.70710678118654752f;
+    float2 y[4][4];
+#pragma unroll
+    for (int n2 = 0; n2 < 4; n2++) {
+      float2 b[4] = {a[n2], a[n2 + 4], a[n2 + 8], a[n2 + 12]};
+      Dft<4, INV>::run(b);
+#pragma unroll
+      for (int k1 = 0; k1 < 4; k1++) y[n2][k1] = b[k1];
+    }
+    const float sg = INV ? 1.f : -1.f;
+    // (n2, k1) -> p: (1,1)=1 (1,2)=2 (1,3)=3 (2,1)=2 (2,2)=4 (2,3)=6 (3,1)=3 (3,2)=6 (3,3)=9
+    const float2 w1 = make_float2(c1, sg * s1), w2 = make_float2(h, sg * h), w3 = make_float2(s1, sg * c1);
+    const float2 w6 = make_float2(-h, sg * h), w9 = make_float2(-c1, -sg * s1);
+    y[1][1] = cmul(y[1][1], w1);
+    y[1][2] = cmul(y[1][2], w2);
+    y[1][3] = cmul(y[1][3], w3);
+    y[2][1] = cmul(y[2][1], w2);
+    y[2][2] = rot<INV>(y[2][2]);
+    y[2][3] = cmul(y[2][3], w6);
+    y[3][1] = cmul(y[3][1], w3);
+    y[3][2] = cmul(y[3][2], w6);
+    y[3][3] = cmul(y[3][3], w9);
+#pragma unroll
+    for (int k1 = 0; k1 < 4; k1++) {
+      float2 c[4] = {y[0][k1], y[1][k1], y[2][k1], y[3][k1]};
+      Dft<4, INV>::run(c);
+#pragma unroll
+      for (int k2 = 0; k2 < 4; k2++) a[k1 + 4 * k2] = c[k2];
+    }
   }
 };
 
@@ -205,6 +244,118 @@ __device__ __forceinline__ float2* fft(float2 (&v)[8], int t, float2* buf0, floa
                                        const float2* __restrict__ tw, int bar_id = 0) {
   Stages<n, 1, INV, TW_SMEM, SYNC>::run(v, t, buf0, buf1, tw, bar_id);
   return (fft_stages(n) & 1) ? buf0 : buf1;
+}
+
+}  // namespace ddm
+
+// ---------------------------------------------------------------------------
+// 16 points per thread, radix-16 stages, one exchange buffer per group.
+//
+// An n-point transform over n/16 threads; stages are radix 16 while n/Ns >= 16
+// (then the remaining radix 8/4/2): 2048 = 16 x 16 x 8 takes three passes
+// through shared memory instead of the four of the radix-8 plan. Layout
+// contract as above with 16 points: on entry to a stage thread t holds
+// v[q] = x[t + q*n/16]. Each stage computes its butterflies in registers,
+// waits until the group has finished reading the buffer, stores, and waits
+// for the stores: one buffer per group, two group barriers per stage. The
+// swizzle for this access pattern is i ^ ((i >> 4) & 15) (conflict-free for
+// every stage store and load, by simulation). Twiddles: a host FP64 table
+// laid out per stage like the radix-8 one, for this plan.
+
+namespace ddm {
+
+__device__ __forceinline__ int pad16(int i) { return i ^ ((i >> 4) & 15); }
+
+__host__ __device__ constexpr int radix16(int n, int ns) { return (n / ns) >= 16 ? 16 : (n / ns); }
+__host__ __device__ constexpr int tw_offset16(int n, int Ns) {
+  int off = 0;
+  for (int ns = 1; ns < Ns;) {
+    const int r = radix16(n, ns);
+    if (ns > 1) off += (r - 1) * ns;
+    ns *= r;
+  }
+  return off;
+}
+__host__ __device__ constexpr int tw_size16(int n) { return tw_offset16(n, n); }
+
+// barrier of the NTG threads of group `id` (named barrier 1 + group)
+template <int NTG>
+__device__ __forceinline__ void group_sync(int id) {
+  if constexpr (NTG <= 32)
+    __syncwarp();
+  else
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "n"(NTG) : "memory");
+}
+
+template <int n, int R, int Ns, bool INV>
+__device__ __forceinline__ void stage16_compute(float2 (&v)[16], int t, const float2* __restrict__ tw) {
+  constexpr int NT = n / 16, B = 16 / R;
+#pragma unroll
+  for (int i = 0; i < B; i++) {
+    const int j = t + i * NT;
+    const int k = j & (Ns - 1);
+    float2 a[R];
+#pragma unroll
+    for (int m = 0; m < R; m++) a[m] = v[i + B * m];
+    if (Ns > 1) {
+      const float2* tws = tw + tw_offset16(n, Ns) + k;
+#pragma unroll
+      for (int m = 1; m < R; m++) {
+        float2 w = tws[(m - 1) * Ns];
+        if (INV) w.y = -w.y;
+        a[m] = cmul(a[m], w);
+      }
+    }
+    Dft<R, INV>::run(a);
+    // butterfly i owns slots i + B*m: in place
+#pragma unroll
+    for (int m = 0; m < R; m++) v[i + B * m] = a[m];
+  }
+}
+
+template <int n, int R, int Ns>
+__device__ __forceinline__ void stage16_store(const float2 (&v)[16], int t, float2* __restrict__ buf) {
+  constexpr int NT = n / 16, B = 16 / R;
+#pragma unroll
+  for (int i = 0; i < B; i++) {
+    const int j = t + i * NT;
+    const int k = j & (Ns - 1);
+    const int base = (j - k) * R + k;
+#pragma unroll
+    for (int m = 0; m < R; m++) buf[pad16(base + m * Ns)] = v[i + B * m];
+  }
+}
+
+template <int n>
+__device__ __forceinline__ void load16(float2 (&v)[16], int t, const float2* __restrict__ buf) {
+  constexpr int NT = n / 16;
+#pragma unroll
+  for (int q = 0; q < 16; q++) v[q] = buf[pad16(t + q * NT)];
+}
+
+template <int n, bool INV, int Ns = 1>
+struct Stages16 {
+  static __device__ __forceinline__ void run(float2 (&v)[16], int t, float2* buf, const float2* __restrict__ tw,
+                                             int bar_id) {
+    constexpr int R = radix16(n, Ns);
+    stage16_compute<n, R, Ns, INV>(v, t, tw);
+    group_sync<n / 16>(bar_id);  // the group is done reading buf
+    stage16_store<n, R, Ns>(v, t, buf);
+    group_sync<n / 16>(bar_id);  // the stores are visible
+    if constexpr (Ns * R < n) {
+      load16<n>(v, t, buf);
+      Stages16<n, INV, Ns * R>::run(v, t, buf, tw, bar_id);
+    }
+  }
+};
+
+// Full n-point FFT of the 16 register points per thread; the natural-order
+// result is left in buf (read it at pad16(k)). The first store waits for the
+// group, so buf may hold this FFT's own input until then.
+template <int n, bool INV>
+__device__ __forceinline__ void fft16(float2 (&v)[16], int t, float2* buf, const float2* __restrict__ tw,
+                                      int bar_id) {
+  Stages16<n, INV>::run(v, t, buf, tw, bar_id);
 }
 
 }  // namespace ddm

@@ -59,7 +59,8 @@ struct TemporalParams {
   const float* mask;       // [T] 0/1
   const float* npairs;     // [L] exact valid-pair counts N(tau)
   const float2* mspec;     // [TPAD] FFT of the zero-padded mask
-  const float2* tw;        // exp(-2 pi i j / TPAD)
+  const float2* tw;        // per-stage twiddle blocks, radix-8 plan of TPAD
+  const float2* tw16;      // per-stage twiddle blocks, radix-16 plan of TPAD
   const int4* items;       // (mode, kx, ky, bin); nullptr: item i is mode i
   const int4* units;       // (first item, count, bin, 0)
   int nunits;
@@ -71,6 +72,7 @@ struct TemporalParams {
   int* err;                // error word (bounded waits that timed out)
   int T, L;                // single video; batched: the largest T and L
   const VideoDesc* videos; // nullptr: one video (the fields above); else units[u].w indexes it
+  int variant;             // 0: one-group radix-8 kernel; 1: two-group radix-16 (TPAD 1024..4096)
 };
 
 struct ReduceParams {
@@ -124,7 +126,9 @@ cudaError_t launch_cols(int N, const ColParams& p, cudaStream_t s);
 int frames_per_col_cta(int N);
 cudaError_t launch_temporal(int TPAD, int L, bool full, const TemporalParams& p, int grid,
                             cudaStream_t s);
-int temporal_max_grid(int TPAD, int T, int L, bool full);
+int temporal_max_grid(int TPAD, int T, int L, bool full, int variant = 0);
+// whether the two-group radix-16 variant exists for this TPAD (fused path)
+bool temporal_has_variant16(int TPAD);
 cudaError_t launch_reduce(const ReduceParams& p, cudaStream_t s);
 cudaError_t launch_radial_full(const RadialFullParams& p, cudaStream_t s);
 cudaError_t launch_lm(const LmParams& p, cudaStream_t s);

@@ -37,11 +37,12 @@ std::vector<double> blackman_harris(int n) {
   return w;
 }
 
-std::vector<float> twiddle_table(int n) {
-  // stage blocks w[(m-1)*Ns + k] = exp(-2 pi i m k / (Ns R)) (fft_block.cuh)
+std::vector<float> twiddle_table(int n, int P) {
+  // stage blocks w[(m-1)*Ns + k] = exp(-2 pi i m k / (Ns R)) (fft_block.cuh),
+  // radix P while n/Ns >= P, then the remainder
   std::vector<float> t;
   for (int ns = 1; ns < n;) {
-    const int r = (n / ns) >= 8 ? 8 : (n / ns);
+    const int r = (n / ns) >= P ? P : (n / ns);
     if (ns > 1)
       for (int m = 1; m < r; m++)
         for (int k = 0; k < ns; k++) {

@@ -20,7 +20,7 @@ std::vector<double> blackman_harris(int n);
 
 // Per-stage twiddle blocks of the n-point device FFT (layout in
 // fft_block.cuh), FP64 rounded to FP32, re/im interleaved.
-std::vector<float> twiddle_table(int n);
+std::vector<float> twiddle_table(int n, int P = 8);
 
 struct BinTable {
   int N = 0, NB = 0, K = 0;

@@ -337,6 +337,244 @@ __global__ void __launch_bounds__(NP / 8, TemporalBounds<NP>::MIN_BLOCKS)
   }
 }
 
+// ---------------------------------------------------------------------------
+// Two-group variant for TPAD 1024..4096 (fused radial epilogue only): the CTA
+// is two groups of TPAD/16 threads, each running 16-point-per-thread radix-16
+// transforms (three exchange passes at 2048 instead of four, one buffer per
+// group). Per mode pair (a, b) the five transforms run in three steps:
+//   1: group 0  Z = FFT(p_a + i p_b)        group 1  Y_b = FFT(x_b)
+//   2: group 0  Y_a = FFT(x_a)              group 1  W_b = IFFT(V_b)
+//   3: group 0  W_a = IFFT(V_a)
+// then all threads run the epilogue of both modes (same lags per thread as
+// the one-group kernel, so the FP64 accumulators stay in registers).
+template <int NP>
+__device__ __forceinline__ void gather16(float2 (&x)[16], const float2* __restrict__ row, const int (&om)[8]) {
+#pragma unroll
+  for (int q = 0; q < 8; q++) x[q] = om[q] >= 0 ? row[om[q]] : make_float2(0.f, 0.f);
+#pragma unroll
+  for (int q = 8; q < 16; q++) x[q] = make_float2(0.f, 0.f);
+}
+
+template <int NP>
+__device__ __forceinline__ void spectrum16(float2 (&v)[16], int t, const float2* __restrict__ Y,
+                                           const float2* __restrict__ Z, const float2* __restrict__ mspec,
+                                           bool second) {
+  constexpr int NTG = NP / 16;
+#pragma unroll
+  for (int q = 0; q < 16; q++) {
+    const int k = t + q * NTG;
+    const float2 y = Y[pad16(k)];
+    const float2 zk = Z[pad16(k)];
+    const float2 zn = Z[pad16((NP - k) & (NP - 1))];
+    const float2 M = __ldg(&mspec[k]);
+    const float Px = second ? 0.5f * (zk.y + zn.y) : 0.5f * (zk.x + zn.x);
+    const float Py = second ? -0.5f * (zk.x - zn.x) : 0.5f * (zk.y - zn.y);
+    const float S = fmaf(y.x, y.x, y.y * y.y);
+    const float R = 2.f * fmaf(M.x, Px, M.y * Py);
+    v[q] = make_float2(S, R);
+  }
+}
+
+template <int NP, int LPT>
+__global__ void __launch_bounds__(NP / 8, TemporalBounds<NP>::MIN_BLOCKS) temporal16_kernel(TemporalParams p) {
+  constexpr int NTG = NP / 16;  // threads per group
+  constexpr int NTH = 2 * NTG;  // threads per CTA
+  extern __shared__ __align__(16) float2 sm[];
+  float2* bufG0 = sm;
+  float2* bufG1 = sm + NP;
+  float2* bufZ = sm + 2 * NP;
+  __shared__ __align__(8) uint64_t mbar[2];
+  __shared__ int s_next;
+  const int t = threadIdx.x;
+  const int g = t / NTG, tl = t % NTG;
+  const int TS = p.T;                 // staging stride: the (largest) T
+  float2* stage = sm + 3 * NP;        // [2 buffers][2 rows][TS]
+  float2* s_tw = stage + 4 * TS;      // per-stage twiddle blocks (radix-16 plan)
+  float* s_np = (float*)(s_tw + tw_size16(NP));
+  const float invn = 0.5f / NP;
+  for (int i = t; i < tw_size16(NP); i += NTH) s_tw[i] = p.tw16[i];
+
+  // per-video state (few registers: the FFTs need them): the slot of each
+  // of this thread's samples, -1 where the mask drops it or beyond T
+  const int4* v_items = nullptr;
+  const float2* v_mspec = nullptr;
+  double* v_partials = nullptr;
+  int cur_v = -1, L = 0, v_unit0 = 0, v_nunits = 0;
+  float np0 = 0.f;
+  int om[8];
+  auto load_video = [&](int vi) {
+    const VideoDesc vd = video_of(p, vi);
+    cur_v = vi;
+    L = vd.L;
+    v_items = vd.items;
+    v_mspec = vd.mspec;
+    v_partials = vd.partials;
+    v_unit0 = vd.unit0;
+    v_nunits = vd.nunits;
+    np0 = vd.npairs[0];
+    for (int i = t; i < L; i += NTH) s_np[i] = vd.npairs[i];
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      const int i = tl + q * NTG;
+      om[q] = (i < vd.T && __ldg(&vd.mask[i]) != 0.f) ? (int)__ldg(&vd.order[i]) : -1;
+    }
+  };
+  if (t == 0) {
+    mbar_init(&mbar[0], 1);
+    mbar_init(&mbar[1], 1);
+    fence_barrier_init();
+    s_next = atomicAdd(p.unit_counter, 1);
+  }
+  __syncthreads();
+  int u = s_next;
+  __syncthreads();
+  if (t == 0) {
+    s_next = atomicAdd(p.unit_counter, 1);
+    if (u < p.nunits) issue_pair(p, u, 0, stage, TS, &mbar[0]);
+  }
+  __syncthreads();
+  int unext = s_next;
+  int k = 0, buf = 0;
+  uint32_t phase = 0;
+  double acc[LPT][PFIELDS];
+  double accP = 0.0;
+#pragma unroll
+  for (int r = 0; r < LPT; r++)
+#pragma unroll
+    for (int c = 0; c < PFIELDS; c++) acc[r][c] = 0.0;
+
+  while (u < p.nunits) {
+    const int4 U = p.units[u];
+    const int vi = p.videos ? U.w : 0;
+    if (vi != cur_v) {
+      __syncthreads();
+      load_video(vi);
+      __syncthreads();
+    }
+    int nu = u, nk = k + 2;
+    if (nk >= U.y) {
+      nu = unext;
+      nk = 0;
+    }
+    const bool prefetched = nu < p.nunits;
+    if (t == 0 && prefetched) issue_pair(p, nu, nk, stage + (buf ^ 1) * 2 * TS, TS, &mbar[buf ^ 1]);
+    if (!mbar_wait(&mbar[buf], (phase >> buf) & 1u, p.err, 1)) {
+      if (prefetched) mbar_wait(&mbar[buf ^ 1], (phase >> (buf ^ 1)) & 1u, p.err, 1);
+      return;
+    }
+    phase ^= 1u << buf;
+    const float2* rowa = stage + buf * 2 * TS;
+    const float2* rowb = rowa + TS;
+    const bool hasb = k + 1 < U.y;
+    const int4 ea = load_item(v_items, U.x + k);
+    const int4 eb = hasb ? load_item(v_items, U.x + k + 1) : ea;
+    float2 v[16];
+    // step 1
+    if (g == 0) {
+      // p_a + i p_b at this thread's samples (T <= TPAD/2: q >= 8 is padding)
+#pragma unroll
+      for (int q = 0; q < 8; q++) {
+        const bool on = om[q] >= 0;
+        const float2 xa = on ? rowa[om[q]] : make_float2(0.f, 0.f);
+        const float2 xb = on && hasb ? rowb[om[q]] : make_float2(0.f, 0.f);
+        v[q] = make_float2(fmaf(xa.x, xa.x, xa.y * xa.y), fmaf(xb.x, xb.x, xb.y * xb.y));
+      }
+#pragma unroll
+      for (int q = 8; q < 16; q++) v[q] = make_float2(0.f, 0.f);
+      fft16<NP, false>(v, tl, bufZ, s_tw, 1);
+    } else if (hasb) {
+      gather16<NP>(v, rowb, om);
+      fft16<NP, false>(v, tl, bufG1, s_tw, 2);
+    }
+    __syncthreads();  // Z and Y_b complete
+    const float2 zsum = bufZ[0];  // (sum p_a, sum p_b)
+    // step 2
+    if (g == 0) {
+      gather16<NP>(v, rowa, om);
+      fft16<NP, false>(v, tl, bufG0, s_tw, 1);
+    } else if (hasb) {
+      spectrum16<NP>(v, tl, bufG1, bufZ, v_mspec, true);
+      fft16<NP, true>(v, tl, bufG1, s_tw, 2);
+    }
+    // step 3 (group 0 only: its own barriers order Y_a)
+    if (g == 0) {
+      spectrum16<NP>(v, tl, bufG0, bufZ, v_mspec, false);
+      fft16<NP, true>(v, tl, bufG0, s_tw, 1);
+    }
+    __syncthreads();  // W_a, W_b complete
+#pragma unroll 1
+    for (int s = 0; s < 2; s++) {
+      if (s == 1 && !hasb) break;
+      const int4 e = s ? eb : ea;
+      const float2* W = s ? bufG1 : bufG0;
+      const float ps = s ? zsum.y : zsum.x;
+      const float P = np0 > 0.5f ? ps / np0 : 0.f;
+      const double kx = e.y, ky = e.z;
+#pragma unroll
+      for (int r = 0; r < LPT; r++) {
+        const int tau = t + r * NTH;
+        if (tau < L) {
+          const float n0 = s_np[tau];
+          const float inp = n0 > 0.5f ? 1.f / n0 : 0.f;
+          const float2 w0 = W[pad16(tau)];
+          const float2 w1 = W[pad16((NP - tau) & (NP - 1))];
+          const float gx = (w0.x + w1.x) * invn, gy = (w0.y - w1.y) * invn;
+          const float ee = (w0.y + w1.y) * invn;
+          acc[r][0] += (double)((ee - 2.f * gx) * inp);
+          if (tau + 1 < L) {
+            const float n1 = s_np[tau + 1];
+            const float inp1 = n1 > 0.5f ? 1.f / n1 : 0.f;
+            const float2 u0 = W[pad16(tau + 1)];
+            const float2 u1 = W[pad16((NP - tau - 1) & (NP - 1))];
+            const float cx = gx * inp, cy = gy * inp;
+            const float c1x = (u0.x + u1.x) * invn * inp1;
+            const float c1y = (u0.y - u1.y) * invn * inp1;
+            const float zr = fmaf(c1x, cx, c1y * cy);  // C(tau+1) conj C(tau)
+            const float zi = fmaf(c1y, cx, -c1x * cy);
+            const float wgt = sqrtf(fmaf(zr, zr, zi * zi));
+            if (wgt > 0.f) {
+              const double wd = wgt, ph = atan2f(zi, zr);
+              acc[r][1] += wd;
+              acc[r][2] += wd * kx * kx;
+              acc[r][3] += wd * kx * ky;
+              acc[r][4] += wd * ky * ky;
+              acc[r][5] += wd * kx * ph;
+              acc[r][6] += wd * ky * ph;
+              acc[r][7] += wd * ph * ph;
+              acc[r][8] += 1.0;
+            }
+          }
+        }
+      }
+      accP += (double)P;
+    }
+    if (k + 2 >= U.y) {
+      const int ul = u - v_unit0;
+#pragma unroll
+      for (int r = 0; r < LPT; r++) {
+        const int tau = t + r * NTH;
+        if (tau < L)
+#pragma unroll
+          for (int c = 0; c < PFIELDS; c++) {
+            v_partials[((size_t)ul * PFIELDS + c) * L + tau] = acc[r][c];
+            acc[r][c] = 0.0;
+          }
+      }
+      if (t == 0) v_partials[(size_t)v_nunits * PFIELDS * L + ul] = accP;
+      accP = 0.0;
+      u = unext;
+      k = 0;
+      if (t == 0) s_next = atomicAdd(p.unit_counter, 1);
+    } else {
+      k += 2;
+    }
+    buf ^= 1;
+    fence_proxy_async_smem();  // this CTA's reads of the staged rows before the next TMA write
+    __syncthreads();           // also: the epilogue is done with bufG0/G1 before the next pair
+    unext = s_next;
+  }
+}
+
 // Sums the unit partials of each bin in unit order (deterministic), divides
 // D and P by the bin's mode count (ddm_ref.js:404-412) and writes the
 // reference's Radial layout: D[b*L+tau], P[b], drift[(b*L+tau)*8+c].
@@ -422,8 +660,27 @@ static int lpt_of(int TPAD, int L) {
   return r <= 1 ? 1 : r <= 2 ? 2 : 4;
 }
 
+// The two-group radix-16 kernel exists for the fused radial path at TPAD
+// 1024..4096 and is chosen by TemporalParams::variant (the autotuner times
+// both); the one-group kernel serves the rest and the full per-mode outputs.
+__host__ __device__ constexpr bool use16(int NP, bool full) { return !full && NP >= 1024 && NP <= 4096; }
+
+template <int NP>
+static size_t temporal16_smem(int T, int L) {
+  return sizeof(float2) * (3 * (size_t)NP + 4 * (size_t)T + tw_size16(NP)) + sizeof(float) * (size_t)L;
+}
+
 template <int NP, int LPT, bool FULL>
 static cudaError_t launch_k(const TemporalParams& p, int grid, cudaStream_t s) {
+  if constexpr (use16(NP, FULL)) {
+    if (p.variant == 1) {
+      auto k = temporal16_kernel<NP, LPT>;
+      const size_t sm = temporal16_smem<NP>(p.T, p.L);
+      cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+      k<<<grid, NP / 8, sm, s>>>(p);
+      return cudaGetLastError();
+    }
+  }
   auto k = temporal_kernel<NP, LPT, FULL>;
   const size_t sm = temporal_smem<NP>(p.T, p.L);
   cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
@@ -441,51 +698,59 @@ static int occupancy_grid(K k, int threads, size_t smem) {
   return sms * (per > 0 ? per : 1);
 }
 
+template <int NP, int LPT, bool FULL>
+static int grid_of(int T, int L, int variant) {
+  if constexpr (use16(NP, FULL))
+    if (variant == 1) return occupancy_grid(temporal16_kernel<NP, LPT>, NP / 8, temporal16_smem<NP>(T, L));
+  return occupancy_grid(temporal_kernel<NP, LPT, FULL>, NP / 8, temporal_smem<NP>(T, L));
+}
+
 template <int NP>
 static cudaError_t dispatch_np(int T, int L, bool full, const TemporalParams* p, int grid,
-                               cudaStream_t s, int* grid_out) {
-  const size_t sm = temporal_smem<NP>(T, L);
+                               cudaStream_t s, int* grid_out, int variant) {
   if (full) {
-    if (grid_out) *grid_out = occupancy_grid(temporal_kernel<NP, 1, true>, NP / 8, sm);
+    if (grid_out) *grid_out = grid_of<NP, 1, true>(T, L, variant);
     return p ? launch_k<NP, 1, true>(*p, grid, s) : cudaSuccess;
   }
   switch (lpt_of(NP, L)) {
     case 1:
-      if (grid_out) *grid_out = occupancy_grid(temporal_kernel<NP, 1, false>, NP / 8, sm);
+      if (grid_out) *grid_out = grid_of<NP, 1, false>(T, L, variant);
       return p ? launch_k<NP, 1, false>(*p, grid, s) : cudaSuccess;
     case 2:
-      if (grid_out) *grid_out = occupancy_grid(temporal_kernel<NP, 2, false>, NP / 8, sm);
+      if (grid_out) *grid_out = grid_of<NP, 2, false>(T, L, variant);
       return p ? launch_k<NP, 2, false>(*p, grid, s) : cudaSuccess;
     default:
-      if (grid_out) *grid_out = occupancy_grid(temporal_kernel<NP, 4, false>, NP / 8, sm);
+      if (grid_out) *grid_out = grid_of<NP, 4, false>(T, L, variant);
       return p ? launch_k<NP, 4, false>(*p, grid, s) : cudaSuccess;
   }
 }
 
 static cudaError_t dispatch(int TPAD, int T, int L, bool full, const TemporalParams* p, int grid,
-                            cudaStream_t s, int* grid_out) {
+                            cudaStream_t s, int* grid_out, int variant) {
   switch (TPAD) {
-    case 128: return dispatch_np<128>(T, L, full, p, grid, s, grid_out);
-    case 256: return dispatch_np<256>(T, L, full, p, grid, s, grid_out);
-    case 512: return dispatch_np<512>(T, L, full, p, grid, s, grid_out);
-    case 1024: return dispatch_np<1024>(T, L, full, p, grid, s, grid_out);
-    case 2048: return dispatch_np<2048>(T, L, full, p, grid, s, grid_out);
-    case 4096: return dispatch_np<4096>(T, L, full, p, grid, s, grid_out);
-    case 8192: return dispatch_np<8192>(T, L, full, p, grid, s, grid_out);
+    case 128: return dispatch_np<128>(T, L, full, p, grid, s, grid_out, variant);
+    case 256: return dispatch_np<256>(T, L, full, p, grid, s, grid_out, variant);
+    case 512: return dispatch_np<512>(T, L, full, p, grid, s, grid_out, variant);
+    case 1024: return dispatch_np<1024>(T, L, full, p, grid, s, grid_out, variant);
+    case 2048: return dispatch_np<2048>(T, L, full, p, grid, s, grid_out, variant);
+    case 4096: return dispatch_np<4096>(T, L, full, p, grid, s, grid_out, variant);
+    case 8192: return dispatch_np<8192>(T, L, full, p, grid, s, grid_out, variant);
     default: return cudaErrorInvalidValue;
   }
 }
 
 cudaError_t launch_temporal(int TPAD, int L, bool full, const TemporalParams& p, int grid,
                             cudaStream_t s) {
-  return dispatch(TPAD, p.T, L, full, &p, grid, s, nullptr);
+  return dispatch(TPAD, p.T, L, full, &p, grid, s, nullptr, p.variant);
 }
 
-int temporal_max_grid(int TPAD, int T, int L, bool full) {
+int temporal_max_grid(int TPAD, int T, int L, bool full, int variant) {
   int g = 0;
-  dispatch(TPAD, T, L, full, nullptr, 0, nullptr, &g);
+  dispatch(TPAD, T, L, full, nullptr, 0, nullptr, &g, variant);
   return g;
 }
+
+bool temporal_has_variant16(int TPAD) { return use16(TPAD, false); }
 
 cudaError_t launch_reduce(const ReduceParams& p, cudaStream_t s) {
   const int threads = p.L >= 256 ? 256 : ((p.L + 31) / 32) * 32;

@@ -226,15 +226,15 @@ class DdmEngine:
         self._check(self._lib.ddm_autotune(self._h, buf, 4096))
         return json.loads(buf.value.decode())
 
-    def set_tuning(self, chunk=0, unit_size=0):
+    def set_tuning(self, chunk=0, unit_size=0, variant=-1):
         self._alive()
-        self._check(self._lib.ddm_set_tuning(self._h, int(chunk), int(unit_size)))
+        self._check(self._lib.ddm_set_tuning(self._h, int(chunk), int(unit_size), int(variant)))
 
     @property
     def tuning(self):
-        c, u = C.c_int32(), C.c_int32()
-        self._check(self._lib.ddm_get_tuning(self._h, C.byref(c), C.byref(u)))
-        return dict(chunk=c.value, unit_size=u.value)
+        c, u, v = C.c_int32(), C.c_int32(), C.c_int32()
+        self._check(self._lib.ddm_get_tuning(self._h, C.byref(c), C.byref(u), C.byref(v)))
+        return dict(chunk=c.value, unit_size=u.value, variant=v.value)
 
     def read_radial(self):
         """readRadial (ddm-engine.ts:391-395) -> Radial (ddm_ref.js:336-348)."""

@@ -145,15 +145,18 @@ int64_t ddm_throttled(const ddm_engine *h);
 int ddm_set_stream(ddm_engine *h, void *stream);
 /* Autotuner (no reference counterpart): times the engine's kernels on this
  * device for its geometry and keeps the fastest spatial chunk (frames per
- * row/column launch pair) and temporal work-unit size (modes per unit). The
+ * row/column launch pair), temporal work-unit size (modes per unit) and
+ * temporal kernel variant (0: one group of TPAD/8 threads, radix-8 stages;
+ * 1: two groups of TPAD/16 threads, radix-16 stages, TPAD 1024..4096). The
  * timing runs overwrite the history ring: call it right after ddm_create,
  * before ingesting and before ddm_batch_create over the engine. `report`
  * (may be NULL) receives a JSON summary of every candidate's time. */
 int ddm_autotune(ddm_engine *h, char *report, int32_t report_len);
-/* The engine's current chunk and unit size; set them without timing (e.g.
- * from a cached autotune report; 0 keeps a value). */
-int ddm_get_tuning(const ddm_engine *h, int32_t *chunk, int32_t *unit_size);
-int ddm_set_tuning(ddm_engine *h, int32_t chunk, int32_t unit_size);
+/* The engine's current chunk, unit size and variant; set them without
+ * timing (e.g. from a cached autotune report; chunk/unit 0 and variant -1
+ * keep a value). */
+int ddm_get_tuning(const ddm_engine *h, int32_t *chunk, int32_t *unit_size, int32_t *variant);
+int ddm_set_tuning(ddm_engine *h, int32_t chunk, int32_t unit_size, int32_t variant);
 
 /* Kernels launched by this engine so far (instrumentation). */
 int64_t ddm_kernel_launches(const ddm_engine *h);

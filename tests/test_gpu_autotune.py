@@ -1,7 +1,8 @@
-"""The autotuner (ddm_autotune) picks its spatial chunk and temporal unit
-size from timed candidates, and the tuned engine computes the same radial
-record as an untuned one (unit size only regroups FP64 partial sums:
-agreement to 1e-10 of each bin's scale)."""
+"""The autotuner (ddm_autotune) picks its spatial chunk, temporal unit size
+and temporal kernel variant from timed candidates, and the tuned engine
+computes the same radial record as an untuned one (unit size regroups FP64
+partial sums, the variant changes the FFT plan's FP32 rounding: agreement to
+1e-5 of each bin's scale, the FP32 transforms' accuracy)."""
 import numpy as np
 import pytest
 
@@ -26,7 +27,10 @@ def test_autotune_report_and_results_unchanged():
             rep = e.autotune()
             t = e.tuning
             assert str(t["chunk"]) in rep["spatial_chunk"] and t["chunk"] == rep["best_chunk"]
-            assert str(t["unit_size"]) in rep["temporal_unit"] and t["unit_size"] == rep["best_unit"]
+            key = ("r16:" if t["variant"] else "") + str(t["unit_size"])
+            assert key in rep["temporal_unit"] and t["unit_size"] == rep["best_unit"]
+            assert t["variant"] == rep["best_variant"]
+            assert any(k.startswith("r16:") for k in rep["temporal_unit"])  # TPAD 1024 has both variants
             assert min(rep["spatial_chunk"].values()) == pytest.approx(rep["us_per_frame"], rel=1e-3)
         e.ingest_frames(frames, slots, 1 / 65535)
         e.compute_temporal(order, mask)
@@ -36,4 +40,4 @@ def test_autotune_report_and_results_unchanged():
     for k in range(32):
         sc = np.abs(b.D2()[k]).max()
         if sc > 0:
-            assert np.abs(a.D2()[k] - b.D2()[k]).max() <= 1e-10 * sc
+            assert np.abs(a.D2()[k] - b.D2()[k]).max() <= 1e-5 * sc

@@ -289,3 +289,30 @@ def test_errors():
     eng.destroy()
     with pytest.raises(H.DdmError):
         eng.read_radial()
+
+
+@pytest.mark.parametrize("variant", [0, 1])
+def test_radial_both_temporal_variants(variant):
+    """Both temporal kernels (one-group radix-8; two-group radix-16, the
+    autotuner's choice at TPAD 1024..4096) against the FP64 oracle at
+    TPAD 1024: radial D within 1e-4 of each bin's scale."""
+    N, T, L = 64, 512, 96
+    sim = dict(O.BASE, N=N, T=T, seed=17, swimmers=dict(n=20, vbar=20.0, sigma=8.0, geometry="3d"),
+               passive=dict(n=20), dropExact=23)
+    frames, valid, _ = O.simulate(sim)
+    idx = np.nonzero(valid)[0]
+    eng = _engine(N=N, T=T, L=L, NB=12, kmin=2, kmax=28)
+    eng.set_tuning(0, 0, variant)
+    assert eng.tuning["variant"] == variant
+    eng.ingest_frames(frames[idx], idx)
+    order, mask = O.linear_order(valid)
+    eng.compute_temporal(order, mask)
+    rg = eng.read_radial()
+    hist = O.history_ingest(O.luma_of(frames[idx]), idx.astype(np.int32), T)
+    ro = O.analyze_radial(hist, order, mask, O.make_bins(N, 12, 2, 28), L)
+    D = rg.D2()
+    for b in range(12):
+        sc = ro["D"][b].max()
+        if sc > 0:
+            assert np.abs(D[b] - ro["D"][b]).max() <= 1e-4 * sc, b
+    eng.destroy()

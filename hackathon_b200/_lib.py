@@ -13,6 +13,33 @@ DDM_OK, DDM_ERR_ARG, DDM_ERR_CUDA, DDM_ERR_STATE, DDM_ERR_NOMEM, DDM_ERR_NODEV =
 DTYPES = {"u8": 0, "u16": 1, "f32": 2}
 
 
+class RadialView(C.Structure):
+    _fields_ = [("N", C.c_int32), ("NB", C.c_int32), ("L", C.c_int32), ("knodes", C.c_int32),
+                ("kCenter", C.c_void_p), ("kNodes", C.c_void_p), ("nModes", C.c_void_p), ("D", C.c_void_p),
+                ("P", C.c_void_p), ("drift", C.c_void_p)]
+
+
+class MotilityOptions(C.Structure):
+    _fields_ = [("dxUm", C.c_double), ("fps", C.c_double), ("geometry2d", C.c_int32),
+                ("exposureLocked", C.c_int32), ("swimMin", C.c_double)]
+
+
+class MotilityFit(C.Structure):
+    _fields_ = [(k, C.c_double) for k in ("vbar", "Z", "Dd", "Vmag", "alpha", "rss")]
+
+
+class MotilityResult(C.Structure):
+    _fields_ = [("verdict", C.c_int32), ("physicsVerdict", C.c_int32), ("insufficient", C.c_int32),
+                ("TSI", C.c_double), ("alpha", C.c_double), ("alphaResolved", C.c_int32),
+                ("resolvedBins", C.c_int32), ("vbar", C.c_double), ("sigmaV", C.c_double), ("Z", C.c_double),
+                ("Ddiff", C.c_double), ("DdiffBrownian", C.c_double), ("dBIC", C.c_double),
+                ("driftVx", C.c_double), ("driftVy", C.c_double), ("driftMag", C.c_double),
+                ("driftSigma", C.c_double), ("driftAngleDeg", C.c_double), ("driftSignificant", C.c_int32),
+                ("driftPairs", C.c_int32), ("driftSamples", C.c_double), ("mu", C.c_double),
+                ("nData", C.c_int32), ("nEff", C.c_double), ("rho", C.c_double), ("nbins", C.c_int32),
+                ("nlags", C.c_int32), ("swim", MotilityFit), ("brown", MotilityFit)]
+
+
 class Geometry(C.Structure):
     _fields_ = [("N", C.c_int32), ("T", C.c_int32), ("TPAD", C.c_int32), ("L", C.c_int32),
                 ("NB", C.c_int32), ("kmin", C.c_double), ("kmax", C.c_double),
@@ -51,6 +78,8 @@ _SIGS = {
     "ddm_autotune": (C.c_int, [_vp, C.c_char_p, _i32]),
     "ddm_get_tuning": (C.c_int, [_vp, C.POINTER(_i32), C.POINTER(_i32), C.POINTER(_i32)]),
     "ddm_set_tuning": (C.c_int, [_vp, _i32, _i32, _i32]),
+    "ddm_analyze_motility": (C.c_int, [C.POINTER(RadialView), C.POINTER(MotilityOptions),
+                                       C.POINTER(MotilityResult)]),
     "ddm_batch_create": (C.c_int, [_vp, _i32, C.POINTER(_vp)]),
     "ddm_batch_destroy": (None, [_vp]),
     "ddm_batch_last_error": (C.c_char_p, [_vp]),

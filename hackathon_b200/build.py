@@ -54,7 +54,10 @@ def build(force=False, verbose=False, ptxas_info=False):
         obj = os.path.join(obj_dir, os.path.basename(src) + ".o")
         cmd = [nvcc, *ARCH, *FLAGS, *extra, "-c", src, "-o", obj]
         if src.endswith(".cpp"):
-            cmd = [nvcc, *FLAGS, "-Wno-deprecated-gpu-targets", "-x", "c++", "-c", src, "-o", obj]
+            # host FP64 code: IEEE operation order, no FMA contraction (the
+            # reference's JavaScript arithmetic)
+            cmd = [nvcc, *FLAGS, "-Wno-deprecated-gpu-targets", "-Xcompiler", "-ffp-contract=off", "-x", "c++",
+                   "-c", src, "-o", obj]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"compile failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")

@@ -162,6 +162,55 @@ int ddm_set_tuning(ddm_engine *h, int32_t chunk, int32_t unit_size, int32_t vari
 int64_t ddm_kernel_launches(const ddm_engine *h);
 
 /* ---------------------------------------------------------------------------
+ * Decision layer: analyzeMotility (motility-ddm/src/motility_fit.js:853-990)
+ * on a Radial record -- Brownian, Brownian+drift and swimmer fits (VarPro +
+ * bounded Nelder-Mead, the reference's start sets), phase drift, temporal
+ * structure index, BIC with the residual autocorrelation, q-scaling, and the
+ * five gates -> verdict. Host FP64 like the reference's fit worker; the
+ * Radial record is the one ddm_read_radial returns with the engine's bins. */
+typedef struct ddm_radial_view {
+  int32_t N, NB, L, knodes;
+  const double *kCenter;   /* [NB] */
+  const double *kNodes;    /* [NB*knodes] */
+  const uint32_t *nModes;  /* [NB] */
+  const double *D;         /* [NB*L] */
+  const double *P;         /* [NB] */
+  const double *drift;     /* [NB*L*8] */
+} ddm_radial_view;
+
+typedef struct ddm_motility_options {
+  double dxUm, fps;        /* pixel pitch (um) and frame rate (1/s) */
+  int32_t geometry2d;      /* 0: 3D swimmers ('3d'), 1: in-plane ('2d') */
+  int32_t exposureLocked;  /* 0 gives UNLOCKED_EXPOSURE (gate G5) */
+  double swimMin;          /* GATES.SWIM_MIN_UM_S, 2 in the reference */
+} ddm_motility_options;
+
+typedef struct ddm_motility_fit {
+  double vbar, Z, Dd, Vmag, alpha, rss;
+} ddm_motility_fit;
+
+/* verdict: 0 MOTILE, 1 NOT_MOTILE, 2 DIRECTED_TRANSPORT, 3 NO_DYNAMICS,
+ * 4 UNLOCKED_EXPOSURE (motility_fit.js:40-46); fields as the reference's
+ * result object (motility_fit.js:918-990). */
+typedef struct ddm_motility_result {
+  int32_t verdict, physicsVerdict, insufficient;
+  double TSI, alpha;
+  int32_t alphaResolved, resolvedBins;
+  double vbar, sigmaV, Z, Ddiff, DdiffBrownian, dBIC;
+  double driftVx, driftVy, driftMag, driftSigma, driftAngleDeg;
+  int32_t driftSignificant, driftPairs;
+  double driftSamples;
+  double mu;
+  int32_t nData;
+  double nEff, rho;
+  int32_t nbins, nlags;
+  ddm_motility_fit swim, brown;
+} ddm_motility_result;
+
+int ddm_analyze_motility(const ddm_radial_view *radial, const ddm_motility_options *opt,
+                         ddm_motility_result *out);
+
+/* ---------------------------------------------------------------------------
  * Batches: many videos of uneven size and frame count analysed together (no
  * counterpart in the reference, whose engine holds one video). A batch
  * borrows existing engines (any geometries, one device; the caller keeps

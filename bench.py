@@ -29,7 +29,6 @@ import argparse
 import json
 import os
 import statistics
-import subprocess
 import sys
 import threading
 import time
@@ -61,64 +60,69 @@ def _peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clock and throttle-reason samples during the timed region."""
+    """SM clock and clock-event (throttle) reasons sampled every 5 ms during
+    the timed region, through NVML (the counters nvidia-smi's
+    clocks.sm / clocks_event_reasons.* report). Read-only: no setting of the
+    GPU is changed."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", 0x8), ("sw_thermal_slowdown", 0x20), ("hw_thermal_slowdown", 0x40),
+               ("sw_power_cap", 0x4))
 
-    def __init__(self, index):
-        self.index = index
-        self.proc = None
-        self.lines = []
+    def __init__(self, cuda_index):
+        self.cuda_index = cuda_index
+        self.samples = []
+        self.window = None
+        self._stop = threading.Event()
+        self.t = None
+
+    def _handle(self, nv):
+        import torch
+        try:
+            return nv.nvmlDeviceGetHandleByUUID("GPU-" + str(torch.cuda.get_device_properties(self.cuda_index).uuid))
+        except Exception:
+            return nv.nvmlDeviceGetHandleByIndex(self.cuda_index)
 
     def start(self):
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits", "-lms", "20",
-                 "-i", str(self.index)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
-            self.t.start()
-        except (OSError, ValueError):
-            self.proc = None
+            import pynvml as nv
+            nv.nvmlInit()
+            self.nv, self.h = nv, self._handle(nv)
+            self.max_mhz = nv.nvmlDeviceGetMaxClockInfo(self.h, nv.NVML_CLOCK_SM)
+        except Exception:
+            self.nv = None
+            return
+        self.t = threading.Thread(target=self._run, daemon=True)
+        self.t.start()
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append((time.perf_counter(), line.strip()))
+    def _run(self):
+        nv, h = self.nv, self.h
+        while not self._stop.is_set():
+            try:
+                self.samples.append((time.perf_counter(), nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM),
+                                     nv.nvmlDeviceGetCurrentClocksEventReasons(h)))
+            except Exception:
+                return
+            time.sleep(0.005)
 
     def mark(self, t0, t1):
-        """Host-time window of the timed region (samples outside are dropped
-        unless none fall inside)."""
+        """Host-time window of the timed region; only samples inside it count
+        (all samples, if none fell inside)."""
         self.window = (t0, t1)
 
     def stop(self):
-        if not self.proc:
+        if self.t is None:
             return None
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        w = getattr(self, "window", None)
-        inside = [ln for t, ln in self.lines if w and w[0] <= t <= w[1]]
-        for ln in inside or [ln for _, ln in self.lines]:
-            f = [x.strip() for x in ln.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                sm.append(float(f[1]))
-                mx = float(f[2])
-            except ValueError:
-                continue
-            for nm, v in zip(names, f[5:9]):
-                if v.lower() == "active":
-                    reasons.add(nm)
-        if not sm:
+        self._stop.set()
+        self.t.join(timeout=2)
+        w = self.window
+        inside = [s for s in self.samples if w and w[0] <= s[0] <= w[1]]
+        use = inside or self.samples
+        if not use:
             return None
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm), "samples_inside_timed_region": len(inside)}
+        reasons = sorted({nm for _, _, r in use for nm, bit in self.REASONS if r & bit})
+        return {"sm_mhz": statistics.median(m for _, m, _ in use), "sm_max_mhz": float(self.max_mhz),
+                "reasons": reasons, "samples": len(use), "samples_inside_timed_region": len(inside),
+                "source": "NVML, 5 ms period"}
 
 
 def _profile_traffic():
@@ -240,7 +244,7 @@ def run_reference(args, rank, world):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")

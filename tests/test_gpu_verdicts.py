@@ -45,6 +45,9 @@ def test_scenario_on_gpu(sc, golden):
     if "vbar" in pub:
         assert abs(res["vbar"] - pub["vbar"]) <= 0.06
     assert abs(res["driftMag"] - pub["V"]) <= 0.006
+    if "angle" in pub:
+        d = abs(res["driftAngleDeg"] - pub["angle"]) % 360
+        assert min(d, 360 - d) <= 0.6
     ref, _, _ = O.run_scenario(sc)
     assert res["verdict"] == ref["verdict"]
     if ref["verdict"] == "MOTILE":

@@ -8,8 +8,9 @@
 // B200 formulation, two kernels per chunk of frames:
 //  rows_kernel  stages batches of raw u8/u16/f32 rows (and the spatial mask's
 //               rows) into shared memory with bulk copies, converts, subtracts
-//               a frame reference level c_f (mean of four fixed pixels of the
-//               frame, exact in FP32 for integer frames), multiplies by
+//               a frame reference level c_f (mean of a fixed 16 x 16 grid of
+//               the frame's pixels, reduced in a fixed order so that every
+//               CTA gets the same value; exact for integer frames), multiplies by
 //               w(x) w(y) scale m(x,y), and transforms two rows per complex
 //               FFT (real-input packing). It writes the row spectra to an
 //               L2-resident scratch in a [frame][kx/2][y][2] blocked layout,
@@ -58,10 +59,15 @@ __host__ __device__ constexpr int GSTRIDE() {
   return 2 * padded(N) + 2;
 }
 
-// The pixels whose mean is a frame's reference level c_f.
+// The pixels whose mean is a frame's reference level c_f: a 16 x 16 grid at
+// the centres of N/16 x N/16 cells, pixel i of the 256 read by thread i. The
+// closer c_f is to the frame mean, the smaller the offset the FP32
+// transforms carry and the correction term (c_f - mu) FFT2(w m) has to
+// cancel (the error of that cancellation grows with N).
+constexpr int CREF = 256;
 template <int N>
 __device__ __forceinline__ int cref_offset(int i) {
-  return (N / 4 + (i >> 1) * (N / 2)) * N + N / 4 + (i & 1) * (N / 2);
+  return ((2 * (i >> 4) + 1) * (N / 32)) * N + (2 * (i & 15) + 1) * (N / 32);
 }
 
 // Persistent: each CTA walks batches of G row pairs (2G consecutive rows of
@@ -115,29 +121,42 @@ __global__ void __launch_bounds__(256) rows_kernel(RowParams p) {
   float wxs[8];  // w(x) at this thread's columns, fixed for the whole kernel
 #pragma unroll
   for (int q = 0; q < 8; q++) wxs[q] = __ldg(&p.win[t + q * NT]);
-  // reference pixels of the first batch's frame (raw loads, converted at use
-  // so that the prefetch never waits on them)
-  Tin cpx[4];
-  {
-    const long long f = blockIdx.x < nbatch ? blockIdx.x / BPF : 0;
-#pragma unroll
-    for (int i = 0; i < 4; i++) cpx[i] = __ldg(frames + f * p.frame_stride + cref_offset<N>(i));
-  }
   // pixel sums: exact integers for u8/u16 (warp totals < 2^31), FP64 for f32
   constexpr bool INT = !std::is_floating_point<Tin>::value;
   using acc_t = typename std::conditional<INT, int, double>::type;
+  static_assert(WARPS * 32 == CREF, "one reference pixel per thread");
+  __shared__ acc_t cred[WARPS];
+  // c_f of a frame from the warp sums in cred[] (fixed order: bit-identical
+  // in every CTA)
+  auto cref_of = [&]() {
+    acc_t c = 0;
+#pragma unroll
+    for (int w = 0; w < WARPS; w++) c += cred[w];
+    return (float)((double)c * (1.0 / CREF));
+  };
+  auto cref_warp = [&](Tin px) {
+    acc_t c = (acc_t)px;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    if ((threadIdx.x & 31) == 0) cred[threadIdx.x >> 5] = c;
+  };
+  {  // the first batch's frame
+    const long long f = blockIdx.x < nbatch ? blockIdx.x / BPF : 0;
+    cref_warp(__ldg(frames + f * p.frame_stride + cref_offset<N>(threadIdx.x)));
+  }
   __syncthreads();
+  float cf_next = cref_of();
   int it = 0;
   for (long long b = blockIdx.x; b < nbatch; b += gridDim.x, it++) {
     const int st = it % ROW_STAGES;
     const int f = (int)(b / BPF);
     const int r = (int)(b % BPF);
-    const float cf = 0.25f * (((float)cpx[0] + (float)cpx[1]) + ((float)cpx[2] + (float)cpx[3]));
-    {  // next batch's reference pixels
+    const float cf = cf_next;
+    Tin cpx;  // next batch's reference pixel (raw load, reduced after the FFT's loads)
+    {
       const long long bn = b + gridDim.x;
       const long long fn = bn < nbatch ? bn / BPF : f;
-#pragma unroll
-      for (int i = 0; i < 4; i++) cpx[i] = __ldg(frames + fn * p.frame_stride + cref_offset<N>(i));
+      cpx = __ldg(frames + fn * p.frame_stride + cref_offset<N>(threadIdx.x));
     }
     if (!mbar_wait(&bar[st], (uint32_t)(it / ROW_STAGES) & 1u, p.err, 2)) {
       // give up: let this CTA's other copies in flight land (bounded), then stop
@@ -171,8 +190,10 @@ __global__ void __launch_bounds__(256) rows_kernel(RowParams p) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = (double)s;
+    cref_warp(cpx);
     const float2* Z = fft<N, false, true, SYNC>(v, t, buf0, buf1, s_tw, 1 + g);
-    __syncthreads();  // red[] complete; every thread is done with stage st
+    __syncthreads();  // red[], cred[] complete; every thread is done with stage st
+    cf_next = cref_of();
     if (threadIdx.x == 0) {
       const long long bn = b + (long long)ROW_STAGES * gridDim.x;
       if (bn < nbatch) issue(bn, st);

@@ -575,6 +575,202 @@ __global__ void __launch_bounds__(NP / 8, TemporalBounds<NP>::MIN_BLOCKS) tempor
   }
 }
 
+// ---------------------------------------------------------------------------
+// One-group radix-16 kernel for TPAD 8192, where the staged kernels above do
+// not fit shared memory (three exchange buffers of 64 KB plus 128 KB of
+// staged rows). NP/16 = 512 threads, 16 points per thread, in-place
+// exchange buffers: F for the transforms of one mode, Z for the packed p
+// spectrum of the pair (2 x 64 KB). The time series are gathered straight
+// from the history (read-only path); the rows of the pair after this one are
+// prefetched into L2 while this pair's transforms run. Twiddles come from the
+// FP64-derived radix-16 table through L1. Per pair (a, b), as above:
+//   Z = FFT(p_a + i p_b);  for s in (a, b): Y = FFT(x_s), W = IFFT(V_s)
+// with V_s = |Y|^2 + i 2 Re(conj(M) P_s), then the fused radial epilogue or
+// the full per-mode outputs.
+__device__ __forceinline__ void prefetch_rows_l2(const float2* row, int T, int t, int nth) {
+  const int lines = T * (int)sizeof(float2) / 128;  // whole lines inside the row
+  const char* base = reinterpret_cast<const char*>(row);
+  for (int i = t; i < lines; i += nth) asm volatile("prefetch.global.L2 [%0];" ::"l"(base + 128 * (size_t)i));
+}
+
+template <int NP, int LPT, bool FULL>
+__global__ void __launch_bounds__(NP / 16, 1) temporal_big_kernel(TemporalParams p) {
+  constexpr int NTH = NP / 16;
+  extern __shared__ __align__(16) float2 sm[];
+  float2* bufF = sm;
+  float2* bufZ = sm + NP;
+  float* s_np = (float*)(sm + 2 * NP);
+  __shared__ int s_next;
+  const int t = threadIdx.x;
+  const float invn = 0.5f / NP;
+  const float2* __restrict__ tw = p.tw16;
+
+  const int4* v_items = nullptr;
+  const float2* v_mspec = nullptr;
+  const float2* v_hist = nullptr;
+  double* v_partials = nullptr;
+  int cur_v = -1, L = 0, v_T = 0, v_unit0 = 0, v_nunits = 0;
+  float np0 = 0.f;
+  int om[8];  // slot of each of this thread's samples, -1 where masked or beyond T
+  auto load_video = [&](int vi) {
+    const VideoDesc vd = video_of(p, vi);
+    cur_v = vi;
+    L = vd.L;
+    v_T = vd.T;
+    v_hist = vd.hist;
+    v_items = vd.items;
+    v_mspec = vd.mspec;
+    v_partials = vd.partials;
+    v_unit0 = vd.unit0;
+    v_nunits = vd.nunits;
+    np0 = vd.npairs[0];
+    for (int i = t; i < L; i += NTH) s_np[i] = vd.npairs[i];
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      const int i = t + q * NTH;
+      om[q] = (i < vd.T && __ldg(&vd.mask[i]) != 0.f) ? (int)__ldg(&vd.order[i]) : -1;
+    }
+  };
+  if (t == 0) s_next = atomicAdd(p.unit_counter, 1);
+  __syncthreads();
+  int u = s_next;
+  __syncthreads();
+  int k = 0;
+  double acc[LPT][PFIELDS];
+  double accP = 0.0;
+#pragma unroll
+  for (int r = 0; r < LPT; r++)
+#pragma unroll
+    for (int c = 0; c < PFIELDS; c++) acc[r][c] = 0.0;
+
+  while (u < p.nunits) {
+    const int4 U = p.units[u];
+    const int vi = p.videos ? U.w : 0;
+    if (vi != cur_v) {
+      __syncthreads();  // s_np is no longer read
+      load_video(vi);
+      __syncthreads();
+    }
+    const bool hasb = k + 1 < U.y;
+    const int4 ea = load_item(v_items, U.x + k);
+    const int4 eb = hasb ? load_item(v_items, U.x + k + 1) : ea;
+    const float2* __restrict__ rowa = v_hist + (size_t)ea.x * v_T;
+    const float2* __restrict__ rowb = v_hist + (size_t)eb.x * v_T;
+    if (k + 2 < U.y) {
+      prefetch_rows_l2(v_hist + (size_t)load_item(v_items, U.x + k + 2).x * v_T, v_T, t, NTH);
+      if (k + 3 < U.y) prefetch_rows_l2(v_hist + (size_t)load_item(v_items, U.x + k + 3).x * v_T, v_T, t, NTH);
+    }
+    float2 v[16];
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      const bool on = om[q] >= 0;
+      const float2 xa = on ? __ldg(&rowa[om[q]]) : make_float2(0.f, 0.f);
+      const float2 xb = on && hasb ? __ldg(&rowb[om[q]]) : make_float2(0.f, 0.f);
+      v[q] = make_float2(fmaf(xa.x, xa.x, xa.y * xa.y), fmaf(xb.x, xb.x, xb.y * xb.y));
+    }
+#pragma unroll
+    for (int q = 8; q < 16; q++) v[q] = make_float2(0.f, 0.f);
+    fft16<NP, false>(v, t, bufZ, tw, 0);  // ends with a barrier after its last store
+    const float2 zsum = bufZ[0];          // (sum p_a, sum p_b)
+
+#pragma unroll 1
+    for (int s = 0; s < 2; s++) {
+      if (s == 1 && !hasb) break;
+      const int4 e = s ? eb : ea;
+      const float2* __restrict__ row = s ? rowb : rowa;
+#pragma unroll
+      for (int q = 0; q < 8; q++) v[q] = om[q] >= 0 ? __ldg(&row[om[q]]) : make_float2(0.f, 0.f);
+#pragma unroll
+      for (int q = 8; q < 16; q++) v[q] = make_float2(0.f, 0.f);
+      // the first store of each transform waits for the whole CTA, so the
+      // previous readers of F (epilogue, spectrum) are done by then
+      fft16<NP, false>(v, t, bufF, tw, 0);
+      spectrum16<NP>(v, t, bufF, bufZ, v_mspec, s == 1);
+      fft16<NP, true>(v, t, bufF, tw, 0);
+      const float2* W = bufF;
+      const float ps = s ? zsum.y : zsum.x;
+      const float P = np0 > 0.5f ? ps / np0 : 0.f;
+      if (FULL) {
+        const size_t mode = (size_t)e.x;
+        for (int tau = t; tau < L; tau += NTH) {
+          const float np = s_np[tau];
+          const float inv = np > 0.5f ? 1.f / np : 0.f;
+          const float2 w0 = W[pad16(tau)];
+          const float2 w1 = W[pad16((NP - tau) & (NP - 1))];
+          const float gx = (w0.x + w1.x) * invn, gy = (w0.y - w1.y) * invn;
+          const float ee = (w0.y + w1.y) * invn;
+          p.outD[mode * L + tau] = (ee - 2.f * gx) * inv;
+          p.outC[mode * L + tau] = make_float2(gx * inv, gy * inv);
+        }
+        if (t == 0) p.outP[mode] = P;
+      } else {
+        const double kx = e.y, ky = e.z;
+#pragma unroll
+        for (int r = 0; r < LPT; r++) {
+          const int tau = t + r * NTH;
+          if (tau < L) {
+            const float n0 = s_np[tau];
+            const float inp = n0 > 0.5f ? 1.f / n0 : 0.f;
+            const float2 w0 = W[pad16(tau)];
+            const float2 w1 = W[pad16((NP - tau) & (NP - 1))];
+            const float gx = (w0.x + w1.x) * invn, gy = (w0.y - w1.y) * invn;
+            const float ee = (w0.y + w1.y) * invn;
+            acc[r][0] += (double)((ee - 2.f * gx) * inp);
+            if (tau + 1 < L) {
+              const float n1 = s_np[tau + 1];
+              const float inp1 = n1 > 0.5f ? 1.f / n1 : 0.f;
+              const float2 u0 = W[pad16(tau + 1)];
+              const float2 u1 = W[pad16((NP - tau - 1) & (NP - 1))];
+              const float cx = gx * inp, cy = gy * inp;
+              const float c1x = (u0.x + u1.x) * invn * inp1;
+              const float c1y = (u0.y - u1.y) * invn * inp1;
+              const float zr = fmaf(c1x, cx, c1y * cy);  // C(tau+1) conj C(tau)
+              const float zi = fmaf(c1y, cx, -c1x * cy);
+              const float wgt = sqrtf(fmaf(zr, zr, zi * zi));
+              if (wgt > 0.f) {
+                const double wd = wgt, ph = atan2f(zi, zr);
+                acc[r][1] += wd;
+                acc[r][2] += wd * kx * kx;
+                acc[r][3] += wd * kx * ky;
+                acc[r][4] += wd * ky * ky;
+                acc[r][5] += wd * kx * ph;
+                acc[r][6] += wd * ky * ph;
+                acc[r][7] += wd * ph * ph;
+                acc[r][8] += 1.0;
+              }
+            }
+          }
+        }
+        accP += (double)P;
+      }
+    }
+    if (k + 2 >= U.y) {
+      if (!FULL) {
+        const int ul = u - v_unit0;
+#pragma unroll
+        for (int r = 0; r < LPT; r++) {
+          const int tau = t + r * NTH;
+          if (tau < L)
+#pragma unroll
+            for (int c = 0; c < PFIELDS; c++) {
+              v_partials[((size_t)ul * PFIELDS + c) * L + tau] = acc[r][c];
+              acc[r][c] = 0.0;
+            }
+        }
+        if (t == 0) v_partials[(size_t)v_nunits * PFIELDS * L + ul] = accP;
+        accP = 0.0;
+      }
+      if (t == 0) s_next = atomicAdd(p.unit_counter, 1);
+      __syncthreads();
+      u = s_next;
+      k = 0;
+    } else {
+      k += 2;
+    }
+    __syncthreads();  // the epilogue is done with F and s_next before they are rewritten
+  }
+}
+
 // Sums the unit partials of each bin in unit order (deterministic), divides
 // D and P by the bin's mode count (ddm_ref.js:404-412) and writes the
 // reference's Radial layout: D[b*L+tau], P[b], drift[(b*L+tau)*8+c].
@@ -670,22 +866,46 @@ static size_t temporal16_smem(int T, int L) {
   return sizeof(float2) * (3 * (size_t)NP + 4 * (size_t)T + tw_size16(NP)) + sizeof(float) * (size_t)L;
 }
 
+// TPAD 8192 runs the one-group radix-16 kernel with in-place buffers, for
+// both epilogues: the staged kernels need more shared memory than a CTA has.
+__host__ __device__ constexpr bool use_big(int NP) { return NP >= 8192; }
+
+template <int NP>
+static size_t temporal_big_smem(int L) {
+  return sizeof(float2) * 2 * (size_t)NP + sizeof(float) * (size_t)L;
+}
+
+// lags per thread of the big kernel (NP/16 threads)
+static int lpt_big(int TPAD, int L) {
+  const int NTH = TPAD / 16;
+  const int r = (L + NTH - 1) / NTH;
+  return r <= 1 ? 1 : r <= 2 ? 2 : r <= 4 ? 4 : 8;
+}
+
 template <int NP, int LPT, bool FULL>
 static cudaError_t launch_k(const TemporalParams& p, int grid, cudaStream_t s) {
-  if constexpr (use16(NP, FULL)) {
-    if (p.variant == 1) {
-      auto k = temporal16_kernel<NP, LPT>;
-      const size_t sm = temporal16_smem<NP>(p.T, p.L);
-      cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-      k<<<grid, NP / 8, sm, s>>>(p);
-      return cudaGetLastError();
+  if constexpr (use_big(NP)) {
+    auto k = temporal_big_kernel<NP, LPT, FULL>;
+    const size_t sm = temporal_big_smem<NP>(p.L);
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k<<<grid, NP / 16, sm, s>>>(p);
+    return cudaGetLastError();
+  } else {
+    if constexpr (use16(NP, FULL)) {
+      if (p.variant == 1) {
+        auto k = temporal16_kernel<NP, LPT>;
+        const size_t sm = temporal16_smem<NP>(p.T, p.L);
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        k<<<grid, NP / 8, sm, s>>>(p);
+        return cudaGetLastError();
+      }
     }
+    auto k = temporal_kernel<NP, LPT, FULL>;
+    const size_t sm = temporal_smem<NP>(p.T, p.L);
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k<<<grid, NP / 8, sm, s>>>(p);
+    return cudaGetLastError();
   }
-  auto k = temporal_kernel<NP, LPT, FULL>;
-  const size_t sm = temporal_smem<NP>(p.T, p.L);
-  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-  k<<<grid, NP / 8, sm, s>>>(p);
-  return cudaGetLastError();
 }
 
 template <typename K>
@@ -700,9 +920,13 @@ static int occupancy_grid(K k, int threads, size_t smem) {
 
 template <int NP, int LPT, bool FULL>
 static int grid_of(int T, int L, int variant) {
-  if constexpr (use16(NP, FULL))
-    if (variant == 1) return occupancy_grid(temporal16_kernel<NP, LPT>, NP / 8, temporal16_smem<NP>(T, L));
-  return occupancy_grid(temporal_kernel<NP, LPT, FULL>, NP / 8, temporal_smem<NP>(T, L));
+  if constexpr (use_big(NP)) {
+    return occupancy_grid(temporal_big_kernel<NP, LPT, FULL>, NP / 16, temporal_big_smem<NP>(L));
+  } else {
+    if constexpr (use16(NP, FULL))
+      if (variant == 1) return occupancy_grid(temporal16_kernel<NP, LPT>, NP / 8, temporal16_smem<NP>(T, L));
+    return occupancy_grid(temporal_kernel<NP, LPT, FULL>, NP / 8, temporal_smem<NP>(T, L));
+  }
 }
 
 template <int NP>
@@ -711,6 +935,22 @@ static cudaError_t dispatch_np(int T, int L, bool full, const TemporalParams* p,
   if (full) {
     if (grid_out) *grid_out = grid_of<NP, 1, true>(T, L, variant);
     return p ? launch_k<NP, 1, true>(*p, grid, s) : cudaSuccess;
+  }
+  if constexpr (use_big(NP)) {
+    switch (lpt_big(NP, L)) {
+      case 1:
+        if (grid_out) *grid_out = grid_of<NP, 1, false>(T, L, variant);
+        return p ? launch_k<NP, 1, false>(*p, grid, s) : cudaSuccess;
+      case 2:
+        if (grid_out) *grid_out = grid_of<NP, 2, false>(T, L, variant);
+        return p ? launch_k<NP, 2, false>(*p, grid, s) : cudaSuccess;
+      case 4:
+        if (grid_out) *grid_out = grid_of<NP, 4, false>(T, L, variant);
+        return p ? launch_k<NP, 4, false>(*p, grid, s) : cudaSuccess;
+      default:
+        if (grid_out) *grid_out = grid_of<NP, 8, false>(T, L, variant);
+        return p ? launch_k<NP, 8, false>(*p, grid, s) : cudaSuccess;
+    }
   }
   switch (lpt_of(NP, L)) {
     case 1:

@@ -229,10 +229,11 @@ def test_ring_slots_wrap():
     eng.destroy()
 
 
-@pytest.mark.parametrize("N", [128, 512])
+@pytest.mark.parametrize("N", [128, 512, 2048])
 def test_spectrum_sizes(N):
-    """Other ROI sizes (extension): 2D spectrum vs the FP64 oracle."""
-    T = 8
+    """Other ROI sizes (extension; 2048 is the large streamed configuration's
+    ROI): 2D spectrum vs the FP64 oracle."""
+    T = 8 if N <= 512 else 4
     rng = np.random.default_rng(N)
     frames = rng.integers(0, 4096, (T, N, N)).astype(np.uint16)
     eng = _engine(N=N, T=T, L=4, NB=8, kmin=2, kmax=N // 4)
@@ -315,4 +316,42 @@ def test_radial_both_temporal_variants(variant):
         sc = ro["D"][b].max()
         if sc > 0:
             assert np.abs(D[b] - ro["D"][b]).max() <= 1e-4 * sc, b
+    eng.destroy()
+
+
+@pytest.mark.parametrize("N,L,NB,kmax", [(64, 128, 12, 28), (64, 2100, 4, 14)])
+def test_temporal_tpad8192(N, L, NB, kmax):
+    """TPAD 8192 (T = 4096 frames, the large streamed configuration's time
+    axis): the one-group in-place radix-16 kernel, fused radial path (1 and 8
+    lags per thread) and full per-mode outputs, against the FP64 oracle."""
+    T = 4096
+    sim = dict(O.BASE, N=N, T=T, seed=23, swimmers=dict(n=6, vbar=20.0, sigma=8.0, geometry="3d"),
+               passive=dict(n=6), dropExact=81)
+    frames, valid, _ = O.simulate(sim)
+    idx = np.nonzero(valid)[0]
+    eng = _engine(N=N, T=T, L=L, NB=NB, kmin=2, kmax=kmax)
+    eng.ingest_frames(frames[idx], idx)
+    order, mask = O.linear_order(valid)
+    order, mask = O.shuffle_order(order, mask, 7) if L > 2048 else (order, mask)
+    eng.compute_temporal(order, mask)
+    rg = eng.read_radial()
+    hist = O.history_ingest(O.luma_of(frames[idx]), idx.astype(np.int32), T)
+    bins = O.make_bins(N, NB, 2, kmax)
+    ro = O.analyze_radial(hist, order, mask, bins, L)
+    D = rg.D2()
+    for b in range(NB):
+        sc = ro["D"][b].max()
+        if sc > 0:
+            assert np.abs(D[b] - ro["D"][b]).max() <= 1e-4 * sc, b
+    assert np.allclose(rg.P, ro["P"], rtol=1e-5, atol=0)
+    if L <= 2048:
+        eng.compute_temporal(order, mask, full=True)
+        g = eng.read_temporal_full()
+        modes = np.unique(bins["binModes"][:, 0])[::7].astype(np.int32)
+        Do, Co, Po = O.analyze_modes(hist, order, mask, L, modes)
+        ok = Po > 0
+        eD = np.abs(g["D"][modes][ok] - Do[ok]) / (2 * Po[ok, None])
+        eC = np.abs(g["C"][modes][ok] - Co[ok]) / Po[ok, None]
+        assert _p99(eD.ravel()) < 1e-4 and _p99(eC.ravel()) < 1e-4
+        assert np.allclose(g["P"][modes][ok], Po[ok], rtol=1e-4, atol=0)
     eng.destroy()

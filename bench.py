@@ -241,6 +241,150 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+LARGE = dict(N=2048, T=4096, TPAD=8192, L=128, NB=1024, KMIN=4.0, KMAX=800.0)
+LARGE_METRIC = "DDM frames/s at 2048²×4096 (large streamed run)"
+LARGE_WORKLOAD = ("2048x2048x4096 u16 video: 40,000 blobs sigma 2 px with the 512x1024 workload's motility "
+                  "statistics, 5% stuck pixels excluded by a pixel mask, Poisson noise mean 400 counts, 2% "
+                  "dropped frames; TPAD=8192, L=128 lags, 1024 q-bins (kmin 4, kmax 800)")
+
+
+def run_large(args, rank, world, dist):
+    """The large streamed configuration: one 2048^2 x 4096 video per GPU
+    (68.8 GB history). value: frames already in HBM; e2e: the frames streamed
+    from host memory through the engine's pinned staging, radial read back.
+    Full-size checks: fused radial == radial of the full per-mode outputs,
+    D(q, 0) = 0, all finite."""
+    import psutil
+    import torch
+
+    import hackathon_b200 as H
+    from hackathon_b200 import replicas as R
+    from hackathon_b200 import synth
+    g = dict(LARGE)
+    if args.frames:  # a shorter video of the same frames (profiling, smoke runs)
+        g["T"] = args.frames
+        g["TPAD"] = max(128, 1 << (2 * args.frames - 1).bit_length())
+    N, T, L, NB = g["N"], g["T"], g["L"], g["NB"]
+    L = g["L"] = min(L, T)
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(local)
+    spec = synth.large(seed=R.rank_seed(1, rank))
+    spec.T = T
+    t_gen = time.perf_counter()
+    frames, valid, _ = synth.generate(spec)
+    torch.cuda.synchronize()
+    t_gen = time.perf_counter() - t_gen
+    slots = np.arange(T, dtype=np.int32)
+    order = np.arange(T, dtype=np.uint32)
+    tmask = valid.astype(np.float32)
+    eng = H.DdmEngine.create(N=N, T=T, TPAD=g["TPAD"], L=L, NB=NB, kmin=g["KMIN"], kmax=g["KMAX"])
+    eng.set_spatial_mask(synth.hot_mask(spec))
+    tune = eng.autotune()
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    eng.set_stream(stream.cuda_stream)
+    scale = 1.0 / 65535
+    for _ in range(max(args.warmup, 3)):
+        eng.ingest_frames(frames, slots, scale)
+        eng.compute_temporal(order, tmask, full=False, wait=False)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    l0 = eng.kernel_launches
+    ev = [tuple(torch.cuda.Event(enable_timing=True) for _ in range(3)) for _ in range(args.steps)]
+    h0 = time.perf_counter()
+    for i in range(args.steps):
+        ev[i][0].record(stream)
+        eng.ingest_frames(frames, slots, scale)
+        ev[i][1].record(stream)
+        eng.compute_temporal(order, tmask, full=False, wait=False)
+        ev[i][2].record(stream)
+    torch.cuda.synchronize()
+    clocks.mark(h0, time.perf_counter())
+    launches = eng.kernel_launches - l0
+    clk = clocks.stop()
+    ms = ev[0][0].elapsed_time(ev[-1][2])
+    t_sp = statistics.mean(a.elapsed_time(b) for a, b, _ in ev)
+    t_tm = statistics.mean(b.elapsed_time(c) for _, b, c in ev)
+    ms_step = R.max_over_ranks(ms, dist, device="cuda") / args.steps
+    value = R.weak_scaling_throughput(T, ms_step, world)
+    fused = eng.read_radial()
+
+    # full-size consistency: the full-output path's radial equals the fused one
+    eng.compute_temporal(order, tmask, full=True)
+    full = eng.read_radial()
+    D1, D2 = fused.D2(), full.D2()
+    sc = np.abs(D1).max(axis=1, keepdims=True)
+    checks = {"finite": bool(np.isfinite(D1).all() and np.isfinite(fused.P).all() and np.isfinite(fused.drift).all()),
+              "fused_vs_full_D_max_rel": float((np.abs(D1 - D2) / np.where(sc > 0, sc, 1)).max()),
+              "fused_vs_full_P_max_rel": float(np.abs(fused.P / np.where(full.P > 0, full.P, 1) - 1)[full.P > 0].max()),
+              "D0_max_rel": float((np.abs(D1[:, 0:1]) / np.where(sc > 0, sc, 1)).max())}
+
+    # e2e from host memory: the whole video in pageable host memory when it
+    # fits, streamed by the engine's pinned staging (frames -> HBM) each step
+    need = frames.numel() * 2
+    avail = psutil.virtual_memory().available
+    e2e = None
+    if args.e2e_steps > 0 and avail > 1.5 * need:
+        host = frames.view(torch.int16).cpu()
+        pinned = avail > 3 * need
+        if pinned:  # page-locked: the copies run at the link's rate
+            host = host.pin_memory()
+        rad_bytes = 8 * (NB * L + NB + NB * L * 8)
+        eng.ingest_frames(host[:64], slots[:64], scale)  # staging warm
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.e2e_steps):
+            eng.ingest_frames(host, slots, scale)
+            eng.compute_temporal(order, tmask, full=False, wait=False)
+            eng.read_radial()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms_e2e = R.max_over_ranks(e0.elapsed_time(e1), dist, device="cuda")
+        e2e = {"value": R.weak_scaling_throughput(T * args.e2e_steps, ms_e2e, world), "unit": "frames/s",
+               "h2d_bytes_per_step": int(need), "d2h_bytes_per_step": rad_bytes,
+               "host_memory": "pinned" if pinned else "pageable, staged through the engine's pinned ring"}
+        del host
+    else:
+        e2e = {"value": None, "unit": "frames/s",
+               "unavailable": "no e2e steps requested" if args.e2e_steps <= 0 else
+               f"host memory {avail / 2**30:.0f} GiB < 1.5 x video"}
+
+    peak, peak_kind = _peaks()
+    nbinned = int(eng.bins["binOffsets"][-1])
+    sp_bytes = T * (N * N * 2 + eng.modes * BYTES_PER_MODE_SLOT)
+    tm_bytes = nbinned * T * BYTES_PER_MODE_SLOT
+    TP = g["TPAD"]
+    stages = {"spatial": {"ms": t_sp, "bytes": sp_bytes, "GBps": sp_bytes / (t_sp * 1e6),
+                          "gflop": T * (N + 1) * 5 * N * np.log2(N) / 1e9},
+              "temporal": {"ms": t_tm, "bytes": tm_bytes, "GBps": tm_bytes / (t_tm * 1e6),
+                           "gflop": nbinned * 2.5 * 5 * TP * np.log2(TP) / 1e9}}
+    for s in stages.values():
+        s["frac"] = s["GBps"] / peak
+        s["fp32_frac_of_nominal"] = s["gflop"] / s["ms"] / FP32_NOMINAL_TFLOPS
+    tm = stages["temporal"]
+    roof = {"bound": "hbm", "kernel": "temporal_big_kernel", "achieved": tm["GBps"], "peak": peak, "unit": "GB/s",
+            "frac": tm["frac"], "peak_source": peak_kind, "traffic": None, "algorithmic_bytes": tm_bytes,
+            "stages": stages}
+    if rank == 0:
+        line = {"metric": LARGE_METRIC, "value": value, "unit": "frames/s", "n_gpus": world, "steps": args.steps,
+                "warmup": max(args.warmup, 3), "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded GPU generator, hackathon_b200/synth.py large())",
+                "config": {"workload": LARGE_WORKLOAD, **{k.lower(): v for k, v in g.items()},
+                           "binned_modes": nbinned, "history_bytes": eng.modes * T * 8,
+                           "l2": "inputs larger than L2", "generation_s": t_gen,
+                           "autotuned": {"chunk": tune["best_chunk"], "unit": tune["best_unit"],
+                                         "temporal_variant": tune["best_variant"]}},
+                "e2e": e2e, "gpu_launches": int(launches), "roofline": roof, "clocks": clk, "checks": checks}
+        print(json.dumps(line), flush=True)
+    eng.destroy()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -251,6 +395,9 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-fit", action="store_true", help="skip the q-fits/s (surrogate + LM) section")
     ap.add_argument("--tuning", default="", help="chunk,unit[,variant]: apply instead of autotuning")
+    ap.add_argument("--workload", default="config2", choices=["config2", "large"],
+                    help="large: one 2048^2 x 4096 video per GPU (68.8 GB history), its own JSON line")
+    ap.add_argument("--frames", type=int, default=0, help="large workload: frames per video (default 4096)")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", 0))
@@ -263,6 +410,12 @@ def main():
         import torch.distributed as dist
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    if args.impl == "ours" and args.workload == "large":
+        run_large(args, rank, world, dist)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
     if args.impl == "reference":
         run_reference(args, rank, world)
         if dist:

@@ -324,8 +324,11 @@ extern "C" int ddm_create(const ddm_geometry *geometry, ddm_engine **out) {
     size_t c = std::max<size_t>(1, target / per);
     c = std::min<size_t>(MAX_CHUNK, std::max<size_t>(c, fg));
     h->chunk = (int)(c / fg * fg);  // whole column-kernel frame groups
-    // buffers hold up to chunk_cap frames, so the autotuner may pick larger chunks
-    h->chunk_cap = std::max(h->chunk, std::min<int>(MAX_CHUNK, (int)std::max<size_t>(fg, (96u << 20) / per)) / fg * fg);
+    // buffers hold up to chunk_cap frames, so the autotuner may pick larger
+    // chunks (at N >= 1024 one frame's scratch is 4 MB or more and a chunk
+    // of four, the column kernel's tile, already passes the L2 target)
+    const size_t cap_bytes = g.N >= 1024 ? (288u << 20) : (96u << 20);
+    h->chunk_cap = std::max(h->chunk, std::min<int>(MAX_CHUNK, (int)std::max<size_t>(fg, cap_bytes / per)) / fg * fg);
   }
   h->bins = make_bins(g.N, g.NB, g.kmin, g.kmax, g.knodes);
   int rc = DDM_OK;

@@ -331,6 +331,148 @@ __global__ void __launch_bounds__(256) cols_kernel(ColParams p) {
   }
 }
 
+// Column pass for N >= 1024, where fewer than four FFT groups of N/8 threads
+// fit a CTA. A tile is (column pair kb, four frames): the frames' row-spectrum
+// blocks stream through a two-deep ring of bulk copies (one block per group
+// at a time, G frames per ring entry), each group transforms both columns of
+// its frame into the tile's output slabs R[c][frame] (the transform's last
+// ping-pong buffer), and the CTA then stores four consecutive ring slots of a
+// mode together -- one full 32 B sector. With one frame per tile every
+// history store covered a quarter sector and the memory controller had to
+// read-modify-write it (about 4x the algorithmic DRAM traffic at N = 2048).
+constexpr int WIDE_F = 4;  // frames per tile of the wide column kernel
+
+template <int N>
+__global__ void __launch_bounds__(256, 1) cols_wide_kernel(ColParams p) {
+  constexpr int NT = N / 8;
+  constexpr int G = row_groups<N>();  // 1 (N = 2048) or 2 (N = 1024)
+  constexpr int F = WIDE_F;
+  constexpr int SYNC = sync_kind(N, G);
+  constexpr uint32_t FRAME_ELEMS = N * KB;
+  constexpr uint32_t FRAME_BYTES = FRAME_ELEMS * sizeof(float2);
+  constexpr uint32_t ITEM_ELEMS = G * FRAME_ELEMS;
+  static_assert(F % G == 0, "groups divide the tile's frames");
+  static_assert((fft_stages(N) & 1) == 0, "the transform must end in its second buffer (the output slab)");
+  extern __shared__ __align__(16) float2 sm[];
+  float2* ring = sm;                   // [2][G][N][KB] staged blocks
+  float2* R = ring + 2 * ITEM_ELEMS;   // [KB][F][N] column transforms of the tile
+  float2* scr = R + KB * F * N;        // [G][N] first ping-pong buffer of each group
+  float2* s_tw = scr + G * N;
+  __shared__ __align__(8) uint64_t bar[2];
+  __shared__ float s_dc[F];
+  __shared__ float2 s_wc4[4];
+  const int g = threadIdx.x / NT, t = threadIdx.x % NT;
+  for (int i = threadIdx.x; i < tw_size(N); i += blockDim.x) s_tw[i] = p.tw[i];
+  if (threadIdx.x < 4) s_wc4[threadIdx.x] = p.wc4[threadIdx.x];
+  const int nfg = (p.nframes + F - 1) / F;
+  const int ntiles = p.NHB * nfg;
+  const float invN = 1.f / N;
+  const double inv_total = p.inv_total[0];
+  // item (tile, j): frames f0 + j*G .. f0 + j*G + G - 1 of the tile (those < nframes)
+  auto items_of = [&](int tile) {
+    const int f0 = (tile / p.NHB) * F;
+    return (min(F, p.nframes - f0) + G - 1) / G;
+  };
+  auto issue = [&](int tile, int j, int s) {
+    const int kb = tile % p.NHB, f0 = (tile / p.NHB) * F + j * G;
+    const int nf = min(G, p.nframes - f0);
+    mbar_arrive_expect_tx(&bar[s], nf * FRAME_BYTES);
+    for (int i = 0; i < nf; i++)
+      bulk_g2s(ring + s * ITEM_ELEMS + i * FRAME_ELEMS,
+               p.rows + ((size_t)(f0 + i) * p.NHB + kb) * FRAME_ELEMS, FRAME_BYTES, &bar[s]);
+  };
+  // the item after (tile, j) in this CTA's sequence
+  auto advance = [&](int& tile, int& j) {
+    if (++j >= items_of(tile)) {
+      j = 0;
+      tile += gridDim.x;
+    }
+  };
+  // thread 0 keeps the issue cursor two items ahead of the consumer
+  int it_tile = blockIdx.x, it_j = 0;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fence_barrier_init();
+    for (int s = 0; s < 2 && it_tile < ntiles; s++) {
+      issue(it_tile, it_j, s);
+      advance(it_tile, it_j);
+    }
+  }
+  __syncthreads();
+  int e = 0;  // items consumed by this CTA
+  constexpr int SPT = 256 / F;  // ky stride of the store loop
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int kb = tile % p.NHB;
+    const int f0 = (tile / p.NHB) * F;
+    const int nf = min(F, p.nframes - f0);
+    if (threadIdx.x < nf) {
+      const int f = f0 + threadIdx.x;
+      const double mu = p.framesum[f] * inv_total;
+      s_dc[threadIdx.x] = (float)(((double)p.framec[f] - mu) * (double)p.scale / N);
+      if (kb == 0) p.means[f] = mu * (double)p.scale;
+    }
+    const int nit = (nf + G - 1) / G;
+    for (int j = 0; j < nit; j++, e++) {
+      const int s = e & 1;
+      if (!mbar_wait(&bar[s], (uint32_t)(e >> 1) & 1u, p.err, 3)) {
+        // give up: let the other copy in flight land (bounded), then stop
+        mbar_wait(&bar[s ^ 1], (uint32_t)((e + 1) >> 1) & 1u, nullptr, 0);
+        return;
+      }
+      const int fi = j * G + g;  // this group's frame within the tile
+      const bool fvalid = fi < nf;
+      const float2* blk = ring + s * ITEM_ELEMS + g * FRAME_ELEMS;
+#pragma unroll 1
+      for (int c = 0; c < KB; c++) {
+        float2 v[8];
+#pragma unroll
+        for (int q = 0; q < 8; q++) v[q] = fvalid ? blk[(t + q * NT) * KB + c] : make_float2(0.f, 0.f);
+        if (c == KB - 1) {
+          // every thread has read ring entry s: its next copy may land
+          fence_proxy_async_smem();
+          __syncthreads();
+          if (threadIdx.x == 0 && it_tile < ntiles) {
+            issue(it_tile, it_j, s);
+            advance(it_tile, it_j);
+          }
+        }
+        fft<N, false, true, SYNC>(v, t, scr + g * N, R + (size_t)(c * F + fi) * N, s_tw, 1 + g);
+      }
+    }
+    __syncthreads();  // R and s_dc complete
+    // store: thread -> (frame sf, ky); lanes 4k..4k+3 write one mode's four slots
+    const int sf = threadIdx.x % F;
+    if (sf < nf) {
+      const int slot = p.slots[f0 + sf];
+      const float dc = s_dc[sf];
+      const size_t mstride = (size_t)p.NH * p.T;
+#pragma unroll 1
+      for (int c = 0; c < KB; c++) {
+        const int kx = kb * KB + c;
+        if (kx >= p.NH) break;
+        const float2* ys = R + (size_t)(c * F + sf) * N;
+        float2* hs = p.hist + (size_t)kx * p.T + slot;
+        const float2 wkx = kx < 4 ? s_wc4[kx] : make_float2(0.f, 0.f);
+#pragma unroll 4
+        for (int i = 0; i < N / SPT; i++) {
+          const int ky = threadIdx.x / F + i * SPT;
+          const float2 y = ys[pad(ky)];
+          float2 w = make_float2(0.f, 0.f);
+          if (p.w2d) {
+            w = __ldg(&p.w2d[(size_t)kx * N + ky]);
+          } else if (kx < 4 && (ky < 4 || ky > N - 4)) {
+            const float2 wk = ky < 4 ? s_wc4[ky] : make_float2(s_wc4[N - ky].x, -s_wc4[N - ky].y);
+            w = cmul(wkx, wk);
+          }
+          hs[(size_t)ky * mstride] = make_float2(fmaf(dc, w.x, y.x * invN), fmaf(dc, w.y, y.y * invN));
+        }
+      }
+    }
+    __syncthreads();  // R and s_dc are rewritten by the next tile
+  }
+}
+
 // ------------------------------------------------------------------ launchers
 
 template <int N>
@@ -404,9 +546,26 @@ cudaError_t launch_rows(int N, int dtype, const RowParams& p, cudaStream_t s) {
   }
 }
 
+// the wide column kernel (four frames per tile) where fewer than four FFT
+// groups fit a CTA
+__host__ __device__ constexpr bool use_wide_cols(int N) { return N >= 1024; }
+
+template <int N>
+static size_t cols_wide_smem() {
+  constexpr int G = groups<N>();
+  return ((size_t)2 * G * N * KB + (size_t)KB * WIDE_F * N + (size_t)G * N + tw_size(N)) * sizeof(float2);
+}
+
 template <int N>
 static cudaError_t cols_n(const ColParams& p, cudaStream_t s) {
   constexpr int G = groups<N>();
+  if constexpr (use_wide_cols(N)) {
+    auto k = cols_wide_kernel<N>;
+    const size_t sm = cols_wide_smem<N>();
+    const int grid = persistent_grid(k, G * (N / 8), sm, (long long)p.NHB * ((p.nframes + WIDE_F - 1) / WIDE_F));
+    k<<<grid, G * (N / 8), sm, s>>>(p);
+    return cudaGetLastError();
+  }
   auto k = cols_kernel<N>;
   const size_t sm = fft_smem<N>() + (size_t)G * N * KB * sizeof(float2);
   const int grid = persistent_grid(k, G * (N / 8), sm, (long long)p.NHB * ((p.nframes + G - 1) / G));
@@ -426,6 +585,6 @@ cudaError_t launch_cols(int N, const ColParams& p, cudaStream_t s) {
   }
 }
 
-int frames_per_col_cta(int N) { return N >= 2048 ? 1 : 256 / (N / 8); }
+int frames_per_col_cta(int N) { return use_wide_cols(N) ? WIDE_F : 256 / (N / 8); }
 
 }  // namespace ddm

@@ -4,9 +4,9 @@ Follows the semantics of the reference's simulator (motility-ddm/test/sim.mjs:
 90-186): Gaussian blobs on a periodic N x N field, straight swimmers with
 Schulz (Gamma) distributed speeds gamma(Z+1, vbar/(Z+1)) and 3D-isotropic
 headings seen in projection, plus Brownian motion, and randomly dropped
-frames. It extends it the way the benchmark workload asks: uint16 frames with
-Poisson shot noise around a mean count, a circular ROI mask, and sizes up to
-2048^2 x 4096.
+frames. It extends it the way the benchmark workloads ask: uint16 frames with
+Poisson shot noise around a mean count, a circular ROI mask or stuck ("hot")
+pixels excluded by a pixel mask, and sizes up to 2048^2 x 4096.
 
 Rendering: a separable Gaussian blob is an outer product gy (x) gx, so a frame
 is Gy^T Gx over all particles -- one batched FP32 GEMM per chunk of frames.
@@ -33,6 +33,8 @@ class VideoSpec:
     blob_peak: float = 300.0    # blob peak, counts
     roi_radius: float = 230.0   # circular ROI (<= 0: none)
     drop_frac: float = 0.02
+    hot_frac: float = 0.0       # share of stuck pixels (excluded by hot_mask)
+    hot_counts: float = 65000.0  # their value
     seed: int = 1
 
 
@@ -40,6 +42,26 @@ def config2(seed=1):
     """512^2 x 1024 uint16 mixed-motility video with a circular ROI and 2 %
     dropped frames (the benchmark's headline workload)."""
     return VideoSpec(seed=seed)
+
+
+def large(seed=1):
+    """2048^2 x 4096 uint16 video with the mixed-motility statistics above,
+    40,000 blobs and 5 % hot pixels (the large streamed configuration)."""
+    return VideoSpec(N=2048, T=4096, n_blobs=40000, roi_radius=0.0, hot_frac=0.05, seed=seed)
+
+
+def _hot_pixels(spec):
+    rng = np.random.default_rng(spec.seed * 104729 + 3)
+    return np.flatnonzero(rng.random(spec.N * spec.N) < spec.hot_frac)
+
+
+def hot_mask(spec):
+    """Pixel mask (1 = used) that excludes the stuck pixels, or None."""
+    if spec.hot_frac <= 0:
+        return None
+    m = np.ones(spec.N * spec.N, np.uint8)
+    m[_hot_pixels(spec)] = 0
+    return m.reshape(spec.N, spec.N)
 
 
 def roi_mask(spec):
@@ -51,9 +73,12 @@ def roi_mask(spec):
     return (((x - c) ** 2 + (y - c) ** 2) <= spec.roi_radius ** 2).astype(np.uint8)
 
 
-def generate(spec, device="cuda", chunk=64):
+def generate(spec, device="cuda", chunk=None):
     """Returns (frames u16 [T, N, N] on `device`, valid bool [T] numpy,
-    truth dict)."""
+    truth dict). `chunk` frames are rendered at once (default: 64, fewer
+    when the per-frame blob profiles would pass 2 GB)."""
+    if chunk is None:
+        chunk = int(max(1, min(64, 2e9 // (spec.n_blobs * 2 * spec.N * 8))))
     g = torch.Generator(device=device)
     g.manual_seed(spec.seed)
     N, T, P = spec.N, spec.T, spec.n_blobs
@@ -75,6 +100,7 @@ def generate(spec, device="cuda", chunk=64):
     bg = spec.mean_counts - spec.blob_peak * P * 2 * np.pi * spec.sigma ** 2 / (N * N)
     grid = torch.arange(N, device=dev, dtype=torch.float64)
     frames = torch.empty((T, N, N), dtype=torch.int16, device=dev)
+    hot = torch.as_tensor(_hot_pixels(spec), device=dev) if spec.hot_frac > 0 else None
     pos = x0.clone()
     inv2s2 = 1.0 / (2 * spec.sigma ** 2)
     for t0 in range(0, T, chunk):
@@ -91,6 +117,8 @@ def generate(spec, device="cuda", chunk=64):
         img = torch.bmm(gy.transpose(1, 2), gx)             # [m, N(y), N(x)]
         lam = (bg + spec.blob_peak * img).clamp_min(0)
         cnt = torch.poisson(lam, generator=g).clamp_(0, 65535)
+        if hot is not None:
+            cnt.view(m, N * N)[:, hot] = spec.hot_counts
         frames[t0:t0 + m] = cnt.to(torch.int32).to(torch.int16)
     rng = np.random.default_rng(spec.seed * 7919 + 13)
     valid = np.ones(T, bool)

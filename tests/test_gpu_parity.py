@@ -229,17 +229,20 @@ def test_ring_slots_wrap():
     eng.destroy()
 
 
-@pytest.mark.parametrize("N", [128, 512, 2048])
+@pytest.mark.parametrize("N", [128, 512, 1024, 2048])
 def test_spectrum_sizes(N):
     """Other ROI sizes (extension; 2048 is the large streamed configuration's
-    ROI): 2D spectrum vs the FP64 oracle."""
-    T = 8 if N <= 512 else 4
+    ROI): 2D spectrum vs the FP64 oracle. At 1024 and 2048 the column pass
+    works on tiles of four frames: 1024 also covers a partial tile (six
+    frames) and slots that are not consecutive."""
+    T = {1024: 6, 2048: 4}.get(N, 8)
     rng = np.random.default_rng(N)
     frames = rng.integers(0, 4096, (T, N, N)).astype(np.uint16)
+    slots = rng.permutation(T).astype(np.int32) if N == 1024 else np.arange(T, dtype=np.int32)
     eng = _engine(N=N, T=T, L=4, NB=8, kmin=2, kmax=N // 4)
-    eng.ingest_frames(frames, np.arange(T), 1.0 / 4095)
+    eng.ingest_frames(frames, slots, 1.0 / 4095)
     g = eng.read_history()
-    hist = O.history_ingest(frames.astype(np.float64) / 4095, np.arange(T, dtype=np.int32), T)
+    hist = O.history_ingest(frames.astype(np.float64) / 4095, slots, T)
     rms = np.sqrt(np.mean(np.abs(hist) ** 2))
     assert np.abs(g - hist).max() / rms < 2e-5
     eng.destroy()

@@ -412,6 +412,15 @@ __global__ void __launch_bounds__(256, 1) cols_wide_kernel(ColParams p) {
       s_dc[threadIdx.x] = (float)(((double)p.framec[f] - mu) * (double)p.scale / N);
       if (kb == 0) p.means[f] = mu * (double)p.scale;
     }
+    if (p.w2d && threadIdx.x == 0) {
+      // the correction rows of this tile's columns, read by the store loop
+      // after the transforms: into L2 now (one bulk prefetch), so those reads
+      // do not wait on DRAM
+      const int ncol = min(KB, p.NH - kb * KB);
+      asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p.w2d + (size_t)kb * KB * N),
+                   "r"((uint32_t)(ncol * N * sizeof(float2)))
+                   : "memory");
+    }
     const int nit = (nf + G - 1) / G;
     for (int j = 0; j < nit; j++, e++) {
       const int s = e & 1;
@@ -454,18 +463,41 @@ __global__ void __launch_bounds__(256, 1) cols_wide_kernel(ColParams p) {
         const float2* ys = R + (size_t)(c * F + sf) * N;
         float2* hs = p.hist + (size_t)kx * p.T + slot;
         const float2 wkx = kx < 4 ? s_wc4[kx] : make_float2(0.f, 0.f);
-#pragma unroll 4
-        for (int i = 0; i < N / SPT; i++) {
-          const int ky = threadIdx.x / F + i * SPT;
-          const float2 y = ys[pad(ky)];
-          float2 w = make_float2(0.f, 0.f);
-          if (p.w2d) {
-            w = __ldg(&p.w2d[(size_t)kx * N + ky]);
-          } else if (kx < 4 && (ky < 4 || ky > N - 4)) {
-            const float2 wk = ky < 4 ? s_wc4[ky] : make_float2(s_wc4[N - ky].x, -s_wc4[N - ky].y);
-            w = cmul(wkx, wk);
+        if (p.w2d) {
+          // correction table loads run one batch of WB ahead of the stores
+          constexpr int WB = 8, NI = N / SPT;
+          static_assert(NI % WB == 0, "store batches");
+          const float2* wcol = p.w2d + (size_t)kx * N + threadIdx.x / F;
+          float2 wcur[WB], wnxt[WB];
+#pragma unroll
+          for (int j = 0; j < WB; j++) wcur[j] = __ldg(&wcol[j * SPT]);
+#pragma unroll 1
+          for (int i0 = 0; i0 < NI; i0 += WB) {
+            if (i0 + WB < NI)
+#pragma unroll
+              for (int j = 0; j < WB; j++) wnxt[j] = __ldg(&wcol[(i0 + WB + j) * SPT]);
+#pragma unroll
+            for (int j = 0; j < WB; j++) {
+              const int ky = threadIdx.x / F + (i0 + j) * SPT;
+              const float2 y = ys[pad(ky)];
+              const float2 w = wcur[j];
+              hs[(size_t)ky * mstride] = make_float2(fmaf(dc, w.x, y.x * invN), fmaf(dc, w.y, y.y * invN));
+            }
+#pragma unroll
+            for (int j = 0; j < WB; j++) wcur[j] = wnxt[j];
           }
-          hs[(size_t)ky * mstride] = make_float2(fmaf(dc, w.x, y.x * invN), fmaf(dc, w.y, y.y * invN));
+        } else {
+#pragma unroll 8
+          for (int i = 0; i < N / SPT; i++) {
+            const int ky = threadIdx.x / F + i * SPT;
+            const float2 y = ys[pad(ky)];
+            float2 w = make_float2(0.f, 0.f);
+            if (kx < 4 && (ky < 4 || ky > N - 4)) {
+              const float2 wk = ky < 4 ? s_wc4[ky] : make_float2(s_wc4[N - ky].x, -s_wc4[N - ky].y);
+              w = cmul(wkx, wk);
+            }
+            hs[(size_t)ky * mstride] = make_float2(fmaf(dc, w.x, y.x * invN), fmaf(dc, w.y, y.y * invN));
+          }
         }
       }
     }

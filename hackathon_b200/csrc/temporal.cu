@@ -580,26 +580,24 @@ __global__ void __launch_bounds__(NP / 8, TemporalBounds<NP>::MIN_BLOCKS) tempor
 // not fit shared memory (three exchange buffers of 64 KB plus 128 KB of
 // staged rows). NP/16 = 512 threads, 16 points per thread, in-place
 // exchange buffers: F for the transforms of one mode, Z for the packed p
-// spectrum of the pair (2 x 64 KB). The time series are gathered straight
-// from the history (read-only path); the rows of the pair after this one are
-// prefetched into L2 while this pair's transforms run. Twiddles come from the
+// spectrum of the pair (2 x 64 KB), and one staging buffer for the pair's two
+// time series (bulk copy, 2 x T x 8 B <= 64 KB): the next pair's copy is
+// issued as soon as the last gather of this pair is done, so it lands while
+// this pair's remaining transforms and epilogue run. Twiddles come from the
 // FP64-derived radix-16 table through L1. Per pair (a, b), as above:
 //   Z = FFT(p_a + i p_b);  for s in (a, b): Y = FFT(x_s), W = IFFT(V_s)
 // with V_s = |Y|^2 + i 2 Re(conj(M) P_s), then the fused radial epilogue or
 // the full per-mode outputs.
-__device__ __forceinline__ void prefetch_rows_l2(const float2* row, int T, int t, int nth) {
-  const int lines = T * (int)sizeof(float2) / 128;  // whole lines inside the row
-  const char* base = reinterpret_cast<const char*>(row);
-  for (int i = t; i < lines; i += nth) asm volatile("prefetch.global.L2 [%0];" ::"l"(base + 128 * (size_t)i));
-}
-
 template <int NP, int LPT, bool FULL>
 __global__ void __launch_bounds__(NP / 16, 1) temporal_big_kernel(TemporalParams p) {
   constexpr int NTH = NP / 16;
   extern __shared__ __align__(16) float2 sm[];
   float2* bufF = sm;
   float2* bufZ = sm + NP;
-  float* s_np = (float*)(sm + 2 * NP);
+  const int TS = p.T;             // staging stride: the (largest) T
+  float2* stage = sm + 2 * NP;    // [2 rows][TS]
+  float* s_np = (float*)(stage + 2 * TS);
+  __shared__ __align__(8) uint64_t mbar;
   __shared__ int s_next;
   const int t = threadIdx.x;
   const float invn = 0.5f / NP;
@@ -607,17 +605,14 @@ __global__ void __launch_bounds__(NP / 16, 1) temporal_big_kernel(TemporalParams
 
   const int4* v_items = nullptr;
   const float2* v_mspec = nullptr;
-  const float2* v_hist = nullptr;
   double* v_partials = nullptr;
-  int cur_v = -1, L = 0, v_T = 0, v_unit0 = 0, v_nunits = 0;
+  int cur_v = -1, L = 0, v_unit0 = 0, v_nunits = 0;
   float np0 = 0.f;
   int om[8];  // slot of each of this thread's samples, -1 where masked or beyond T
   auto load_video = [&](int vi) {
     const VideoDesc vd = video_of(p, vi);
     cur_v = vi;
     L = vd.L;
-    v_T = vd.T;
-    v_hist = vd.hist;
     v_items = vd.items;
     v_mspec = vd.mspec;
     v_partials = vd.partials;
@@ -631,10 +626,21 @@ __global__ void __launch_bounds__(NP / 16, 1) temporal_big_kernel(TemporalParams
       om[q] = (i < vd.T && __ldg(&vd.mask[i]) != 0.f) ? (int)__ldg(&vd.order[i]) : -1;
     }
   };
-  if (t == 0) s_next = atomicAdd(p.unit_counter, 1);
+  if (t == 0) {
+    mbar_init(&mbar, 1);
+    fence_barrier_init();
+    s_next = atomicAdd(p.unit_counter, 1);
+  }
   __syncthreads();
   int u = s_next;
   __syncthreads();
+  if (t == 0) {
+    s_next = atomicAdd(p.unit_counter, 1);
+    if (u < p.nunits) issue_pair(p, u, 0, stage, TS, &mbar);
+  }
+  __syncthreads();
+  int unext = s_next;
+  uint32_t phase = 0;
   int k = 0;
   double acc[LPT][PFIELDS];
   double accP = 0.0;
@@ -651,21 +657,19 @@ __global__ void __launch_bounds__(NP / 16, 1) temporal_big_kernel(TemporalParams
       load_video(vi);
       __syncthreads();
     }
+    if (!mbar_wait(&mbar, phase, p.err, 1)) return;  // nothing else is in flight
+    phase ^= 1u;
     const bool hasb = k + 1 < U.y;
     const int4 ea = load_item(v_items, U.x + k);
     const int4 eb = hasb ? load_item(v_items, U.x + k + 1) : ea;
-    const float2* __restrict__ rowa = v_hist + (size_t)ea.x * v_T;
-    const float2* __restrict__ rowb = v_hist + (size_t)eb.x * v_T;
-    if (k + 2 < U.y) {
-      prefetch_rows_l2(v_hist + (size_t)load_item(v_items, U.x + k + 2).x * v_T, v_T, t, NTH);
-      if (k + 3 < U.y) prefetch_rows_l2(v_hist + (size_t)load_item(v_items, U.x + k + 3).x * v_T, v_T, t, NTH);
-    }
+    const float2* rowa = stage;
+    const float2* rowb = stage + TS;
     float2 v[16];
 #pragma unroll
     for (int q = 0; q < 8; q++) {
       const bool on = om[q] >= 0;
-      const float2 xa = on ? __ldg(&rowa[om[q]]) : make_float2(0.f, 0.f);
-      const float2 xb = on && hasb ? __ldg(&rowb[om[q]]) : make_float2(0.f, 0.f);
+      const float2 xa = on ? rowa[om[q]] : make_float2(0.f, 0.f);
+      const float2 xb = on && hasb ? rowb[om[q]] : make_float2(0.f, 0.f);
       v[q] = make_float2(fmaf(xa.x, xa.x, xa.y * xa.y), fmaf(xb.x, xb.x, xb.y * xb.y));
     }
 #pragma unroll
@@ -677,11 +681,23 @@ __global__ void __launch_bounds__(NP / 16, 1) temporal_big_kernel(TemporalParams
     for (int s = 0; s < 2; s++) {
       if (s == 1 && !hasb) break;
       const int4 e = s ? eb : ea;
-      const float2* __restrict__ row = s ? rowb : rowa;
+      const float2* row = s ? rowb : rowa;
 #pragma unroll
-      for (int q = 0; q < 8; q++) v[q] = om[q] >= 0 ? __ldg(&row[om[q]]) : make_float2(0.f, 0.f);
+      for (int q = 0; q < 8; q++) v[q] = om[q] >= 0 ? row[om[q]] : make_float2(0.f, 0.f);
 #pragma unroll
       for (int q = 8; q < 16; q++) v[q] = make_float2(0.f, 0.f);
+      if (s == 1 || !hasb) {
+        // the pair's last gather: every thread is done with the staged rows,
+        // so the next pair's copy may land there while this one finishes
+        fence_proxy_async_smem();
+        __syncthreads();
+        int nu = u, nk = k + 2;
+        if (nk >= U.y) {
+          nu = unext;
+          nk = 0;
+        }
+        if (t == 0 && nu < p.nunits) issue_pair(p, nu, nk, stage, TS, &mbar);
+      }
       // the first store of each transform waits for the whole CTA, so the
       // previous readers of F (epilogue, spectrum) are done by then
       fft16<NP, false>(v, t, bufF, tw, 0);
@@ -760,14 +776,14 @@ __global__ void __launch_bounds__(NP / 16, 1) temporal_big_kernel(TemporalParams
         if (t == 0) v_partials[(size_t)v_nunits * PFIELDS * L + ul] = accP;
         accP = 0.0;
       }
-      if (t == 0) s_next = atomicAdd(p.unit_counter, 1);
-      __syncthreads();
-      u = s_next;
+      u = unext;
       k = 0;
+      if (t == 0) s_next = atomicAdd(p.unit_counter, 1);
     } else {
       k += 2;
     }
-    __syncthreads();  // the epilogue is done with F and s_next before they are rewritten
+    __syncthreads();  // the epilogue is done with F; s_next is complete
+    unext = s_next;
   }
 }
 
@@ -871,8 +887,8 @@ static size_t temporal16_smem(int T, int L) {
 __host__ __device__ constexpr bool use_big(int NP) { return NP >= 8192; }
 
 template <int NP>
-static size_t temporal_big_smem(int L) {
-  return sizeof(float2) * 2 * (size_t)NP + sizeof(float) * (size_t)L;
+static size_t temporal_big_smem(int T, int L) {
+  return sizeof(float2) * (2 * (size_t)NP + 2 * (size_t)T) + sizeof(float) * (size_t)L;
 }
 
 // lags per thread of the big kernel (NP/16 threads)
@@ -886,7 +902,7 @@ template <int NP, int LPT, bool FULL>
 static cudaError_t launch_k(const TemporalParams& p, int grid, cudaStream_t s) {
   if constexpr (use_big(NP)) {
     auto k = temporal_big_kernel<NP, LPT, FULL>;
-    const size_t sm = temporal_big_smem<NP>(p.L);
+    const size_t sm = temporal_big_smem<NP>(p.T, p.L);
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     k<<<grid, NP / 16, sm, s>>>(p);
     return cudaGetLastError();
@@ -921,7 +937,7 @@ static int occupancy_grid(K k, int threads, size_t smem) {
 template <int NP, int LPT, bool FULL>
 static int grid_of(int T, int L, int variant) {
   if constexpr (use_big(NP)) {
-    return occupancy_grid(temporal_big_kernel<NP, LPT, FULL>, NP / 16, temporal_big_smem<NP>(L));
+    return occupancy_grid(temporal_big_kernel<NP, LPT, FULL>, NP / 16, temporal_big_smem<NP>(T, L));
   } else {
     if constexpr (use16(NP, FULL))
       if (variant == 1) return occupancy_grid(temporal16_kernel<NP, LPT>, NP / 8, temporal16_smem<NP>(T, L));

@@ -60,3 +60,28 @@ def test_exposure_gate_on_gpu():
     res = analyze_motility(_gpu_radial(sc), dxUm=sc["sim"]["dxUm"], fps=sc["sim"]["fps"], geometry=sc["geometry"],
                            exposureLocked=False)
     assert res["verdict"] == "UNLOCKED_EXPOSURE" and res["physicsVerdict"] == "MOTILE"
+
+
+def test_fit_worker_bin_fits_on_gpu():
+    """The fit-worker protocol serving GPU per-bin fits (opt binFits): the
+    reply carries the batched GPU LM's fits of every prepared bin, equal to a
+    direct fit_bins call; "seeded" on a record whose lag grid differs from
+    the surrogate's falls back to "plain" and says so."""
+    from hackathon_b200 import fit as F
+    from hackathon_b200.fit_worker import FitWorker
+    from hackathon_b200.surrogate import Surrogate
+    sc = O.SCENARIOS[0]
+    radial = _gpu_radial(sc)
+    base = dict(dxUm=sc["sim"]["dxUm"], fps=sc["sim"]["fps"], geometry=sc["geometry"])
+    net = Surrogate(batch_max=1024, seed=1)
+    with FitWorker(surrogate=net) as w:
+        res = w.run_fit(radial, dict(base, binFits="plain")).result(600)
+        res2 = w.run_fit(radial, dict(base, binFits="seeded")).result(600)
+    assert res["verdict"] == "MOTILE"
+    bf = res["binFits"]
+    pr, _, direct = F.fit_bins(radial, base["dxUm"], base["fps"], mode="plain")
+    assert bf["mode"] == "plain" and bf["bins"] == pr.bins.tolist()
+    assert np.array_equal(np.array(bf["cost"]), direct.cost)
+    assert np.array_equal(np.array(bf["alpha"]), direct.alpha)
+    assert res2["binFits"]["mode"] == "plain" and res2["binFits"]["cost"] == bf["cost"]
+    net.close()

@@ -37,6 +37,11 @@ struct ddm_engine {
   cudaStream_t own_stream = nullptr, stream = nullptr, copy_stream = nullptr;
   cudaEvent_t ready_ev[NSTAGE]{}, free_ev[NSTAGE]{}, meta_ev = nullptr;
   std::vector<cudaEvent_t> inflight;  // completion events of recent ingests
+  // live analyses run on their own stream, concurrently with later ingests
+  cudaStream_t ana_stream = nullptr;
+  cudaEvent_t ana_ev = nullptr, ingest_ev = nullptr;
+  bool ana_busy = false;          // a live analysis may still be running
+  bool radial_from_live = false;  // the radial record is a live analysis' snapshot
 
   // geometry tables
   BinTable bins;
@@ -124,6 +129,7 @@ static void release(ddm_engine *h) {
   cudaSetDevice(h->device);
   if (h->own_stream) cudaStreamSynchronize(h->own_stream);
   if (h->copy_stream) cudaStreamSynchronize(h->copy_stream);
+  if (h->ana_stream) cudaStreamSynchronize(h->ana_stream);
   void *dev[] = {h->d_hist, h->d_rows, h->d_rowc, h->d_framesum, h->d_means, h->d_win, h->d_wys, h->d_ninv,
                  h->d_invtot, h->d_tw_s, h->d_tw_t, h->d_tw_t16, h->d_wcorr4, h->d_wcorr_full, h->d_smask,
                  h->d_stage[0], h->d_stage[1], h->d_order, h->d_mask, h->d_npairs,
@@ -139,8 +145,11 @@ static void release(ddm_engine *h) {
   }
   for (cudaEvent_t e : h->inflight) cudaEventDestroy(e);
   if (h->meta_ev) cudaEventDestroy(h->meta_ev);
+  if (h->ana_ev) cudaEventDestroy(h->ana_ev);
+  if (h->ingest_ev) cudaEventDestroy(h->ingest_ev);
   if (h->own_stream) cudaStreamDestroy(h->own_stream);
   if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
+  if (h->ana_stream) cudaStreamDestroy(h->ana_stream);
   delete h;
 }
 
@@ -338,7 +347,8 @@ extern "C" int ddm_create(const ddm_geometry *geometry, ddm_engine **out) {
     return code;
   };
   if (cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking) != cudaSuccess) {
+      cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&h->ana_stream, cudaStreamNonBlocking) != cudaSuccess) {
     h->err = "stream creation failed";
     return bail(DDM_ERR_CUDA);
   }
@@ -348,6 +358,8 @@ extern "C" int ddm_create(const ddm_geometry *geometry, ddm_engine **out) {
     cudaEventCreateWithFlags(&h->free_ev[i], cudaEventDisableTiming);
   }
   cudaEventCreateWithFlags(&h->meta_ev, cudaEventDisableTiming);
+  cudaEventCreateWithFlags(&h->ana_ev, cudaEventDisableTiming);
+  cudaEventCreateWithFlags(&h->ingest_ev, cudaEventDisableTiming);
   const int N = g.N;
   h->stage_bytes = (size_t)h->chunk_cap * N * N * sizeof(float);
   if ((rc = dalloc(h, &h->d_hist, (size_t)h->modes * g.T)) ||
@@ -547,7 +559,7 @@ static int ingest_impl(ddm_engine *h, const void *frames, int dtype, int n, cons
   // the caller's host buffer is free once the copies have run
   CK(cudaStreamSynchronize(h->copy_stream));
   note_inflight(h);
-  h->radial_valid = false;
+  if (!h->radial_from_live) h->radial_valid = false;  // a live snapshot stays readable
   return DDM_OK;
 }
 
@@ -607,7 +619,7 @@ extern "C" int ddm_set_spatial_mask(ddm_engine *h, const uint8_t *mask) {
   return upload_mask_tables(h, mask);
 }
 
-static int temporal_impl(ddm_engine *h, const uint32_t *order, const float *mask, int full) {
+static int temporal_impl(ddm_engine *h, const uint32_t *order, const float *mask, int full, cudaStream_t st) {
   cudaSetDevice(h->device);
   const int T = h->g.T, L = h->g.L, TPAD = h->g.TPAD;
   if (!order || !mask) return fail(h, DDM_ERR_ARG, "computeTemporal: order/mask must have length %d", T);
@@ -626,11 +638,11 @@ static int temporal_impl(ddm_engine *h, const uint32_t *order, const float *mask
   for (int j = 0; j < T; j++) hm[j] = mask[j] != 0.f ? 1.f : 0.f;
   memcpy(hn, npairs.data(), sizeof(float) * L);
   memcpy(hs, mspec.data(), sizeof(float) * 2 * TPAD);
-  CK(cudaMemcpyAsync(h->d_order, ho, sizeof(uint32_t) * T, cudaMemcpyHostToDevice, h->stream));
-  CK(cudaMemcpyAsync(h->d_mask, hm, sizeof(float) * T, cudaMemcpyHostToDevice, h->stream));
-  CK(cudaMemcpyAsync(h->d_npairs, hn, sizeof(float) * L, cudaMemcpyHostToDevice, h->stream));
-  CK(cudaMemcpyAsync(h->d_mspec, hs, sizeof(float2) * TPAD, cudaMemcpyHostToDevice, h->stream));
-  CK(cudaEventRecord(h->meta_ev, h->stream));
+  CK(cudaMemcpyAsync(h->d_order, ho, sizeof(uint32_t) * T, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(h->d_mask, hm, sizeof(float) * T, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(h->d_npairs, hn, sizeof(float) * L, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(h->d_mspec, hs, sizeof(float2) * TPAD, cudaMemcpyHostToDevice, st));
+  CK(cudaEventRecord(h->meta_ev, st));
 
   TemporalParams tp{};
   tp.hist = h->d_hist;
@@ -659,8 +671,8 @@ static int temporal_impl(ddm_engine *h, const uint32_t *order, const float *mask
     tp.outC = h->d_fullC;
     tp.outP = h->d_fullP;
     const int grid = std::min(temporal_max_grid(TPAD, T, L, true), h->nunits_full);
-    CK(cudaMemsetAsync(h->d_counter, 0, sizeof(int), h->stream));
-    CKL(launch_temporal(TPAD, L, true, tp, std::max(grid, 1), h->stream));
+    CK(cudaMemsetAsync(h->d_counter, 0, sizeof(int), st));
+    CKL(launch_temporal(TPAD, L, true, tp, std::max(grid, 1), st));
     RadialFullParams rp{};
     rp.D = h->d_fullD;
     rp.C = h->d_fullC;
@@ -672,7 +684,7 @@ static int temporal_impl(ddm_engine *h, const uint32_t *order, const float *mask
     rp.oD = h->d_radD;
     rp.oP = h->d_radP;
     rp.odrift = h->d_radDrift;
-    CKL(launch_radial_full(rp, h->stream));
+    CKL(launch_radial_full(rp, st));
     h->full_valid = true;
   } else {
     tp.items = h->d_items;
@@ -680,8 +692,8 @@ static int temporal_impl(ddm_engine *h, const uint32_t *order, const float *mask
     tp.nunits = h->nunits;
     tp.partials = h->d_partials;
     const int grid = std::min(temporal_max_grid(TPAD, T, L, false, h->variant), h->nunits);
-    CK(cudaMemsetAsync(h->d_counter, 0, sizeof(int), h->stream));
-    if (h->nunits > 0) CKL(launch_temporal(TPAD, L, false, tp, std::max(grid, 1), h->stream));
+    CK(cudaMemsetAsync(h->d_counter, 0, sizeof(int), st));
+    if (h->nunits > 0) CKL(launch_temporal(TPAD, L, false, tp, std::max(grid, 1), st));
     ReduceParams rp{};
     rp.partials = h->d_partials;
     rp.bin_units = h->d_bin_units;
@@ -692,7 +704,7 @@ static int temporal_impl(ddm_engine *h, const uint32_t *order, const float *mask
     rp.D = h->d_radD;
     rp.P = h->d_radP;
     rp.drift = h->d_radDrift;
-    CKL(launch_reduce(rp, h->stream));
+    CKL(launch_reduce(rp, st));
     h->full_valid = false;
   }
   h->radial_valid = true;
@@ -713,31 +725,101 @@ static int check_device_error(ddm_engine *h) {
   return DDM_OK;
 }
 
+// Waits for a live analysis still in flight (it shares the temporal buffers
+// and the record the reads return) and surfaces its device error word.
+static int join_analysis(ddm_engine *h) {
+  if (!h->ana_busy) return DDM_OK;
+  CK(cudaEventSynchronize(h->ana_ev));
+  h->ana_busy = false;
+  return check_device_error(h);
+}
+
 extern "C" int ddm_compute_temporal_async(ddm_engine *h, const uint32_t *order, const float *mask,
                                           int32_t full) {
   if (!h) return DDM_ERR_ARG;
-  return temporal_impl(h, order, mask, full);
+  cudaSetDevice(h->device);
+  int rc = join_analysis(h);
+  if (rc) return rc;
+  h->radial_from_live = false;
+  return temporal_impl(h, order, mask, full, h->stream);
 }
 
 extern "C" int ddm_compute_temporal(ddm_engine *h, const uint32_t *order, const float *mask,
                                     int32_t full) {
   if (!h) return DDM_ERR_ARG;
-  int rc = temporal_impl(h, order, mask, full);
+  cudaSetDevice(h->device);
+  int rc = join_analysis(h);
   if (rc) return rc;
+  h->radial_from_live = false;
+  if ((rc = temporal_impl(h, order, mask, full, h->stream))) return rc;
   CK(cudaStreamSynchronize(h->stream));
   return check_device_error(h);
+}
+
+// Live analysis (the dashboard's analysis tick, main.ts:366-398, with
+// computeTemporal running while frames keep arriving, ddm-engine.ts:331-365):
+// the snapshot holds every frame queued on the ingest stream so far; the
+// analysis runs on its own stream and later ingests proceed concurrently.
+// Slots those ingests overwrite must be masked out of `mask` by the caller
+// (FrameClock.snapshot's guard). One live analysis at a time, as the
+// reference's temporalBusy.
+extern "C" int ddm_compute_temporal_live(ddm_engine *h, const uint32_t *order, const float *mask,
+                                         int32_t full) {
+  if (!h) return DDM_ERR_ARG;
+  cudaSetDevice(h->device);
+  if (h->ana_busy) {
+    const cudaError_t q = cudaEventQuery(h->ana_ev);
+    if (q == cudaErrorNotReady) {
+      cudaGetLastError();
+      return fail(h, DDM_ERR_STATE, "computeTemporal is already running");
+    }
+    int rc = join_analysis(h);
+    if (rc) return rc;
+  }
+  CK(cudaEventRecord(h->ingest_ev, h->stream));
+  CK(cudaStreamWaitEvent(h->ana_stream, h->ingest_ev, 0));
+  int rc = temporal_impl(h, order, mask, full, h->ana_stream);
+  if (rc) return rc;
+  CK(cudaEventRecord(h->ana_ev, h->ana_stream));
+  h->ana_busy = true;
+  h->radial_from_live = true;
+  return DDM_OK;
+}
+
+extern "C" int ddm_analysis_poll(ddm_engine *h, int32_t *done) {
+  if (!h || !done) return DDM_ERR_ARG;
+  cudaSetDevice(h->device);
+  *done = 1;
+  if (!h->ana_busy) return DDM_OK;
+  const cudaError_t q = cudaEventQuery(h->ana_ev);
+  if (q == cudaErrorNotReady) {
+    cudaGetLastError();
+    *done = 0;
+    return DDM_OK;
+  }
+  return join_analysis(h);
+}
+
+extern "C" int ddm_wait_analysis(ddm_engine *h) {
+  if (!h) return DDM_ERR_ARG;
+  cudaSetDevice(h->device);
+  return join_analysis(h);
 }
 
 extern "C" int ddm_read_radial(ddm_engine *h, double *D, double *P, double *drift) {
   if (!h) return DDM_ERR_ARG;
   cudaSetDevice(h->device);
+  int rc = join_analysis(h);
+  if (rc) return rc;
   if (!h->radial_valid) return fail(h, DDM_ERR_STATE, "readRadial: no computeTemporal since the last ingest");
   const size_t NB = h->g.NB, L = h->g.L;
-  if (D) CK(cudaMemcpyAsync(D, h->d_radD, sizeof(double) * NB * L, cudaMemcpyDeviceToHost, h->stream));
-  if (P) CK(cudaMemcpyAsync(P, h->d_radP, sizeof(double) * NB, cudaMemcpyDeviceToHost, h->stream));
-  if (drift)
-    CK(cudaMemcpyAsync(drift, h->d_radDrift, sizeof(double) * NB * L * DRIFT, cudaMemcpyDeviceToHost, h->stream));
-  CK(cudaStreamSynchronize(h->stream));
+  // a live snapshot's record is read on the analysis stream: no waiting for
+  // the ingests queued after it
+  cudaStream_t st = h->radial_from_live ? h->ana_stream : h->stream;
+  if (D) CK(cudaMemcpyAsync(D, h->d_radD, sizeof(double) * NB * L, cudaMemcpyDeviceToHost, st));
+  if (P) CK(cudaMemcpyAsync(P, h->d_radP, sizeof(double) * NB, cudaMemcpyDeviceToHost, st));
+  if (drift) CK(cudaMemcpyAsync(drift, h->d_radDrift, sizeof(double) * NB * L * DRIFT, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
   return check_device_error(h);
 }
 
@@ -753,13 +835,16 @@ extern "C" int ddm_read_history(ddm_engine *h, float *out) {
 extern "C" int ddm_read_temporal_full(ddm_engine *h, float *D, float *C, float *P) {
   if (!h) return DDM_ERR_ARG;
   cudaSetDevice(h->device);
+  int rc = join_analysis(h);
+  if (rc) return rc;
   if (!h->full_valid)
     return fail(h, DDM_ERR_STATE, "readTemporalFull: the last computeTemporal did not keep full outputs");
   const size_t M = h->modes, L = h->g.L;
-  if (D) CK(cudaMemcpyAsync(D, h->d_fullD, sizeof(float) * M * L, cudaMemcpyDeviceToHost, h->stream));
-  if (C) CK(cudaMemcpyAsync(C, h->d_fullC, sizeof(float2) * M * L, cudaMemcpyDeviceToHost, h->stream));
-  if (P) CK(cudaMemcpyAsync(P, h->d_fullP, sizeof(float) * M, cudaMemcpyDeviceToHost, h->stream));
-  CK(cudaStreamSynchronize(h->stream));
+  cudaStream_t st = h->radial_from_live ? h->ana_stream : h->stream;
+  if (D) CK(cudaMemcpyAsync(D, h->d_fullD, sizeof(float) * M * L, cudaMemcpyDeviceToHost, st));
+  if (C) CK(cudaMemcpyAsync(C, h->d_fullC, sizeof(float2) * M * L, cudaMemcpyDeviceToHost, st));
+  if (P) CK(cudaMemcpyAsync(P, h->d_fullP, sizeof(float) * M, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
   return check_device_error(h);
 }
 
@@ -779,6 +864,8 @@ extern "C" int ddm_idle(ddm_engine *h) {
   CK(cudaStreamSynchronize(h->copy_stream));
   CK(cudaStreamSynchronize(h->stream));
   prune_inflight(h);
+  int rc = join_analysis(h);
+  if (rc) return rc;
   return check_device_error(h);
 }
 
@@ -1131,6 +1218,8 @@ extern "C" int ddm_batch_launch_graph(ddm_batch *b) {
 extern "C" int ddm_autotune(ddm_engine *h, char *report, int32_t report_len) {
   if (!h) return DDM_ERR_ARG;
   cudaSetDevice(h->device);
+  if (int rc0 = join_analysis(h)) return rc0;
+  h->radial_from_live = false;
   const int N = h->g.N, T = h->g.T;
   const int fg = frames_per_col_cta(N);
   const int nfr = std::min(T, std::max(4 * h->chunk_cap, 64) / fg * fg);
@@ -1194,7 +1283,7 @@ extern "C" int ddm_autotune(ddm_engine *h, char *report, int32_t report_len) {
     float t[3];
     for (int r = -1; r < 3; r++) {
       cudaEventRecord(e0, h->stream);
-      if ((rc = temporal_impl(h, order.data(), mask.data(), 0))) break;
+      if ((rc = temporal_impl(h, order.data(), mask.data(), 0, h->stream))) break;
       cudaEventRecord(e1, h->stream);
       if (cudaEventSynchronize(e1) != cudaSuccess) {
         rc = fail(h, DDM_ERR_CUDA, "autotune: %s", cudaGetErrorString(cudaGetLastError()));

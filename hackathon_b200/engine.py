@@ -205,16 +205,36 @@ class DdmEngine:
         self._check(self._lib.ddm_set_spatial_mask(self._h, _ptr(m)))
 
     # ------------------------------------------------------------ analysis
-    def compute_temporal(self, order, mask, full=False, wait=True):
+    def compute_temporal(self, order, mask, full=False, wait=True, live=False):
         """computeTemporal (ddm-engine.ts:331-365). order[j] = slot of time
-        index j, mask[j] = 1 where time index j holds a valid frame."""
+        index j, mask[j] = 1 where time index j holds a valid frame.
+        live=True: start the analysis on the engine's analysis stream and
+        return; later ingests run concurrently (mask out the slots they
+        overwrite: FrameClock.snapshot's guard). DdmError "computeTemporal
+        is already running" while the previous live analysis is in flight."""
         self._alive()
         o = np.ascontiguousarray(order, dtype=np.uint32).reshape(-1)
         m = np.ascontiguousarray(mask, dtype=np.float32).reshape(-1)
         if o.size != self.T or m.size != self.T:
             raise DdmArgError(_lib.DDM_ERR_ARG, f"temporalMeta: order/mask must have length {self.T}")
-        f = self._lib.ddm_compute_temporal if wait else self._lib.ddm_compute_temporal_async
+        if live:
+            f = self._lib.ddm_compute_temporal_live
+        else:
+            f = self._lib.ddm_compute_temporal if wait else self._lib.ddm_compute_temporal_async
         self._check(f(self._h, _ptr(o), _ptr(m), 1 if full else 0))
+
+    @property
+    def analysis_done(self):
+        """True once no live analysis is in flight."""
+        self._alive()
+        d = C.c_int32(1)
+        self._check(self._lib.ddm_analysis_poll(self._h, C.byref(d)))
+        return bool(d.value)
+
+    def wait_analysis(self):
+        """Waits for the live analysis in flight, if any."""
+        self._alive()
+        self._check(self._lib.ddm_wait_analysis(self._h))
 
     def autotune(self):
         """Times chunk and unit-size candidates on this device and keeps the

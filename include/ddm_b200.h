@@ -119,6 +119,22 @@ int ddm_compute_temporal(ddm_engine *h, const uint32_t *order,
 /* Same, without waiting: the work is queued on the engine's stream. */
 int ddm_compute_temporal_async(ddm_engine *h, const uint32_t *order,
                                const float *mask, int32_t full);
+/* Live analysis: the dashboard's analysis tick (main.ts:366-398) with
+ * computeTemporal running while frames keep arriving (ddm-engine.ts:331-365).
+ * The snapshot holds every frame queued before the call; the analysis runs
+ * on the engine's analysis stream and returns at once, so later ingests
+ * proceed concurrently. Ring slots those ingests overwrite must be masked
+ * out of `mask` (the guard of FrameClock.snapshot, camera.ts:408-425).
+ * DDM_ERR_STATE "computeTemporal is already running" while the previous
+ * live analysis is in flight (ddm-engine.ts:332). The result stays readable
+ * (ddm_read_radial, ddm_read_temporal_full) until the next computeTemporal,
+ * whatever is ingested meanwhile. */
+int ddm_compute_temporal_live(ddm_engine *h, const uint32_t *order,
+                              const float *mask, int32_t full);
+/* *done = 1 once no live analysis is in flight (surfacing its device error). */
+int ddm_analysis_poll(ddm_engine *h, int32_t *done);
+/* Waits for the live analysis in flight, if any. */
+int ddm_wait_analysis(ddm_engine *h);
 
 /* DdmEngine.readRadial (ddm-engine.ts:391-395) + radialFromGpu
  * (ddm_ref.js:584-590): D[NB*L], P[NB], drift[NB*L*8] in FP64. */

@@ -40,6 +40,16 @@ class MotilityResult(C.Structure):
                 ("nlags", C.c_int32), ("swim", MotilityFit), ("brown", MotilityFit)]
 
 
+class SimParams(C.Structure):
+    """ddm_sim_params (include/ddm_b200.h)."""
+    _fields_ = [("N", C.c_int32), ("T", C.c_int32), ("fps", C.c_double), ("dxUm", C.c_double),
+                ("seed", C.c_uint32), ("nSwim", C.c_int32), ("swimVbar", C.c_double), ("swimSigma", C.c_double),
+                ("swim2d", C.c_int32), ("nPassive", C.c_int32), ("Dum2s", C.c_double), ("nFixed", C.c_int32),
+                ("hasDrift", C.c_int32), ("driftSpeed", C.c_double), ("driftAngleDeg", C.c_double),
+                ("dropFrac", C.c_double), ("dropExact", C.c_int32), ("blobSigmaPx", C.c_double),
+                ("amp", C.c_double), ("background", C.c_double), ("noise", C.c_double)]
+
+
 class Geometry(C.Structure):
     _fields_ = [("N", C.c_int32), ("T", C.c_int32), ("TPAD", C.c_int32), ("L", C.c_int32),
                 ("NB", C.c_int32), ("kmin", C.c_double), ("kmax", C.c_double),
@@ -81,6 +91,8 @@ _SIGS = {
     "ddm_autotune": (C.c_int, [_vp, C.c_char_p, _i32]),
     "ddm_get_tuning": (C.c_int, [_vp, C.POINTER(_i32), C.POINTER(_i32), C.POINTER(_i32)]),
     "ddm_set_tuning": (C.c_int, [_vp, _i32, _i32, _i32]),
+    "ddm_simulate": (C.c_int, [C.POINTER(SimParams), _vp, _i32, _vp, _vp, _vp]),
+    "ddm_simulate_error": (C.c_char_p, []),
     "ddm_analyze_motility": (C.c_int, [C.POINTER(RadialView), C.POINTER(MotilityOptions),
                                        C.POINTER(MotilityResult)]),
     "ddm_batch_create": (C.c_int, [_vp, _i32, C.POINTER(_vp)]),

@@ -21,6 +21,11 @@ FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxe
          "-I" + os.path.join(ROOT, "include")]
 
 
+# sim.cu restates the reference's JavaScript arithmetic: every product and sum
+# rounded on its own (no fused multiply-add)
+PER_FILE = {"sim.cu": ["--fmad=false"]}
+
+
 def _nvcc():
     cand = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
     if not os.path.exists(cand):
@@ -52,7 +57,7 @@ def build(force=False, verbose=False, ptxas_info=False):
 
     def compile_one(src):
         obj = os.path.join(obj_dir, os.path.basename(src) + ".o")
-        cmd = [nvcc, *ARCH, *FLAGS, *extra, "-c", src, "-o", obj]
+        cmd = [nvcc, *ARCH, *FLAGS, *extra, *PER_FILE.get(os.path.basename(src), []), "-c", src, "-o", obj]
         if src.endswith(".cpp"):
             # host FP64 code: IEEE operation order, no FMA contraction (the
             # reference's JavaScript arithmetic)

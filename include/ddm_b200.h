@@ -374,6 +374,38 @@ int ddm_spectra_noalloc(const void *frames, int32_t dtype, int32_t n, int32_t N,
                         int32_t T, const int32_t *slots, float scale, void *hist,
                         void *stream);
 
+/* ------------------------------------------------------------------ movies
+ * The reference's seeded movie generator (test/sim.mjs:90-186: mulberry32
+ * stream, polar normals, Marsaglia-Tsang gammas, periodic Gaussian blobs, u8
+ * quantisation, drop masks) on the GPU, for training data and large inputs.
+ * Same seed, same random streams: frames equal the reference's up to one grey
+ * level where a pixel sits on a rounding boundary (exp/log within an ulp).
+ * Field names follow SimParams (sim.mjs:66-84); swimmers/passive/fixed/drift
+ * are flattened. */
+typedef struct ddm_sim_params {
+  int32_t N, T;             /* frame size (multiple of 16), frames */
+  double fps, dxUm;
+  uint32_t seed;
+  int32_t nSwim;            /* swimmers: count, mean speed, speed sd, 2-D flag */
+  double swimVbar, swimSigma;
+  int32_t swim2d;
+  int32_t nPassive;         /* Brownian particles */
+  double Dum2s;             /* diffusion coefficient, um^2/s */
+  int32_t nFixed;           /* particles stuck to the glass */
+  int32_t hasDrift;
+  double driftSpeed, driftAngleDeg;
+  double dropFrac;          /* random frame drops (frame 0 always kept) */
+  int32_t dropExact;        /* exactly this many drops instead, if > 0 */
+  double blobSigmaPx, amp, background, noise;
+} ddm_sim_params;
+
+/* frames: T*N*N u8 (device memory if frames_on_device, else host); valid[T]
+ * 1/0; truth[4] (may be NULL): mean swim speed, Vx, Vy, D. Runs on `stream`
+ * (NULL: the legacy default stream) and returns when the movie is complete. */
+int ddm_simulate(const ddm_sim_params *p, uint8_t *frames, int32_t frames_on_device,
+                 uint8_t *valid, double *truth, void *stream);
+const char *ddm_simulate_error(void);
+
 #ifdef __cplusplus
 }
 #endif

@@ -112,10 +112,8 @@ __device__ __forceinline__ void model_c(const LmProblem& P, int lane, float al, 
 // VarPro amplitudes at fixed nonlinear parameters: the 2-column NNLS of the
 // reference's evalModel (motility_fit.js:450-474) by nnls3's support
 // enumeration (:243-263) over {A}, {B}, {A, B}. Returns the weighted cost.
-__device__ __forceinline__ double varpro(const LmProblem& P, int lane, double al, double lv, double lZ,
-                                         double lD, double& A, double& B) {
-  float c[4];
-  model_c(P, lane, (float)al, (float)exp(lv), (float)exp(lZ), (float)exp(lD), c);
+template <typename CT>
+__device__ __forceinline__ double varpro_c(const LmProblem& P, int lane, const CT (&c)[4], double& A, double& B) {
   double g11 = 0, g12 = 0, h1 = 0, h2 = 0, dd = 0;
 #pragma unroll
   for (int r = 0; r < 4; r++) {
@@ -153,6 +151,35 @@ __device__ __forceinline__ double varpro(const LmProblem& P, int lane, double al
   A = bA;
   B = bB;
   return fmax(best, 0.0) * (double)P.w * (double)P.w;
+}
+
+__device__ __forceinline__ double varpro(const LmProblem& P, int lane, double al, double lv, double lZ,
+                                         double lD, double& A, double& B) {
+  float c[4];
+  model_c(P, lane, (float)al, (float)exp(lv), (float)exp(lZ), (float)exp(lD), c);
+  return varpro_c(P, lane, c, A, B);
+}
+
+// The Brownian column c(tau) = 1 - <exp(-D q_n^2 tau)> in FP64, for the
+// Brownian-only fit: its golden section walks a valley that can be flat to
+// FP32 rounding (noise-dominated or barely decaying bins).
+__device__ __forceinline__ double varpro_brownian64(const LmProblem& P, int lane, double lD, double& A,
+                                                    double& B) {
+  const double D = exp(lD), iK = 1.0 / P.K;
+  double c[4];
+#pragma unroll
+  for (int r = 0; r < 4; r++) {
+    c[r] = 0.0;
+    if (lane + 32 * r >= P.nt) continue;
+    const double t = P.tau[r];
+    double sE = 0.0;
+    for (int n = 0; n < P.K; n++) {
+      const double q = P.qn[n];
+      sE += exp(-D * q * q * t);
+    }
+    c[r] = 1.0 - sE * iK;
+  }
+  return varpro_c(P, lane, c, A, B);
 }
 
 // Normal equations at theta: H (upper triangle, 21), g (6), cost; warp-reduced.
@@ -330,18 +357,23 @@ __device__ int lm_run(const LmProblem& P, int lane, double (&th)[LM_NP], double&
   return it32 + it64;
 }
 
-// The reference's start strategy (fitBrownian, motility_fit.js:500-536;
-// fitSwimmer :577-611) per bin, LM from the best `nrefine` of 64 starts
-// (oracle/lm.c or_lm_fit_plain). Accumulates iterations and evaluations.
-__device__ void plain_fit(const LmProblem& P, int lane, int nrefine, int max_iter, double tol,
-                          double (&th)[LM_NP], double& cost, int& iters, int& evals, bool& converged) {
+// The Brownian fit of one bin (fitBrownian, motility_fit.js:500-536, per
+// bin): the model at alpha = 0, c(tau) = 1 - <exp(-D q_n^2 tau)> over the
+// q-nodes, VarPro amplitudes; a 49-point scan of ln D over its bounds, then
+// golden section (at most 60 steps, to 1e-6 in ln D). Returns ln D;
+// `settled` when the bracket closed.
+template <bool F64>
+__device__ double brownian_search(const LmProblem& P, int lane, int& evals, bool& settled) {
   double A, B;
+  auto cost_at = [&](double x) {
+    return F64 ? varpro_brownian64(P, lane, x, A, B) : varpro(P, lane, 0.0, P.lo[3], 0.0, x, A, B);
+  };
   const double lo = P.lo[5], hi = P.hi[5];
   int bi = 0;
   double bf = 1e308;
   for (int i = 0; i <= 48; i++) {
     const double x = lo + ((hi - lo) * i) / 48;
-    const double v = varpro(P, lane, 0.0, P.lo[3], 0.0, x, A, B);
+    const double v = cost_at(x);
     if (v < bf) bf = v, bi = i;
   }
   evals += 49;
@@ -349,8 +381,8 @@ __device__ void plain_fit(const LmProblem& P, int lane, int nrefine, int max_ite
   double b = lo + ((hi - lo) * (bi < 48 ? bi + 1 : 48)) / 48;
   const double gr = (sqrt(5.0) - 1) / 2;
   double c = b - gr * (b - a), dd = a + gr * (b - a);
-  double fc = varpro(P, lane, 0.0, P.lo[3], 0.0, c, A, B);
-  double fd = varpro(P, lane, 0.0, P.lo[3], 0.0, dd, A, B);
+  double fc = cost_at(c);
+  double fd = cost_at(dd);
   evals += 2;
   for (int it = 0; it < 60 && b - a > 1e-6; it++) {
     if (fc < fd) {
@@ -358,17 +390,28 @@ __device__ void plain_fit(const LmProblem& P, int lane, int nrefine, int max_ite
       dd = c;
       fd = fc;
       c = b - gr * (b - a);
-      fc = varpro(P, lane, 0.0, P.lo[3], 0.0, c, A, B);
+      fc = cost_at(c);
     } else {
       a = c;
       c = dd;
       fc = fd;
       dd = a + gr * (b - a);
-      fd = varpro(P, lane, 0.0, P.lo[3], 0.0, dd, A, B);
+      fd = cost_at(dd);
     }
     evals++;
   }
-  const double lD0 = fc < fd ? c : dd;
+  settled = b - a <= 1e-6;
+  return fc < fd ? c : dd;
+}
+
+// The reference's start strategy (fitBrownian, motility_fit.js:500-536;
+// fitSwimmer :577-611) per bin, LM from the best `nrefine` of 64 starts
+// (oracle/lm.c or_lm_fit_plain). Accumulates iterations and evaluations.
+__device__ void plain_fit(const LmProblem& P, int lane, int nrefine, int max_iter, double tol,
+                          double (&th)[LM_NP], double& cost, int& iters, int& evals, bool& converged) {
+  double A, B;
+  bool settled;
+  const double lD0 = brownian_search<false>(P, lane, evals, settled);
   // 64 starts: lane l holds starts 2l and 2l+1 (index = 4 iv + 2 iz + ia)
   const double lZs0 = fmin(P.hi[4], fmax(P.lo[4], log(1.5)));
   const double lZs1 = fmin(P.hi[4], fmax(P.lo[4], log(8.0)));
@@ -487,6 +530,14 @@ __device__ __noinline__ void lm_one(const LmParams& p, int fit, int lane) {
         for (int q = 0; q < LM_NP; q++) th[q] = t2[q];
       }
     }
+  } else if (p.mode == LM_BROWNIAN) {
+    // the Brownian model alone: theta = (A, B, 0, ln vbar_lo, ln Z_lo, ln D)
+    th[5] = brownian_search<true>(P, lane, evals, conv);
+    th[2] = 0.0;
+    th[3] = P.lo[3];
+    th[4] = P.lo[4];
+    cost = varpro_brownian64(P, lane, th[5], th[0], th[1]);
+    evals++;
   } else {
     plain_fit(P, lane, p.nrefine, p.max_iter, p.tol, th, cost, iters, evals, conv);
   }
@@ -568,12 +619,14 @@ extern "C" int ddm_fit_lm(int32_t nfit, int32_t nt_max, int32_t K, const int32_t
   if (nfit < 0 || nt_max < 1 || nt_max > ddm::LM_MAX_LAGS || K < 1 || K > ddm::LM_MAX_NODES)
     return lm_fail(DDM_ERR_ARG, "ddm_fit_lm: need nfit >= 0, 1 <= nt_max <= %d, 1 <= K <= %d",
                    ddm::LM_MAX_LAGS, ddm::LM_MAX_NODES);
-  if (mode != ddm::LM_PLAIN && mode != ddm::LM_SEEDED && mode != ddm::LM_SEEDED_FALLBACK)
-    return lm_fail(DDM_ERR_ARG, "ddm_fit_lm: mode must be 0 (reference starts), 1 (seeded) or 2 (seeded, fallback)");
+  if (mode != ddm::LM_PLAIN && mode != ddm::LM_SEEDED && mode != ddm::LM_SEEDED_FALLBACK && mode != ddm::LM_BROWNIAN)
+    return lm_fail(DDM_ERR_ARG,
+                   "ddm_fit_lm: mode must be 0 (reference starts), 1 (seeded), 2 (seeded, fallback) or 3 (Brownian)");
   if (max_iter < 1 || nrefine < 1 || nrefine > 64 || !(tol >= 0))
     return lm_fail(DDM_ERR_ARG, "ddm_fit_lm: need max_iter >= 1, 1 <= nrefine <= 64, tol >= 0");
   if (nfit == 0) return DDM_OK;
-  if (!nt || !d || !tau || !qn || !w || !bounds || !theta || !cost || (mode != ddm::LM_PLAIN && !start))
+  const bool seeded = mode == ddm::LM_SEEDED || mode == ddm::LM_SEEDED_FALLBACK;
+  if (!nt || !d || !tau || !qn || !w || !bounds || !theta || !cost || (seeded && !start))
     return lm_fail(DDM_ERR_ARG, "ddm_fit_lm: null array");
   cudaStream_t s = (cudaStream_t)stream;
   ddm::LmParams p{};
@@ -608,7 +661,7 @@ extern "C" int ddm_fit_lm(int32_t nfit, int32_t nt_max, int32_t K, const int32_t
   step(stage_in(&dqn, qn, nf * K, s));
   step(stage_in(&dw, w, nf, s));
   step(stage_in(&db, bounds, nf * 6, s));
-  if (mode != ddm::LM_PLAIN) step(stage_in(&ds, start, nf * 4, s));
+  if (seeded) step(stage_in(&ds, start, nf * 4, s));
   step(stage_in<double>(&dth, nullptr, nf * 6, s));
   step(stage_in<double>(&dc, nullptr, nf, s));
   step(stage_in<int>(&dit, nullptr, nf, s));

@@ -21,7 +21,7 @@ import numpy as np
 from . import _lib
 
 SWIM_MIN_UM_S = 2.0  # GATES.SWIM_MIN_UM_S, motility_fit.js:28-38
-MODES = {"plain": 0, "seeded": 1, "seeded_fallback": 2}
+MODES = {"plain": 0, "seeded": 1, "seeded_fallback": 2, "brownian": 3}
 MAX_LAGS = 128
 MAX_NODES = 8
 
@@ -129,7 +129,9 @@ def fit_lm(d, tau, qn, w, bnds, mode="plain", start=None, nt=None, max_iter=200,
 
     d, tau [nfit, nt_max]; qn [nfit, K]; w [nfit]; bnds [6] or [nfit, 6];
     start [nfit, 4] = (alpha, vbar, Z, D) for mode "seeded"; nt [nfit] lags
-    used per fit (default nt_max)."""
+    used per fit (default nt_max). mode "brownian" fits the Brownian model
+    alone, A (1 - <exp(-D q^2 tau)>) + B per bin (fitBrownian's search,
+    motility_fit.js:500-536, one D per bin)."""
     lib = _lib.load()
     d = np.ascontiguousarray(d, np.float32)
     nfit, nt_max = d.shape
@@ -142,7 +144,7 @@ def fit_lm(d, tau, qn, w, bnds, mode="plain", start=None, nt=None, max_iter=200,
     ntv = np.ascontiguousarray(np.full(nfit, nt_max) if nt is None else nt, np.int32)
     m = MODES[mode]
     st = None
-    if m != 0:
+    if mode in ("seeded", "seeded_fallback"):
         st = np.ascontiguousarray(start, np.float32).reshape(nfit, 4)
     theta = np.zeros((nfit, 6))
     cost = np.zeros(nfit)

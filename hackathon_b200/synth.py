@@ -44,6 +44,17 @@ def config2(seed=1):
     return VideoSpec(seed=seed)
 
 
+def config1(seed=1):
+    """64 frames of 128^2 (u8 range): 200 blobs sigma 1.5 px, peak 120 over a
+    background of 20 counts, pure Brownian motion D = 0.3 px^2/frame,
+    periodic, Poisson noise, no mask and no dropped frames (the small plain
+    DDM configuration)."""
+    n, sig, peak, bg = 200, 1.5, 120.0, 20.0
+    return VideoSpec(N=128, T=64, n_blobs=n, sigma=sig, frac_brownian=1.0, D=0.3,
+                     mean_counts=bg + peak * n * 2 * np.pi * sig ** 2 / 128 ** 2, blob_peak=peak, roi_radius=0.0,
+                     drop_frac=0.0, seed=seed)
+
+
 def large(seed=1):
     """2048^2 x 4096 uint16 video with the mixed-motility statistics above,
     40,000 blobs and 5 % hot pixels (the large streamed configuration)."""

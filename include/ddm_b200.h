@@ -293,6 +293,10 @@ int ddm_batch_launch_graph(ddm_batch *b);
  *           (alpha = 0) scan -- impossible at a global optimum, since the
  *           Brownian model is nested -- also runs mode 0 and keeps the lower
  *           cost (the reference's starts as the fallback).
+ *   mode 3: the Brownian model alone, A (1 - <exp(-D q_n^2 tau)>) + B, one D
+ *           per bin by fitBrownian's search (the 49-point scan + golden
+ *           section of mode 0); theta = (A, B, 0, ln vmin, ln Zmin, ln D),
+ *           status bit 0 = the golden-section bracket closed.
  * Arrays: nt[nfit] lags per fit (<= nt_max <= 128), d and tau [nfit][nt_max],
  * qn [nfit][K] (K <= 8), w[nfit], bounds [nfit][6], start [nfit][4];
  * out theta [nfit][6], cost[nfit], iters/evals/status [nfit] (may be NULL;

@@ -311,11 +311,10 @@ int or_lm_fit_start(int nt, int K, const double *d, const double *tau, const dou
  *     cost (stable order on ties);
  *  3. LM from the best `nrefine` starts; the lowest cost wins (first on ties).
  * Returns total LM iterations; *evals counts model evaluations. */
-int or_lm_fit_plain(int nt, int K, const double *d, const double *tau, const double *qn, double w,
-                    const double *bounds6, int max_iter, double tol, int nrefine, double *theta,
-                    double *cost_out, int *evals) {
-  lm_prob P;
-  init_prob(&P, nt, K, d, tau, qn, w, bounds6);
+/* fitBrownian's search (motility_fit.js:500-536) for one bin: 49-point scan
+ * of ln D, then golden section (<= 60 steps, to 1e-6). Returns ln D. */
+static double brownian_search(const lm_prob *Pp, int *ne_out) {
+  const lm_prob P = *Pp;
   double A, B;
   int ne = 0;
   const double lo = P.lo[5], hi = P.hi[5];
@@ -349,7 +348,37 @@ int or_lm_fit_plain(int nt, int K, const double *d, const double *tau, const dou
     }
     ne++;
   }
-  const double lD0 = fc < fd ? c : dd;
+  *ne_out += ne;
+  return fc < fd ? c : dd;
+}
+
+/* The Brownian model alone per bin (alpha = 0): theta = (A, B, 0, ln vbar_lo,
+ * ln Z_lo, ln D), cost = VarPro weighted RSS at that D. */
+double or_lm_fit_brownian(int nt, int K, const double *d, const double *tau, const double *qn, double w,
+                          const double *bounds6, double *theta) {
+  lm_prob P;
+  init_prob(&P, nt, K, d, tau, qn, w, bounds6);
+  int ne = 0;
+  const double lD = brownian_search(&P, &ne);
+  double A, B;
+  const double cost = varpro(&P, 0, P.lo[3], 0, lD, &A, &B);
+  theta[0] = A;
+  theta[1] = B;
+  theta[2] = 0;
+  theta[3] = P.lo[3];
+  theta[4] = P.lo[4];
+  theta[5] = lD;
+  return cost;
+}
+
+int or_lm_fit_plain(int nt, int K, const double *d, const double *tau, const double *qn, double w,
+                    const double *bounds6, int max_iter, double tol, int nrefine, double *theta,
+                    double *cost_out, int *evals) {
+  lm_prob P;
+  init_prob(&P, nt, K, d, tau, qn, w, bounds6);
+  double A, B;
+  int ne = 0;
+  const double lD0 = brownian_search(&P, &ne);
   /* 64 starts */
   double su[64][3], sf[64];
   int ord[64], ns = 0;

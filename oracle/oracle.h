@@ -178,6 +178,9 @@ int or_lm_fit_start(int nt, int K, const double *d, const double *tau, const dou
                     double *theta, double *cost_out);
 /* LM from the reference's start strategy (Brownian scan, 64 starts, best
  * nrefine refined). */
+/* Brownian model per bin (fitBrownian's search, alpha = 0) -> cost. */
+double or_lm_fit_brownian(int nt, int K, const double *d, const double *tau, const double *qn, double w,
+                          const double *bounds6, double *theta);
 int or_lm_fit_plain(int nt, int K, const double *d, const double *tau, const double *qn, double w,
                     const double *bounds6, int max_iter, double tol, int nrefine, double *theta,
                     double *cost_out, int *evals);

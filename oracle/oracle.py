@@ -129,6 +129,7 @@ def lib():
         "or_lm_model": (None, [C.c_int, C.c_int, _dp, _dp, _dp, _dp]),
         "or_lm_fit_start": (C.c_int, [C.c_int, C.c_int, _dp, _dp, _dp, C.c_double, _dp, _dp,
                                       C.c_int, C.c_double, _dp, C.POINTER(C.c_double)]),
+        "or_lm_fit_brownian": (C.c_double, [C.c_int, C.c_int, _dp, _dp, _dp, C.c_double, _dp, _dp]),
         "or_lm_fit_plain": (C.c_int, [C.c_int, C.c_int, _dp, _dp, _dp, C.c_double, _dp, C.c_int,
                                       C.c_double, C.c_int, _dp, C.POINTER(C.c_double),
                                       C.POINTER(C.c_int)]),
@@ -549,6 +550,13 @@ def lm_fit_start(d, tau, qn, w, bounds6, start4, max_iter=200, tol=1e-10):
     it = lib().or_lm_fit_start(len(d), len(qn), _f64(d), _f64(tau), _f64(qn), float(w),
                                _f64(bounds6), _f64(start4), max_iter, tol, th, C.byref(cost))
     return th, cost.value, it
+
+
+def lm_fit_brownian(d, tau, qn, w, bounds6):
+    """FP64 Brownian model per bin (fitBrownian's scan + golden section) -> (theta, cost)."""
+    th = np.zeros(6)
+    cost = lib().or_lm_fit_brownian(len(d), len(qn), _f64(d), _f64(tau), _f64(qn), float(w), _f64(bounds6), th)
+    return th, cost
 
 
 def lm_fit_plain(d, tau, qn, w, bounds6, max_iter=200, tol=1e-10, nrefine=3):

@@ -247,3 +247,20 @@ def test_translation_sign_convention(sx, sy):
     d = O.estimate_drift(r, 1.0, _fps)
     Vx, Vy = sx * _fps, sy * _fps
     assert math.hypot(d["Vx"] - Vx, d["Vy"] - Vy) / math.hypot(Vx, Vy) < 0.1
+
+
+def test_brownian_per_bin_recovers_d():
+    """The oracle's per-bin Brownian fit (fitBrownian's scan + golden
+    section) on noise-free Brownian curves returns the generating D and
+    amplitudes."""
+    tau = np.arange(1, 64, dtype=np.float64)
+    for k, D in ((6.0, 0.3), (15.0, 0.05), (30.0, 0.8)):
+        q = 2 * np.pi * k / 128
+        qn = q * np.array([0.99, 0.997, 1.003, 1.01])
+        th = np.array([1.7, 0.05, 0.0, 0.0, 0.0, np.log(D)])
+        d = O.lm_model(tau, qn, th)
+        b6 = np.array([0.01, 10.0, 0.5, 100.0, 1e-4, 100.0])
+        got, cost = O.lm_fit_brownian(d, tau, qn, 1.0 / d.max(), b6)
+        # golden section stops at a 1e-6 bracket of a flat valley: D to 1e-4
+        assert abs(got[5] - np.log(D)) < 1e-4 and cost < 1e-12
+        assert abs(got[0] / 1.7 - 1) < 1e-3 and abs(got[1] - 0.05) < 2e-4

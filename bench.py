@@ -393,6 +393,120 @@ def run_large(args, rank, world, dist):
     eng.destroy()
 
 
+BATCH_METRIC = "DDM frames/s, 48 uneven videos in one persistent launch"
+BATCH_WORKLOAD = ("48 seeded u16 videos, N in {256, 512} (384 and 768 need radix-3 transforms, not built), "
+                  "T uniform in [300, 2000], per-video motile fraction in [0, 0.9], mean speed in [0.3, 3] "
+                  "px/frame, D in [0.05, 0.5] px^2/frame, circular ROI of random radius, 2% dropped frames; "
+                  "L = min(512, T/2), NB = N/4, kmin 4, kmax 0.39 N; one batched ingest + ONE temporal launch "
+                  "over all videos, replayed from a CUDA graph; all q-bins of all videos in one LM launch")
+
+
+def run_batch(args, rank, world, dist):
+    """The batched-videos configuration: every video's spatial chunks and one
+    persistent temporal launch over the work units of all videos, captured
+    once into a CUDA graph and replayed (value), then all q-bins of all
+    videos fitted by one batched LM launch (q-fits/s). Tile shapes come from
+    the autotuner (one engine of each size, applied to the others)."""
+    import torch
+
+    import hackathon_b200 as H
+    from hackathon_b200 import fit as F
+    from hackathon_b200 import replicas as R
+    from hackathon_b200 import synth
+    from hackathon_b200.batch import DdmBatch
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(local)
+    rng = np.random.default_rng(R.rank_seed(7, rank))
+    nvid = args.videos
+    vids, engines, tuned = [], [], {}
+    t_gen = time.perf_counter()
+    for i in range(nvid):
+        N = int(rng.choice([256, 512]))
+        T = int(rng.integers(300, 2001)) // 2 * 2
+        al, vb, Dd = rng.uniform(0, 0.9), rng.uniform(0.3, 3.0), rng.uniform(0.05, 0.5)
+        spec = synth.VideoSpec(N=N, T=T, n_blobs=int(2000 * (N / 512) ** 2), frac_brownian=1 - al, D=Dd, vbar=vb,
+                               roi_radius=float(rng.uniform(0.30, 0.48)) * N, drop_frac=0.02,
+                               seed=int(R.rank_seed(1000, rank) * 100 + i))
+        frames, valid, _ = synth.generate(spec)
+        L, NB = min(512, T // 2), N // 4
+        e = H.DdmEngine.create(N=N, T=T, L=L, NB=NB, kmin=4.0, kmax=0.39 * N)
+        e.set_spatial_mask(synth.roi_mask(spec))
+        if N not in tuned:
+            tuned[N] = e.autotune()
+        else:
+            t = tuned[N]
+            e.set_tuning(t["best_chunk"], t["best_unit"], t["best_variant"])
+        vids.append(dict(frames=frames.contiguous(), valid=valid, T=T, N=N))
+        engines.append(e)
+    torch.cuda.synchronize()
+    t_gen = time.perf_counter() - t_gen
+    total = sum(v["T"] for v in vids)
+    slots = [np.arange(v["T"], dtype=np.int32) for v in vids]
+    orders = [np.arange(v["T"], dtype=np.uint32) for v in vids]
+    masks = [v["valid"].astype(np.float32) for v in vids]
+    scales = [1.0 / 65535] * nvid
+    frames = [v["frames"] for v in vids]
+    batch = DdmBatch(engines)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    batch.set_stream(stream.cuda_stream)
+    batch.ingest(frames, slots, scales)
+    batch.compute_temporal(orders, masks)  # per-video tables, then the launch
+    batch.sync()
+    l0 = sum(e.kernel_launches for e in engines)
+    batch.ingest(frames, slots, scales)    # one step outside the graph: its launch count
+    batch.enqueue_temporal()
+    batch.sync()
+    per_step = sum(e.kernel_launches for e in engines) - l0
+    batch.capture(frames, slots, scales)   # ingest + temporal of all videos as one graph
+    for _ in range(max(args.warmup, 3)):
+        batch.launch_graph()
+    batch.sync()
+    if dist:
+        dist.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    steps = max(1, min(args.steps, 10))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    h0 = time.perf_counter()
+    e0.record(stream)
+    for _ in range(steps):
+        batch.launch_graph()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clocks.mark(h0, time.perf_counter())
+    clk = clocks.stop()
+    ms_step = R.max_over_ranks(e0.elapsed_time(e1), dist, device="cuda") / steps
+    value = R.weak_scaling_throughput(total, ms_step, world)
+    radials = batch.read_radials()
+    # all q-bins of all videos: one LM launch (host arrays in and out)
+    torch.cuda.synchronize()
+    f0 = time.perf_counter()
+    fits = batch.fit_all(radials, swim_min=0.0)
+    f_s = time.perf_counter() - f0
+    nfit = sum(len(p.bins) for p, _ in fits)
+    finite = all(np.isfinite(r.cost).all() for _, r in fits)
+    if rank == 0:
+        line = {"metric": BATCH_METRIC, "value": value, "unit": "frames/s", "n_gpus": world, "steps": steps,
+                "warmup": max(args.warmup, 3), "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded GPU generator, hackathon_b200/synth.py)",
+                "config": {"workload": BATCH_WORKLOAD, "videos": nvid, "frames_per_step": total,
+                           "sizes": {str(n): sum(v["N"] == n for v in vids) for n in (256, 512)},
+                           "l2": "inputs larger than L2", "generation_s": t_gen,
+                           "autotuned": {str(n): {k: t[k] for k in ("best_chunk", "best_unit", "best_variant")}
+                                         for n, t in tuned.items()}},
+                "e2e": {"value": None, "unit": "frames/s",
+                        "unavailable": "the batched ingest takes frames already on the device"},
+                "gpu_launches": int(per_step * steps), "clocks": clk,
+                "fit": {"qfits": nfit, "one_launch_s_host_timed": f_s, "qfits_per_s": nfit / f_s,
+                        "all_finite": bool(finite)}}
+        print(json.dumps(line), flush=True)
+    batch.destroy()
+    for e in engines:
+        e.destroy()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -403,10 +517,11 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-fit", action="store_true", help="skip the q-fits/s (surrogate + LM) section")
     ap.add_argument("--tuning", default="", help="chunk,unit[,variant]: apply instead of autotuning")
-    ap.add_argument("--workload", default="config2", choices=["config2", "large"],
+    ap.add_argument("--workload", default="config2", choices=["config2", "large", "batch"],
                     help="large: one 2048^2 x 4096 video per GPU (68.8 GB history), its own JSON line")
     ap.add_argument("--frames", type=int, default=0, help="large workload: frames per video (default 4096)")
     ap.add_argument("--roi", type=int, default=0, help="large workload: ROI size (default 2048)")
+    ap.add_argument("--videos", type=int, default=48, help="batch workload: number of videos")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", 0))
@@ -419,8 +534,8 @@ def main():
         import torch.distributed as dist
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    if args.impl == "ours" and args.workload == "large":
-        run_large(args, rank, world, dist)
+    if args.impl == "ours" and args.workload in ("large", "batch"):
+        (run_large if args.workload == "large" else run_batch)(args, rank, world, dist)
         if dist:
             dist.barrier()
             dist.destroy_process_group()

@@ -9,7 +9,9 @@ analyzeRadial, motility-ddm/src/ddm_ref.js:196-206, 425-437).
   value  frames/s with the frames already in HBM (device-timed, CUDA events on
          the engine's stream, max over ranks, summed over ranks)
   e2e    the same through the C ABI from pinned HOST frames: every step copies
-         its frames host->device and reads the radial record back
+         its frames host->device and reads the radial record back; two engines
+         take the videos in turn, so one video's copies overlap the previous
+         video's temporal analysis
 Under torchrun each rank analyses its own video (weak scaling, no collective
 on the data path).
 
@@ -514,7 +516,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--e2e-steps", type=int, default=6)
     ap.add_argument("--no-fit", action="store_true", help="skip the q-fits/s (surrogate + LM) section")
     ap.add_argument("--tuning", default="", help="chunk,unit[,variant]: apply instead of autotuning")
     ap.add_argument("--workload", default="config2", choices=["config2", "large", "batch"],
@@ -616,27 +618,45 @@ def main():
     ms_step = ms / args.steps
     value = R.weak_scaling_throughput(T, ms_step, world)
 
-    # ---------------- e2e: pinned host frames through the C ABI
+    # ---------------- e2e: pinned host frames through the C ABI. Two engines
+    # take videos in turn (a user with a stream of videos): while one
+    # video's temporal analysis runs, the next video's frames already cross
+    # PCIe into the other engine; every video's radial record is read back.
     host = frames.view(torch.int16).cpu().pin_memory()
     rad_bytes = 8 * (NB * L + NB + NB * L * 8)
     eng.set_stream(stream.cuda_stream)
-    for _ in range(2):
-        eng.ingest_frames(host, slots, scale)
-        eng.compute_temporal(order, tmask, full=False, wait=False)
-        eng.read_radial()
+    eng2 = H.DdmEngine.create(N=N, T=T, TPAD=TPAD, L=L, NB=NB, kmin=KMIN, kmax=KMAX)
+    eng2.set_spatial_mask(mask_roi)
+    eng2.set_tuning(tune["best_chunk"], tune["best_unit"], tune["best_variant"])
+    stream2 = torch.cuda.Stream()
+    eng2.set_stream(stream2.cuda_stream)
+    engs = (eng, eng2)
+
+    def e2e_run(n):
+        prev = None
+        for i in range(n):
+            x = engs[i % 2]
+            x.ingest_frames(host, slots, scale)
+            x.compute_temporal(order, tmask, full=False, wait=False)
+            if prev is not None:
+                prev.read_radial()
+            prev = x
+        return prev.read_radial()
+
+    e2e_run(2)
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    for _ in range(args.e2e_steps):
-        eng.ingest_frames(host, slots, scale)
-        eng.compute_temporal(order, tmask, full=False, wait=False)
-        radial = eng.read_radial()
+    stream2.wait_stream(stream)
+    radial = e2e_run(args.e2e_steps)
+    stream.wait_stream(stream2)
     e1.record(stream)
     torch.cuda.synchronize()
     ms_e2e = e0.elapsed_time(e1)
+    eng2.destroy()
     ms_e2e = R.max_over_ranks(ms_e2e, dist, device="cuda")
     e2e = R.weak_scaling_throughput(T * args.e2e_steps, ms_e2e, world)
 
@@ -690,7 +710,8 @@ def main():
                            "l2": "inputs larger than L2 (537 MB frames, 1.08 GB history per video)",
                            "autotuned": {"chunk": tune["best_chunk"], "unit": tune["best_unit"],
                                          "temporal_variant": tune["best_variant"]}},
-                "e2e": {"value": e2e, "unit": "frames/s", "h2d_bytes_per_step": int(host.numel() * 2),
+                "e2e": {"value": e2e, "unit": "frames/s", "pipeline": "two engines take videos in turn",
+                        "h2d_bytes_per_step": int(host.numel() * 2),
                         "d2h_bytes_per_step": rad_bytes},
                 "gpu_launches": int(launches),
                 "roofline": roof,

@@ -70,6 +70,29 @@ __device__ __forceinline__ int cref_offset(int i) {
   return ((2 * (i >> 4) + 1) * (N / 32)) * N + (2 * (i & 15) + 1) * (N / 32);
 }
 
+// Frame reference levels c_f of a chunk, one CTA per frame: the mean of the
+// CREF grid pixels, warp sums added in a fixed order (the rows kernel reads
+// the result for every batch of the frame).
+template <int N, typename Tin>
+__global__ void __launch_bounds__(CREF) cref_kernel(const Tin* __restrict__ frames, long long frame_stride,
+                                                    float* __restrict__ framec) {
+  constexpr bool INT = !std::is_floating_point<Tin>::value;
+  using acc_t = typename std::conditional<INT, int, double>::type;
+  __shared__ acc_t cred[CREF / 32];
+  const long long f = blockIdx.x;
+  acc_t c = (acc_t)__ldg(frames + f * frame_stride + cref_offset<N>(threadIdx.x));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+  if ((threadIdx.x & 31) == 0) cred[threadIdx.x >> 5] = c;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    acc_t sum = 0;
+#pragma unroll
+    for (int w = 0; w < CREF / 32; w++) sum += cred[w];
+    framec[f] = (float)((double)sum * (1.0 / CREF));
+  }
+}
+
 // Persistent: each CTA walks batches of G row pairs (2G consecutive rows of
 // one frame; G divides N/2, so a batch never straddles frames). A batch (and
 // the mask's matching rows) is staged into shared memory by bulk copies (TMA,
@@ -124,40 +147,13 @@ __global__ void __launch_bounds__(256) rows_kernel(RowParams p) {
   // pixel sums: exact integers for u8/u16 (warp totals < 2^31), FP64 for f32
   constexpr bool INT = !std::is_floating_point<Tin>::value;
   using acc_t = typename std::conditional<INT, int, double>::type;
-  static_assert(WARPS * 32 == CREF, "one reference pixel per thread");
-  __shared__ acc_t cred[WARPS];
-  // c_f of a frame from the warp sums in cred[] (fixed order: bit-identical
-  // in every CTA)
-  auto cref_of = [&]() {
-    acc_t c = 0;
-#pragma unroll
-    for (int w = 0; w < WARPS; w++) c += cred[w];
-    return (float)((double)c * (1.0 / CREF));
-  };
-  auto cref_warp = [&](Tin px) {
-    acc_t c = (acc_t)px;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
-    if ((threadIdx.x & 31) == 0) cred[threadIdx.x >> 5] = c;
-  };
-  {  // the first batch's frame
-    const long long f = blockIdx.x < nbatch ? blockIdx.x / BPF : 0;
-    cref_warp(__ldg(frames + f * p.frame_stride + cref_offset<N>(threadIdx.x)));
-  }
-  __syncthreads();
-  float cf_next = cref_of();
+  __syncthreads();  // barriers initialised, twiddles and w(y) in shared memory
   int it = 0;
   for (long long b = blockIdx.x; b < nbatch; b += gridDim.x, it++) {
     const int st = it % ROW_STAGES;
     const int f = (int)(b / BPF);
     const int r = (int)(b % BPF);
-    const float cf = cf_next;
-    Tin cpx;  // next batch's reference pixel (raw load, reduced after the FFT's loads)
-    {
-      const long long bn = b + gridDim.x;
-      const long long fn = bn < nbatch ? bn / BPF : f;
-      cpx = __ldg(frames + fn * p.frame_stride + cref_offset<N>(threadIdx.x));
-    }
+    const float cf = p.framec[f];  // cref_kernel, earlier on this stream
     if (!mbar_wait(&bar[st], (uint32_t)(it / ROW_STAGES) & 1u, p.err, 2)) {
       // give up: let this CTA's other copies in flight land (bounded), then stop
       if (threadIdx.x == 0)
@@ -166,7 +162,7 @@ __global__ void __launch_bounds__(256) rows_kernel(RowParams p) {
             mbar_wait(&bar[(it + k) % ROW_STAGES], (uint32_t)((it + k) / ROW_STAGES) & 1u, nullptr, 0);
       return;
     }
-    const int y0 = r * 2 * G + 2 * g;
+    const int y0 = r * 2 * G + 2 * g;  // this group's row pair
     const Tin* r0 = ring + st * BATCH_ELEMS + 2 * g * N;
     const Tin* r1 = r0 + N;
     const uint8_t* m0p = mring + st * BATCH_ELEMS + 2 * g * N;
@@ -190,10 +186,8 @@ __global__ void __launch_bounds__(256) rows_kernel(RowParams p) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = (double)s;
-    cref_warp(cpx);
     const float2* Z = fft<N, false, true, SYNC>(v, t, buf0, buf1, s_tw, 1 + g);
-    __syncthreads();  // red[], cred[] complete; every thread is done with stage st
-    cf_next = cref_of();
+    __syncthreads();  // red[] and every group's row spectra complete; stage st is free
     if (threadIdx.x == 0) {
       const long long bn = b + (long long)ROW_STAGES * gridDim.x;
       if (bn < nbatch) issue(bn, st);
@@ -201,17 +195,33 @@ __global__ void __launch_bounds__(256) rows_kernel(RowParams p) {
 #pragma unroll
       for (int w = 0; w < WARPS; w++) tot += red[w];
       atomicAdd(&p.framesum[f], tot);
-      if (r == 0) p.framec[f] = cf;
     }
-    float2* out = p.rows + (size_t)f * NHB * N * KB;
-    for (int kx = t; kx <= N / 2; kx += NT) {
-      const float2 zk = Z[pad(kx)];
-      const float2 zn = Z[pad((N - kx) & (N - 1))];
-      const float2 R0 = make_float2(0.5f * (zk.x + zn.x), 0.5f * (zk.y - zn.y));
-      const float2 R1 = make_float2(0.5f * (zk.y + zn.y), -0.5f * (zk.x - zn.x));
-      float2* o = out + ((size_t)(kx / KB) * N + y0) * KB + (kx % KB);
-      o[0] = R0;
-      o[KB] = R1;
+    // Row spectra out by the CTA as a whole: item (kx pair kb, row rr of the
+    // batch) is one 16 B float4 (both kx of the pair), and consecutive items
+    // are consecutive rows of one kx pair, so a warp writes whole 128 B lines
+    // of the [frame][kx/2][y][2] scratch. Row rr of the batch is the
+    // real-input half (rr even: real part, odd: imaginary part) of group
+    // rr/2's packed transform, split by Hermitian symmetry.
+    {
+      const int zoff = (int)(Z - (sm + (size_t)g * GSTRIDE<N>()));  // same in every group
+      const int yb = r * 2 * G;
+      float4* out4 = reinterpret_cast<float4*>(p.rows + (size_t)f * NHB * N * KB);
+      static_assert(KB == 2, "a float4 holds one kx pair");
+      for (int item = threadIdx.x; item < NHB * 2 * G; item += blockDim.x) {
+        const int rr = item % (2 * G), kb = item / (2 * G);
+        const float2* Zg = sm + (size_t)(rr >> 1) * GSTRIDE<N>() + zoff;
+        float2 R[KB];
+#pragma unroll
+        for (int c = 0; c < KB; c++) {
+          const int kx = kb * KB + c;
+          const float2 zk = Zg[pad(kx & (N - 1))];
+          const float2 zn = Zg[pad((N - kx) & (N - 1))];
+          R[c] = (rr & 1) ? make_float2(0.5f * (zk.y + zn.y), -0.5f * (zk.x - zn.x))
+                          : make_float2(0.5f * (zk.x + zn.x), 0.5f * (zk.y - zn.y));
+          if (kx > N / 2) R[c] = make_float2(0.f, 0.f);  // past the half plane
+        }
+        out4[(size_t)kb * N + yb + rr] = make_float4(R[0].x, R[0].y, R[1].x, R[1].y);
+      }
     }
     __syncthreads();  // buffers and red[] are reused by the next batch
   }
@@ -552,6 +562,7 @@ static cudaError_t rows_n(const RowParams& p, cudaStream_t s) {
   auto k = rows_kernel<N, Tin>;
   const size_t sm = fft_smem<N>() + N * sizeof(float) + (size_t)ROW_STAGES * 2 * G * N * (sizeof(Tin) + 1);
   const int grid = persistent_grid(k, G * (N / 8), sm, (npairs + G - 1) / G);
+  if (p.nframes > 0) cref_kernel<N, Tin><<<p.nframes, CREF, 0, s>>>((const Tin*)p.frames, p.frame_stride, p.framec);
   k<<<grid, G * (N / 8), sm, s>>>(p);
   return cudaGetLastError();
 }

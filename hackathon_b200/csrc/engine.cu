@@ -46,7 +46,7 @@ struct ddm_engine {
   // geometry tables
   BinTable bins;
   float2 *d_hist = nullptr;            // [modes][T]
-  float2 *d_rows = nullptr;            // [chunk][NHB][N][KB]
+  float2 *d_rows = nullptr;            // [chunk][NHB][KB][N]
   float *d_rowc = nullptr;             // [chunk] frame reference levels c_f
   double *d_framesum = nullptr;        // [chunk] pixel sums
   double *d_means = nullptr;           // [chunk]

@@ -19,14 +19,14 @@ struct RowParams {
   const float* wys;        // w(y) * scale
   const uint8_t* smask;    // spatial mask [N][N] or nullptr (extension)
   const float2* tw;        // per-stage twiddle blocks of the N-point FFT
-  float2* rows;            // [nframes][NHB][N][KB]
+  float2* rows;            // [nframes][NHB][KB][N]
   float* framec;           // [nframes] frame reference level c_f (raw units, out)
   double* framesum;        // [nframes] masked pixel sums (zeroed before launch)
   int* err;                // error word (bounded waits that timed out), or nullptr
 };
 
 struct ColParams {
-  const float2* rows;      // [nframes][NHB][N][KB]
+  const float2* rows;      // [nframes][NHB][KB][N]
   const float* framec;     // [nframes] c_f
   const double* framesum;  // [nframes]
   const double* inv_total; // [1] 1 / (valid pixels of the frame)

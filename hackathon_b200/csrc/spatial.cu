@@ -13,7 +13,7 @@
 //               CTA gets the same value; exact for integer frames), multiplies by
 //               w(x) w(y) scale m(x,y), and transforms two rows per complex
 //               FFT (real-input packing). It writes the row spectra to an
-//               L2-resident scratch in a [frame][kx/2][y][2] blocked layout,
+//               L2-resident scratch in a [frame][kx/2][2][y] blocked layout,
 //               c_f, and one FP64 atomic per CTA into the frame's pixel sum.
 //  cols_kernel  stages a tile (column pair, G frames) of row spectra with bulk
 //               copies, runs the column FFTs and restores the exact frame mean
@@ -51,12 +51,15 @@ __host__ __device__ constexpr int row_groups() {
 constexpr int ROW_STAGES = 2;  // depth of the row-batch staging ring
 
 // float2 between the buffer pairs of consecutive FFT groups: two buffers
-// plus a skew of 2 float2, so the column kernel's stores, which read the same
-// index from G groups at once, hit different banks (16-byte aligned: the
-// bulk-copy destinations after the groups stay aligned).
+// plus a skew, so accesses that read the same index from several groups at
+// once (the column kernel's stores, the row kernel's output loop) hit
+// different banks. 4 float2 from N = 512 on, 2 below (where a warp spans
+// groups inside the transforms); chosen by simulating every shared-memory
+// access pattern of both kernels. Even, so the bulk-copy destinations after
+// the groups stay 16-byte aligned.
 template <int N>
 __host__ __device__ constexpr int GSTRIDE() {
-  return 2 * padded(N) + 2;
+  return 2 * padded(N) + (N >= 512 ? 4 : 2);
 }
 
 // The pixels whose mean is a frame's reference level c_f: a 16 x 16 grid at
@@ -197,16 +200,16 @@ __global__ void __launch_bounds__(256) rows_kernel(RowParams p) {
       atomicAdd(&p.framesum[f], tot);
     }
     // Row spectra out by the CTA as a whole: item (kx pair kb, row rr of the
-    // batch) is one 16 B float4 (both kx of the pair), and consecutive items
-    // are consecutive rows of one kx pair, so a warp writes whole 128 B lines
-    // of the [frame][kx/2][y][2] scratch. Row rr of the batch is the
+    // batch) writes both kx of the pair, and consecutive items are
+    // consecutive rows, so a warp writes whole sectors of the
+    // [frame][kx/2][2][y] scratch (each column contiguous in y, as the column
+    // kernel reads it). Row rr of the batch is the
     // real-input half (rr even: real part, odd: imaginary part) of group
     // rr/2's packed transform, split by Hermitian symmetry.
     {
       const int zoff = (int)(Z - (sm + (size_t)g * GSTRIDE<N>()));  // same in every group
       const int yb = r * 2 * G;
-      float4* out4 = reinterpret_cast<float4*>(p.rows + (size_t)f * NHB * N * KB);
-      static_assert(KB == 2, "a float4 holds one kx pair");
+      float2* out = p.rows + (size_t)f * NHB * N * KB;
       for (int item = threadIdx.x; item < NHB * 2 * G; item += blockDim.x) {
         const int rr = item % (2 * G), kb = item / (2 * G);
         const float2* Zg = sm + (size_t)(rr >> 1) * GSTRIDE<N>() + zoff;
@@ -220,7 +223,8 @@ __global__ void __launch_bounds__(256) rows_kernel(RowParams p) {
                           : make_float2(0.5f * (zk.x + zn.x), 0.5f * (zk.y - zn.y));
           if (kx > N / 2) R[c] = make_float2(0.f, 0.f);  // past the half plane
         }
-        out4[(size_t)kb * N + yb + rr] = make_float4(R[0].x, R[0].y, R[1].x, R[1].y);
+#pragma unroll
+        for (int c = 0; c < KB; c++) out[((size_t)kb * KB + c) * N + yb + rr] = R[c];
       }
     }
     __syncthreads();  // buffers and red[] are reused by the next batch
@@ -228,7 +232,7 @@ __global__ void __launch_bounds__(256) rows_kernel(RowParams p) {
 }
 
 // Persistent: each CTA walks tiles (column pair kb, group of G frames). The
-// tile's G row-spectrum blocks ([y][KB] float2, contiguous per frame) are
+// tile's G row-spectrum blocks ([KB][y] float2, contiguous per frame) are
 // staged into shared memory by bulk copies; the next tile's copies are
 // issued as soon as every thread has read the current one, so they overlap
 // the second column's transform and the history stores. Group g transforms
@@ -251,7 +255,7 @@ __global__ void __launch_bounds__(256) cols_kernel(ColParams p) {
   float2* buf0 = sm + (size_t)g * GSTRIDE<N>();
   float2* buf1 = buf0 + PN;
   float2* s_tw = sm + (size_t)G * GSTRIDE<N>();
-  float2* stage = s_tw + tw_size(N);  // [G][N][KB]
+  float2* stage = s_tw + tw_size(N);  // [G][KB][N]
   for (int i = threadIdx.x; i < tw_size(N); i += blockDim.x) s_tw[i] = p.tw[i];
   if (threadIdx.x < 4) s_wc4[threadIdx.x] = p.wc4[threadIdx.x];
   const int nfg = (p.nframes + G - 1) / G;
@@ -295,7 +299,7 @@ __global__ void __launch_bounds__(256) cols_kernel(ColParams p) {
       if (kx >= p.NH) break;  // uniform over the CTA
       float2 v[8];
 #pragma unroll
-      for (int q = 0; q < 8; q++) v[q] = fvalid ? blk[(t + q * NT) * KB + c] : make_float2(0.f, 0.f);
+      for (int q = 0; q < 8; q++) v[q] = fvalid ? blk[c * N + t + q * NT] : make_float2(0.f, 0.f);
       if (c == KB - 1 || kx + 1 >= p.NH) {
         // every thread has read the stage: the next tile's copies may land
         fence_proxy_async_smem();
@@ -364,7 +368,7 @@ __global__ void __launch_bounds__(256, 1) cols_wide_kernel(ColParams p) {
   static_assert(F % G == 0, "groups divide the tile's frames");
   static_assert((fft_stages(N) & 1) == 0, "the transform must end in its second buffer (the output slab)");
   extern __shared__ __align__(16) float2 sm[];
-  float2* ring = sm;                   // [2][G][N][KB] staged blocks
+  float2* ring = sm;                   // [2][G][KB][N] staged blocks
   float2* R = ring + 2 * ITEM_ELEMS;   // [KB][F][N] column transforms of the tile
   float2* scr = R + KB * F * N;        // [G][N] first ping-pong buffer of each group
   float2* s_tw = scr + G * N;
@@ -446,7 +450,7 @@ __global__ void __launch_bounds__(256, 1) cols_wide_kernel(ColParams p) {
       for (int c = 0; c < KB; c++) {
         float2 v[8];
 #pragma unroll
-        for (int q = 0; q < 8; q++) v[q] = fvalid ? blk[(t + q * NT) * KB + c] : make_float2(0.f, 0.f);
+        for (int q = 0; q < 8; q++) v[q] = fvalid ? blk[c * N + t + q * NT] : make_float2(0.f, 0.f);
         if (c == KB - 1) {
           // every thread has read ring entry s: its next copy may land
           fence_proxy_async_smem();

@@ -175,7 +175,8 @@ def cpu_baseline(frames_u16, valid, sample_frames=24, sample_modes=6144, threads
                       f"modes of the TPAD={TPAD} masked WK, FP64, scaled to the {T}-frame video"}
 
 
-def fit_benchmark(n_eval=100000, n_train=1 << 19, n_videos=48, epochs=8, oracle_sample=256):
+def fit_benchmark(n_eval=100000, n_train=1 << 19, n_videos=48, epochs=8, oracle_sample=256, pipeline=None,
+                  heldout_videos=0):
     """q-fits/s of the batched LM on held-out q-curves: plain (the reference's
     start strategy), surrogate-seeded, and surrogate-seeded with the plain
     strategy as fallback; the surrogate trained here on the GPU (analytic
@@ -186,7 +187,8 @@ def fit_benchmark(n_eval=100000, n_train=1 << 19, n_videos=48, epochs=8, oracle_
     import torch
     from hackathon_b200 import surrogate_train as ST
     t0 = time.perf_counter()
-    net = ST.build_and_train(n_analytic=n_train, n_videos=n_videos, epochs=epochs, seed=0, batch_max=8192)
+    net = ST.build_and_train(n_analytic=n_train, n_videos=n_videos, epochs=epochs, seed=0, batch_max=8192,
+                             pipeline=pipeline, log=lambda m: print(m, file=sys.stderr, flush=True))
     t_train = time.perf_counter() - t0
     held = ST.analytic_set(n_eval, seed=12345)
     bnds = ST.swim_bounds(held["qn"])
@@ -203,6 +205,7 @@ def fit_benchmark(n_eval=100000, n_train=1 << 19, n_videos=48, epochs=8, oracle_
     fb = res["fallback"]
     summary.update({
         "train_curves": int(n_train), "train_videos": int(n_videos), "train_s": t_train,
+        "train_set": getattr(net, "train_info", None),
         "oracle_sample": int(len(idx)), "oracle_qfits_per_s_1core": len(idx) / t_or,
         # equal fit error: cost within 1e-3 of the FP64 oracle's, or lower
         "fallback_frac_equal_or_better_than_fp64_oracle": float((fb["cost"][idx] <= oc * (1 + 1e-3)).mean()),
@@ -210,6 +213,12 @@ def fit_benchmark(n_eval=100000, n_train=1 << 19, n_videos=48, epochs=8, oracle_
             (res["seeded"]["cost"][idx] <= oc * (1 + 1e-3)).mean()),
         "plain_frac_cost_within_1e-3_of_fp64_oracle": float(
             (np.abs(res["plain"]["cost"][idx] - oc) <= 1e-3 * oc).mean())})
+    if heldout_videos:
+        # held-out curves from the pipeline itself (fresh videos and seeds)
+        hp = ST.pipeline_set(heldout_videos, 777, label="truth",
+                             **{k: v for k, v in (pipeline or {}).items() if k != "max_curves"})
+        ps, pres = ST.compare_fits(net, hp, ST.swim_bounds(hp["qn"]))
+        summary["heldout_pipeline"] = {k: v for k, v in ps.items()}
     net.close()
     torch.cuda.synchronize()
     return summary
@@ -419,7 +428,7 @@ def run_batch(args, rank, world, dist):
     local = int(os.environ.get("LOCAL_RANK", 0))
     torch.cuda.set_device(local)
     rng = np.random.default_rng(R.rank_seed(7, rank))
-    nvid = args.videos
+    nvid = args.videos or 48
     vids, engines, tuned = [], [], {}
     t_gen = time.perf_counter()
     for i in range(nvid):
@@ -509,6 +518,36 @@ def run_batch(args, rank, world, dist):
         e.destroy()
 
 
+
+SURROGATE_METRIC = "q-fits/s learned+LM vs plain LM at equal fit error (surrogate trained on 2^20 curves)"
+
+
+def run_surrogate(args, rank, world, dist):
+    """The learned-surrogate configuration at its stated size: the network is
+    trained on the GPU on 2^20 curves, 2^19 analytic model curves with 1 %
+    noise and 2^19 radial curves the engine itself produces from seeded
+    512^2 x 1024 videos (1024 q-bins over the network's q range, each video
+    labelled with its generator's parameters), then evaluated as the LM's
+    initial guess against plain LM on 10^5 held-out analytic curves and on
+    held-out pipeline curves of fresh videos."""
+    import torch
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+    half = 1 << 19
+    pipe = dict(N=512, T=1024, NB=1024, kmin=4.0, kmax=60.0, max_curves=half)
+    t0 = time.perf_counter()
+    fit = fit_benchmark(n_train=half, n_videos=args.videos or 2000, pipeline=pipe, heldout_videos=24)
+    if rank == 0:
+        line = {"metric": SURROGATE_METRIC, "value": fit["seeded_qfits_per_s"], "unit": "q-fits/s",
+                "n_gpus": 1, "higher_is_better": True, "dtype": "bf16 network, f32/f64 LM",
+                "data": "synthetic (analytic model curves + the engine's radial curves of seeded videos)",
+                "config": {"workload": "surrogate: 2^19 analytic + 2^19 pipeline training curves "
+                                       "(512^2 x 1024 videos, 1024 q-bins, k in [4, 60]); 10^5 held-out analytic "
+                                       "curves + held-out pipeline curves of 24 fresh videos",
+                           "pipeline": {k: v for k, v in pipe.items()}},
+                "vs_baseline": None, "total_s": time.perf_counter() - t0, "fit": fit}
+        print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -519,11 +558,12 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=6)
     ap.add_argument("--no-fit", action="store_true", help="skip the q-fits/s (surrogate + LM) section")
     ap.add_argument("--tuning", default="", help="chunk,unit[,variant]: apply instead of autotuning")
-    ap.add_argument("--workload", default="config2", choices=["config2", "large", "batch"],
+    ap.add_argument("--workload", default="config2", choices=["config2", "large", "batch", "surrogate"],
                     help="large: one 2048^2 x 4096 video per GPU (68.8 GB history), its own JSON line")
     ap.add_argument("--frames", type=int, default=0, help="large workload: frames per video (default 4096)")
     ap.add_argument("--roi", type=int, default=0, help="large workload: ROI size (default 2048)")
-    ap.add_argument("--videos", type=int, default=48, help="batch workload: number of videos")
+    ap.add_argument("--videos", type=int, default=0,
+                    help="batch workload: number of videos (48); surrogate: cap on pipeline videos (2000)")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", 0))
@@ -536,8 +576,8 @@ def main():
         import torch.distributed as dist
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    if args.impl == "ours" and args.workload in ("large", "batch"):
-        (run_large if args.workload == "large" else run_batch)(args, rank, world, dist)
+    if args.impl == "ours" and args.workload in ("large", "batch", "surrogate"):
+        {"large": run_large, "batch": run_batch, "surrogate": run_surrogate}[args.workload](args, rank, world, dist)
         if dist:
             dist.barrier()
             dist.destroy_process_group()

@@ -405,7 +405,7 @@ def run_large(args, rank, world, dist):
 
 
 BATCH_METRIC = "DDM frames/s, 48 uneven videos in one persistent launch"
-BATCH_WORKLOAD = ("48 seeded u16 videos, N in {256, 512} (384 and 768 need radix-3 transforms, not built), "
+BATCH_WORKLOAD = ("48 seeded u16 videos, N in {256, 384, 512, 768}, "
                   "T uniform in [300, 2000], per-video motile fraction in [0, 0.9], mean speed in [0.3, 3] "
                   "px/frame, D in [0.05, 0.5] px^2/frame, circular ROI of random radius, 2% dropped frames; "
                   "L = min(512, T/2), NB = N/4, kmin 4, kmax 0.39 N; one batched ingest + ONE temporal launch "
@@ -432,7 +432,7 @@ def run_batch(args, rank, world, dist):
     vids, engines, tuned = [], [], {}
     t_gen = time.perf_counter()
     for i in range(nvid):
-        N = int(rng.choice([256, 512]))
+        N = int(rng.choice([256, 384, 512, 768]))
         T = int(rng.integers(300, 2001)) // 2 * 2
         al, vb, Dd = rng.uniform(0, 0.9), rng.uniform(0.3, 3.0), rng.uniform(0.05, 0.5)
         spec = synth.VideoSpec(N=N, T=T, n_blobs=int(2000 * (N / 512) ** 2), frac_brownian=1 - al, D=Dd, vbar=vb,
@@ -503,7 +503,7 @@ def run_batch(args, rank, world, dist):
                 "warmup": max(args.warmup, 3), "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded GPU generator, hackathon_b200/synth.py)",
                 "config": {"workload": BATCH_WORKLOAD, "videos": nvid, "frames_per_step": total,
-                           "sizes": {str(n): sum(v["N"] == n for v in vids) for n in (256, 512)},
+                           "sizes": {str(n): sum(v["N"] == n for v in vids) for n in (256, 384, 512, 768)},
                            "l2": "inputs larger than L2", "generation_s": t_gen,
                            "autotuned": {str(n): {k: t[k] for k in ("best_chunk", "best_unit", "best_variant")}
                                          for n, t in tuned.items()}},

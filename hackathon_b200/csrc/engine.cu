@@ -287,8 +287,8 @@ extern "C" int ddm_create(const ddm_geometry *geometry, ddm_engine **out) {
     while (g.TPAD < 2 * g.T) g.TPAD <<= 1;
   }
   char msg[256] = {0};
-  if (!is_pow2(g.N) || g.N < 64 || g.N > 2048)
-    snprintf(msg, sizeof msg, "N = %d: must be a power of two in [64, 2048]", g.N);
+  if (!((is_pow2(g.N) && g.N >= 64 && g.N <= 2048) || g.N == 384 || g.N == 768))
+    snprintf(msg, sizeof msg, "N = %d: must be a power of two in [64, 2048], or 384 or 768", g.N);
   else if (g.T < 2 || !is_pow2(g.TPAD) || g.TPAD < 128 || g.TPAD > 8192 || 2 * g.T > g.TPAD)
     snprintf(msg, sizeof msg, "T = %d, TPAD = %d: need TPAD a power of two in [128, 8192] and TPAD >= 2T",
              g.T, g.TPAD);

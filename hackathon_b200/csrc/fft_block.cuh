@@ -118,6 +118,41 @@ struct Dft<8, INV> {
   }
 };
 
+// 3-point DFT: X1,2 = a0 - (a1 + a2)/2 -+ i (sqrt(3)/2)(a1 - a2) (forward).
+template <bool INV>
+struct Dft<3, INV> {
+  static DDM_HD void run(float2* a) {
+    const float h = 0.86602540378443865f;  // sin(2 pi / 3)
+    const float2 s = cadd(a[1], a[2]), d = csub(a[1], a[2]);
+    const float2 m = make_float2(fmaf(-0.5f, s.x, a[0].x), fmaf(-0.5f, s.y, a[0].y));
+    const float2 r = rot<INV>(make_float2(h * d.x, h * d.y));  // -+ i h d
+    a[0] = cadd(a[0], s);
+    a[1] = cadd(m, r);
+    a[2] = csub(m, r);
+  }
+};
+
+// 6-point DFT as 2 x 3: DFT-3 of the even and the odd inputs, then
+// X[k] = E[k] + W6^k O[k], X[k + 3] = E[k] - W6^k O[k], k < 3.
+template <bool INV>
+struct Dft<6, INV> {
+  static DDM_HD void run(float2* a) {
+    float2 e[3] = {a[0], a[2], a[4]};
+    float2 o[3] = {a[1], a[3], a[5]};
+    Dft<3, INV>::run(e);
+    Dft<3, INV>::run(o);
+    const float h = 0.86602540378443865f, sg = INV ? 1.f : -1.f;
+    const float2 w1 = cmul(o[1], make_float2(0.5f, sg * h));   // W6^1
+    const float2 w2 = cmul(o[2], make_float2(-0.5f, sg * h));  // W6^2
+    a[0] = cadd(e[0], o[0]);
+    a[3] = csub(e[0], o[0]);
+    a[1] = cadd(e[1], w1);
+    a[4] = csub(e[1], w1);
+    a[2] = cadd(e[2], w2);
+    a[5] = csub(e[2], w2);
+  }
+};
+
 // 16-point DFT as 4 x 4: inner DFT-4 over n1 of x[4 n1 + n2], twiddle
 // W16^(n2 k1), outer DFT-4 over n2; output X[k1 + 4 k2].
 template <bool INV>
@@ -356,6 +391,98 @@ template <int n, bool INV>
 __device__ __forceinline__ void fft16(float2 (&v)[16], int t, float2* buf, const float2* __restrict__ tw,
                                       int bar_id) {
   Stages16<n, INV>::run(v, t, buf, tw, bar_id);
+}
+
+}  // namespace ddm
+
+// ---------------------------------------------------------------------------
+// P points per thread, mixed radix (sizes with a factor 3: 384, 768).
+//
+// An n-point transform over n/P threads, P = 24 (= 8 x 3) points per thread;
+// stage radices are 8 while n/Ns is a multiple of 8, then 6, 4, 3 or 2
+// (384 = 8 x 8 x 6, 768 = 8 x 8 x 6 x 2); every radix divides P, so a stage
+// is P/R butterflies per thread. Same layout contract, ping-pong buffers,
+// swizzle (n is a multiple of 16) and twiddle-table layout as the radix-8
+// transforms, with this plan.
+
+namespace ddm {
+
+__host__ __device__ constexpr int radix_p(int n, int ns) {
+  return (n / ns) % 8 == 0 ? 8 : (n / ns) % 6 == 0 ? 6 : (n / ns) % 4 == 0 ? 4 : (n / ns) % 3 == 0 ? 3 : 2;
+}
+__host__ __device__ constexpr int fft_stages_p(int n) {
+  int s = 0;
+  for (int ns = 1; ns < n; ns *= radix_p(n, ns)) s++;
+  return s;
+}
+__host__ __device__ constexpr int tw_offset_p(int n, int Ns) {
+  int off = 0;
+  for (int ns = 1; ns < Ns;) {
+    const int r = radix_p(n, ns);
+    if (ns > 1) off += (r - 1) * ns;
+    ns *= r;
+  }
+  return off;
+}
+__host__ __device__ constexpr int tw_size_p(int n) { return tw_offset_p(n, n); }
+
+template <int n, int P, int R, int Ns, bool INV>
+__device__ __forceinline__ void stage_p(float2 (&v)[P], int t, float2* __restrict__ out,
+                                        const float2* __restrict__ tw) {
+  constexpr int NT = n / P;
+  constexpr int B = P / R;
+  static_assert(P % R == 0, "the radix divides the points per thread");
+#pragma unroll
+  for (int i = 0; i < B; i++) {
+    const int j = t + i * NT;
+    const int k = j % Ns;
+    float2 a[R];
+#pragma unroll
+    for (int m = 0; m < R; m++) a[m] = v[i + B * m];
+    if (Ns > 1) {
+      const float2* tws = tw + tw_offset_p(n, Ns) + k;
+#pragma unroll
+      for (int m = 1; m < R; m++) {
+        float2 w = tws[(m - 1) * Ns];
+        if (INV) w.y = -w.y;
+        a[m] = cmul(a[m], w);
+      }
+    }
+    Dft<R, INV>::run(a);
+    const int base = (j - k) * R + k;
+#pragma unroll
+    for (int m = 0; m < R; m++) out[pad(base + m * Ns)] = a[m];
+  }
+}
+
+template <int n, int P>
+__device__ __forceinline__ void load_p(float2 (&v)[P], int t, const float2* __restrict__ buf) {
+  constexpr int NT = n / P;
+#pragma unroll
+  for (int q = 0; q < P; q++) v[q] = buf[pad(t + q * NT)];
+}
+
+template <int n, int P, int Ns, bool INV, int SYNC>
+struct StagesP {
+  static __device__ __forceinline__ void run(float2 (&v)[P], int t, float2* a, float2* b,
+                                             const float2* __restrict__ tw, int bar_id) {
+    constexpr int R = radix_p(n, Ns);
+    stage_p<n, P, R, Ns, INV>(v, t, a, tw);
+    stage_sync<n * 8 / P, SYNC>(bar_id);  // the group's n/P threads
+    if constexpr (Ns * R < n) {
+      load_p<n, P>(v, t, a);
+      StagesP<n, P, Ns * R, INV, SYNC>::run(v, t, b, a, tw, bar_id);
+    }
+  }
+};
+
+// Full n-point transform of the P register points per thread; returns the
+// buffer holding the natural-order result (read it at pad(k)).
+template <int n, int P, bool INV, int SYNC>
+__device__ __forceinline__ float2* fft_p(float2 (&v)[P], int t, float2* buf0, float2* buf1,
+                                         const float2* __restrict__ tw, int bar_id = 0) {
+  StagesP<n, P, 1, INV, SYNC>::run(v, t, buf0, buf1, tw, bar_id);
+  return (fft_stages_p(n) & 1) ? buf0 : buf1;
 }
 
 }  // namespace ddm

@@ -44,9 +44,33 @@ __device__ __forceinline__ float ld_pix(const Tin* p) {
   return (float)__ldg(p);
 }
 
+// Points per thread of an N-point transform: 8 (radix-8 plan) for powers of
+// two, 24 (mixed radix, fft_p) for the sizes with a factor 3 (384, 768).
+__host__ __device__ constexpr int pts(int N) { return N % 3 == 0 ? 24 : 8; }
+
 template <int N>
 __host__ __device__ constexpr int row_groups() {
-  return 256 / (N / 8) >= 1 ? 256 / (N / 8) : 1;
+  return 256 / (N / pts(N)) >= 1 ? 256 / (N / pts(N)) : 1;
+}
+
+// twiddle table length and barrier scope of the plan of N
+template <int N>
+__host__ __device__ constexpr int tw_count() {
+  return pts(N) == 8 ? tw_size(N) : tw_size_p(N);
+}
+template <int N>
+__host__ __device__ constexpr int sync_of() {
+  return sync_kind(8 * N / pts(N), row_groups<N>());  // groups of N/pts(N) threads
+}
+
+// The column / row transform of this size.
+template <int N, bool INV, int SYNC>
+__device__ __forceinline__ float2* fft_n(float2 (&v)[pts(N)], int t, float2* buf0, float2* buf1,
+                                         const float2* __restrict__ tw, int bar_id) {
+  if constexpr (pts(N) == 8)
+    return fft<N, INV, true, SYNC>(v, t, buf0, buf1, tw, bar_id);
+  else
+    return fft_p<N, pts(N), INV, SYNC>(v, t, buf0, buf1, tw, bar_id);
 }
 constexpr int ROW_STAGES = 2;  // depth of the row-batch staging ring
 
@@ -104,12 +128,13 @@ __global__ void __launch_bounds__(CREF) cref_kernel(const Tin* __restrict__ fram
 // them.
 template <int N, typename Tin>
 __global__ void __launch_bounds__(256) rows_kernel(RowParams p) {
-  constexpr int NT = N / 8;
+  constexpr int P = pts(N);
+  constexpr int NT = N / P;
   constexpr int G = row_groups<N>();
   constexpr int PN = padded(N);
   constexpr int NHB = (N / 2 + 1 + KB - 1) / KB;
   constexpr int WARPS = (G * NT + 31) / 32;
-  constexpr int SYNC = sync_kind(N, G);
+  constexpr int SYNC = sync_of<N>();
   constexpr int BPF = N / (2 * G);  // batches per frame
   constexpr uint32_t BATCH_ELEMS = 2u * G * N;
   constexpr uint32_t BATCH_BYTES = BATCH_ELEMS * sizeof(Tin);
@@ -121,10 +146,10 @@ __global__ void __launch_bounds__(256) rows_kernel(RowParams p) {
   float2* buf0 = sm + (size_t)g * GSTRIDE<N>();
   float2* buf1 = buf0 + PN;
   float2* s_tw = sm + (size_t)G * GSTRIDE<N>();
-  float* s_wy = (float*)(s_tw + tw_size(N));                     // [N] w(y) scale
+  float* s_wy = (float*)(s_tw + tw_count<N>());                     // [N] w(y) scale
   Tin* ring = (Tin*)(s_wy + N);                                   // [ROW_STAGES][2G][N]
   uint8_t* mring = (uint8_t*)(ring + ROW_STAGES * BATCH_ELEMS);  // [ROW_STAGES][2G][N]
-  for (int i = threadIdx.x; i < tw_size(N); i += blockDim.x) s_tw[i] = p.tw[i];
+  for (int i = threadIdx.x; i < tw_count<N>(); i += blockDim.x) s_tw[i] = p.tw[i];
   for (int i = threadIdx.x; i < N; i += blockDim.x) s_wy[i] = p.wys[i];
   const long long nbatch = (long long)p.nframes * BPF;
   const Tin* frames = (const Tin*)p.frames;
@@ -144,9 +169,9 @@ __global__ void __launch_bounds__(256) rows_kernel(RowParams p) {
       if (b < nbatch) issue(b, s);
     }
   }
-  float wxs[8];  // w(x) at this thread's columns, fixed for the whole kernel
+  float wxs[P];  // w(x) at this thread's columns, fixed for the whole kernel
 #pragma unroll
-  for (int q = 0; q < 8; q++) wxs[q] = __ldg(&p.win[t + q * NT]);
+  for (int q = 0; q < P; q++) wxs[q] = __ldg(&p.win[t + q * NT]);
   // pixel sums: exact integers for u8/u16 (warp totals < 2^31), FP64 for f32
   constexpr bool INT = !std::is_floating_point<Tin>::value;
   using acc_t = typename std::conditional<INT, int, double>::type;
@@ -170,10 +195,10 @@ __global__ void __launch_bounds__(256) rows_kernel(RowParams p) {
     const Tin* r1 = r0 + N;
     const uint8_t* m0p = mring + st * BATCH_ELEMS + 2 * g * N;
     const float wy0 = s_wy[y0], wy1 = s_wy[y0 + 1];
-    float2 v[8];
+    float2 v[P];
     acc_t s = 0;
 #pragma unroll
-    for (int q = 0; q < 8; q++) {
+    for (int q = 0; q < P; q++) {
       const int x = t + q * NT;
       const float m0 = masked ? (float)m0p[x] : 1.f;
       const float m1 = masked ? (float)m0p[N + x] : 1.f;
@@ -189,7 +214,7 @@ __global__ void __launch_bounds__(256) rows_kernel(RowParams p) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = (double)s;
-    const float2* Z = fft<N, false, true, SYNC>(v, t, buf0, buf1, s_tw, 1 + g);
+    const float2* Z = fft_n<N, false, SYNC>(v, t, buf0, buf1, s_tw, 1 + g);
     __syncthreads();  // red[] and every group's row spectra complete; stage st is free
     if (threadIdx.x == 0) {
       const long long bn = b + (long long)ROW_STAGES * gridDim.x;
@@ -217,8 +242,8 @@ __global__ void __launch_bounds__(256) rows_kernel(RowParams p) {
 #pragma unroll
         for (int c = 0; c < KB; c++) {
           const int kx = kb * KB + c;
-          const float2 zk = Zg[pad(kx & (N - 1))];
-          const float2 zn = Zg[pad((N - kx) & (N - 1))];
+          const float2 zk = Zg[pad(kx < N ? kx : 0)];
+          const float2 zn = Zg[pad((N - kx) % N)];
           R[c] = (rr & 1) ? make_float2(0.5f * (zk.y + zn.y), -0.5f * (zk.x - zn.x))
                           : make_float2(0.5f * (zk.x + zn.x), 0.5f * (zk.y - zn.y));
           if (kx > N / 2) R[c] = make_float2(0.f, 0.f);  // past the half plane
@@ -241,10 +266,11 @@ __global__ void __launch_bounds__(256) rows_kernel(RowParams p) {
 // adding the mean correction (c_f - mu) FFT2(w m)(ky, kx) on the way.
 template <int N>
 __global__ void __launch_bounds__(256) cols_kernel(ColParams p) {
-  constexpr int NT = N / 8;
+  constexpr int P = pts(N);
+  constexpr int NT = N / P;
   constexpr int G = row_groups<N>();  // frames per tile, one per group
   constexpr int PN = padded(N);
-  constexpr int SYNC = sync_kind(N, G);
+  constexpr int SYNC = sync_of<N>();
   constexpr uint32_t FRAME_ELEMS = N * KB;  // float2 of one frame's block
   constexpr uint32_t FRAME_BYTES = FRAME_ELEMS * sizeof(float2);
   extern __shared__ __align__(16) float2 sm[];
@@ -255,8 +281,8 @@ __global__ void __launch_bounds__(256) cols_kernel(ColParams p) {
   float2* buf0 = sm + (size_t)g * GSTRIDE<N>();
   float2* buf1 = buf0 + PN;
   float2* s_tw = sm + (size_t)G * GSTRIDE<N>();
-  float2* stage = s_tw + tw_size(N);  // [G][KB][N]
-  for (int i = threadIdx.x; i < tw_size(N); i += blockDim.x) s_tw[i] = p.tw[i];
+  float2* stage = s_tw + tw_count<N>();  // [G][KB][N]
+  for (int i = threadIdx.x; i < tw_count<N>(); i += blockDim.x) s_tw[i] = p.tw[i];
   if (threadIdx.x < 4) s_wc4[threadIdx.x] = p.wc4[threadIdx.x];
   const int nfg = (p.nframes + G - 1) / G;
   const int ntiles = p.NHB * nfg;
@@ -297,9 +323,9 @@ __global__ void __launch_bounds__(256) cols_kernel(ColParams p) {
     for (int c = 0; c < KB; c++) {
       const int kx = kb * KB + c;
       if (kx >= p.NH) break;  // uniform over the CTA
-      float2 v[8];
+      float2 v[P];
 #pragma unroll
-      for (int q = 0; q < 8; q++) v[q] = fvalid ? blk[c * N + t + q * NT] : make_float2(0.f, 0.f);
+      for (int q = 0; q < P; q++) v[q] = fvalid ? blk[c * N + t + q * NT] : make_float2(0.f, 0.f);
       if (c == KB - 1 || kx + 1 >= p.NH) {
         // every thread has read the stage: the next tile's copies may land
         fence_proxy_async_smem();
@@ -314,7 +340,7 @@ __global__ void __launch_bounds__(256) cols_kernel(ColParams p) {
 #pragma unroll
         for (int i = 0; i < N / KYS; i++) wreg[i] = __ldg(&p.w2d[(size_t)kx * N + threadIdx.x / G + i * KYS]);
       }
-      const float2* Y = fft<N, false, true, SYNC>(v, t, buf0, buf1, s_tw, 1 + g);
+      const float2* Y = fft_n<N, false, SYNC>(v, t, buf0, buf1, s_tw, 1 + g);
       __syncthreads();  // every group's column (and s_dc) is in shared memory
       // Y of group g sits at the same offset in every group's buffer pair; the
       // CTA writes frame sf = tid % G of each mode: G consecutive ring slots
@@ -523,12 +549,12 @@ __global__ void __launch_bounds__(256, 1) cols_wide_kernel(ColParams p) {
 
 template <int N>
 static constexpr int groups() {
-  return 256 / (N / 8) >= 1 ? 256 / (N / 8) : 1;
+  return row_groups<N>();
 }
 
 template <int N>
 static size_t fft_smem() {
-  return ((size_t)groups<N>() * GSTRIDE<N>() + tw_size(N)) * sizeof(float2);
+  return ((size_t)groups<N>() * GSTRIDE<N>() + tw_count<N>()) * sizeof(float2);
 }
 
 // One wave of persistent CTAs. The occupancy query and the shared-memory
@@ -565,9 +591,9 @@ static cudaError_t rows_n(const RowParams& p, cudaStream_t s) {
   const long long npairs = (long long)p.nframes * (N / 2);
   auto k = rows_kernel<N, Tin>;
   const size_t sm = fft_smem<N>() + N * sizeof(float) + (size_t)ROW_STAGES * 2 * G * N * (sizeof(Tin) + 1);
-  const int grid = persistent_grid(k, G * (N / 8), sm, (npairs + G - 1) / G);
+  const int grid = persistent_grid(k, G * (N / pts(N)), sm, (npairs + G - 1) / G);
   if (p.nframes > 0) cref_kernel<N, Tin><<<p.nframes, CREF, 0, s>>>((const Tin*)p.frames, p.frame_stride, p.framec);
-  k<<<grid, G * (N / 8), sm, s>>>(p);
+  k<<<grid, G * (N / pts(N)), sm, s>>>(p);
   return cudaGetLastError();
 }
 
@@ -586,7 +612,9 @@ cudaError_t launch_rows(int N, int dtype, const RowParams& p, cudaStream_t s) {
     case 64: return rows_dt<64>(dtype, p, s);
     case 128: return rows_dt<128>(dtype, p, s);
     case 256: return rows_dt<256>(dtype, p, s);
+    case 384: return rows_dt<384>(dtype, p, s);
     case 512: return rows_dt<512>(dtype, p, s);
+    case 768: return rows_dt<768>(dtype, p, s);
     case 1024: return rows_dt<1024>(dtype, p, s);
     case 2048: return rows_dt<2048>(dtype, p, s);
     default: return cudaErrorInvalidValue;
@@ -610,13 +638,13 @@ static cudaError_t cols_n(const ColParams& p, cudaStream_t s) {
     auto k = cols_wide_kernel<N>;
     const size_t sm = cols_wide_smem<N>();
     const int grid = persistent_grid(k, G * (N / 8), sm, (long long)p.NHB * ((p.nframes + WIDE_F - 1) / WIDE_F));
-    k<<<grid, G * (N / 8), sm, s>>>(p);
+    k<<<grid, G * (N / pts(N)), sm, s>>>(p);
     return cudaGetLastError();
   }
   auto k = cols_kernel<N>;
   const size_t sm = fft_smem<N>() + (size_t)G * N * KB * sizeof(float2);
-  const int grid = persistent_grid(k, G * (N / 8), sm, (long long)p.NHB * ((p.nframes + G - 1) / G));
-  k<<<grid, G * (N / 8), sm, s>>>(p);
+  const int grid = persistent_grid(k, G * (N / pts(N)), sm, (long long)p.NHB * ((p.nframes + G - 1) / G));
+  k<<<grid, G * (N / pts(N)), sm, s>>>(p);
   return cudaGetLastError();
 }
 
@@ -625,13 +653,15 @@ cudaError_t launch_cols(int N, const ColParams& p, cudaStream_t s) {
     case 64: return cols_n<64>(p, s);
     case 128: return cols_n<128>(p, s);
     case 256: return cols_n<256>(p, s);
+    case 384: return cols_n<384>(p, s);
     case 512: return cols_n<512>(p, s);
+    case 768: return cols_n<768>(p, s);
     case 1024: return cols_n<1024>(p, s);
     case 2048: return cols_n<2048>(p, s);
     default: return cudaErrorInvalidValue;
   }
 }
 
-int frames_per_col_cta(int N) { return use_wide_cols(N) ? WIDE_F : 256 / (N / 8); }
+int frames_per_col_cta(int N) { return use_wide_cols(N) ? WIDE_F : 256 / (N / pts(N)); }
 
 }  // namespace ddm

@@ -5,8 +5,48 @@
 
 namespace ddm {
 
+// Decimation in time by the smallest prime factor p of n (p = 2 or 3, else
+// a direct DFT): p transforms of n/p points, combined with FP64 twiddles.
+// For lengths that are not powers of two (384, 768).
+static void mixed_fft(std::vector<cd>& a, bool inverse) {
+  const size_t n = a.size();
+  if (n <= 1) return;
+  const size_t p = n % 2 == 0 ? 2 : n % 3 == 0 ? 3 : n;
+  const double sgn = inverse ? 1.0 : -1.0;
+  if (p == n) {
+    std::vector<cd> out(n);
+    for (size_t k = 0; k < n; k++) {
+      cd s(0, 0);
+      for (size_t j = 0; j < n; j++) {
+        const double ang = sgn * 2.0 * M_PI * (double)((j * k) % n) / (double)n;
+        s += a[j] * cd(std::cos(ang), std::sin(ang));
+      }
+      out[k] = s;
+    }
+    a.swap(out);
+    return;
+  }
+  const size_t m = n / p;
+  std::vector<std::vector<cd>> sub(p, std::vector<cd>(m));
+  for (size_t r = 0; r < p; r++)
+    for (size_t k = 0; k < m; k++) sub[r][k] = a[k * p + r];
+  for (size_t r = 0; r < p; r++) mixed_fft(sub[r], inverse);
+  for (size_t k = 0; k < n; k++) {
+    cd s(0, 0);
+    for (size_t r = 0; r < p; r++) {
+      const double ang = sgn * 2.0 * M_PI * (double)((r * k) % n) / (double)n;
+      s += sub[r][k % m] * cd(std::cos(ang), std::sin(ang));
+    }
+    a[k] = s;
+  }
+}
+
 void host_fft(std::vector<cd>& a, bool inverse) {
   const size_t n = a.size();
+  if (n & (n - 1)) {  // not a power of two
+    mixed_fft(a, inverse);
+    return;
+  }
   for (size_t i = 1, j = 0; i < n; i++) {  // bit reversal
     size_t bit = n >> 1;
     for (; j & bit; bit >>= 1) j ^= bit;
@@ -39,10 +79,15 @@ std::vector<double> blackman_harris(int n) {
 
 std::vector<float> twiddle_table(int n, int P) {
   // stage blocks w[(m-1)*Ns + k] = exp(-2 pi i m k / (Ns R)) (fft_block.cuh),
-  // radix P while n/Ns >= P, then the remainder
+  // radix P while n/Ns >= P, then the remainder; sizes with a factor 3 take
+  // the mixed-radix plan of fft_p (radix 8 while n/Ns is a multiple of 8,
+  // then 6, 4, 3, 2)
   std::vector<float> t;
+  const bool mixed = n % 3 == 0;
   for (int ns = 1; ns < n;) {
-    const int r = (n / ns) >= P ? P : (n / ns);
+    const int q = n / ns;
+    const int r = mixed ? (q % 8 == 0 ? 8 : q % 6 == 0 ? 6 : q % 4 == 0 ? 4 : q % 3 == 0 ? 3 : 2)
+                        : (q >= P ? P : q);
     if (ns > 1)
       for (int m = 1; m < r; m++)
         for (int k = 0; k < ns; k++) {

@@ -23,6 +23,7 @@ VIDEOS = [  # (N, T, L, NB, kmin, kmax) -- uneven sizes and frame counts
     (128, 1000, 400, 16, 2.0, 40.0),
     (512, 512, 200, 32, 4.0, 120.0),
     (256, 2000, 512, 24, 3.0, 60.0),
+    (384, 400, 160, 24, 4.0, 90.0),  # mixed-radix size
 ]
 
 

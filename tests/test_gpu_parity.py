@@ -229,20 +229,37 @@ def test_ring_slots_wrap():
     eng.destroy()
 
 
-@pytest.mark.parametrize("N", [128, 512, 1024, 2048])
+def _numpy_history(luma, slots, T):
+    """FP64 reference history for any N (numpy FFT): per frame the half-plane
+    spectrum of (I - mean) w(x) w(y) / N, mode ky*NH + kx, ring slot."""
+    F_, N, _ = luma.shape
+    NH = N // 2 + 1
+    w = O.blackman_harris(N)
+    hist = np.zeros((N * NH, T), np.complex128)
+    for i in range(F_):
+        img = luma[i]
+        hist[:, slots[i] % T] = (np.fft.fft2((img - img.mean()) * w[None, :] * w[:, None])[:, :NH] / N).reshape(-1)
+    return hist
+
+
+@pytest.mark.parametrize("N", [128, 384, 512, 768, 1024, 2048])
 def test_spectrum_sizes(N):
     """Other ROI sizes (extension; 2048 is the large streamed configuration's
-    ROI): 2D spectrum vs the FP64 oracle. At 1024 and 2048 the column pass
-    works on tiles of four frames: 1024 also covers a partial tile (six
-    frames) and slots that are not consecutive."""
-    T = {1024: 6, 2048: 4}.get(N, 8)
+    ROI; 384 and 768, of the batched-video configuration, run the mixed-radix
+    transforms): 2D spectrum vs the FP64 oracle (numpy's FP64 FFT for 384 and
+    768: the oracle's transform, like the reference's, is radix 2). At 1024
+    and 2048 the column pass works on tiles of four frames: 1024 also covers
+    a partial tile (six frames) and slots that are not consecutive, and so
+    does 768 (twenty frames, eight per tile)."""
+    T = {1024: 6, 2048: 4, 768: 20}.get(N, 8)
     rng = np.random.default_rng(N)
     frames = rng.integers(0, 4096, (T, N, N)).astype(np.uint16)
-    slots = rng.permutation(T).astype(np.int32) if N == 1024 else np.arange(T, dtype=np.int32)
+    slots = rng.permutation(T).astype(np.int32) if N in (768, 1024) else np.arange(T, dtype=np.int32)
     eng = _engine(N=N, T=T, L=4, NB=8, kmin=2, kmax=N // 4)
     eng.ingest_frames(frames, slots, 1.0 / 4095)
     g = eng.read_history()
-    hist = O.history_ingest(frames.astype(np.float64) / 4095, slots, T)
+    luma = frames.astype(np.float64) / 4095
+    hist = _numpy_history(luma, slots, T) if N % 3 == 0 else O.history_ingest(luma, slots, T)
     rms = np.sqrt(np.mean(np.abs(hist) ** 2))
     assert np.abs(g - hist).max() / rms < 2e-5
     eng.destroy()
@@ -358,3 +375,29 @@ def test_temporal_tpad8192(N, L, NB, kmax):
         assert _p99(eD.ravel()) < 1e-4 and _p99(eC.ravel()) < 1e-4
         assert np.allclose(g["P"][modes][ok], Po[ok], rtol=1e-4, atol=0)
     eng.destroy()
+
+
+def test_radial_mixed_radix_size():
+    """A 384^2 video (the batched-video configuration's size with a factor
+    3): radial D, P against the oracle's temporal analysis of the FP64
+    (numpy) history of the same frames."""
+    N, T, L = 384, 64, 24
+    sim = dict(O.BASE, N=N, T=T, seed=41, swimmers=dict(n=40, vbar=20.0, sigma=8.0, geometry="3d"),
+               passive=dict(n=40), dropExact=5)
+    frames, valid, _ = O.simulate(sim)
+    idx = np.nonzero(valid)[0]
+    eng = _engine(N=N, T=T, L=L, NB=16, kmin=4, kmax=100)
+    eng.ingest_frames(frames[idx], idx)
+    order, mask = O.linear_order(valid)
+    eng.compute_temporal(order, mask)
+    rg = eng.read_radial()
+    eng.destroy()
+    hist = _numpy_history(O.luma_of(frames[idx]), idx.astype(np.int32), T)
+    bins = O.make_bins(N, 16, 4, 100)
+    ro = O.analyze_radial(hist, order, mask, bins, L)
+    D = rg.D2()
+    for b in range(16):
+        sc = ro["D"][b].max()
+        if sc > 0:
+            assert np.abs(D[b] - ro["D"][b]).max() <= 1e-4 * sc, b
+    assert np.allclose(rg.P, ro["P"], rtol=1e-5, atol=0)

@@ -39,7 +39,7 @@ typedef struct ddm_engine ddm_engine;
  * Supported: N in {64..2048} and TPAD in {128..8192} powers of two,
  * 2 <= L <= T <= TPAD/2. */
 typedef struct ddm_geometry {
-  int32_t N;       /* ROI side in pixels */
+  int32_t N;       /* ROI side in pixels: a power of two in [64, 2048], or 384 or 768 */
   int32_t T;       /* history slots (frames) */
   int32_t TPAD;    /* temporal FFT length; 0 = smallest power of two >= max(2T, 128) */
   int32_t L;       /* lags 0..L-1 */

@@ -36,8 +36,8 @@ typedef struct ddm_engine ddm_engine;
 
 /* Geometry. The reference freezes N=256, T=256, TPAD=512, L=128, NB=32,
  * KMIN=4, KMAX=100, KNODES=4 (ddm_ref.js:18-31); here they are parameters.
- * Supported: N in {64..2048} and TPAD in {128..8192} powers of two,
- * 2 <= L <= T <= TPAD/2. */
+ * Supported: N a power of two in {64..2048} or 384 or 768 (mixed-radix
+ * transforms), TPAD a power of two in {128..8192}, 2 <= L <= T <= TPAD/2. */
 typedef struct ddm_geometry {
   int32_t N;       /* ROI side in pixels: a power of two in [64, 2048], or 384 or 768 */
   int32_t T;       /* history slots (frames) */

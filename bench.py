@@ -17,8 +17,9 @@ on the data path).
 
   fit    (rank 0) q-fits/s of the batched GPU LM on 10^5 held-out q-curves:
          plain (the reference's start strategy), seeded by the tensor-core
-         surrogate (trained in the run on 2^19 analytic curves + the engine's
-         own radial curves of 48 seeded videos), and seeded with the plain
+         surrogate (trained in the run on 2^20 curves: 2^19 analytic + 2^19
+         radial curves the engine produces from seeded 512^2 x 1024 videos;
+         also evaluated on held-out pipeline curves), and seeded with the plain
          strategy as fallback; fit error as the share of curves whose cost is
          within 1e-3 of the plain LM's, and agreement with the FP64 LM oracle
          on a bounded sample.
@@ -175,8 +176,13 @@ def cpu_baseline(frames_u16, valid, sample_frames=24, sample_modes=6144, threads
                       f"modes of the TPAD={TPAD} masked WK, FP64, scaled to the {T}-frame video"}
 
 
-def fit_benchmark(n_eval=100000, n_train=1 << 19, n_videos=48, epochs=8, oracle_sample=256, pipeline=None,
-                  heldout_videos=0):
+# the surrogate's training videos: 512^2 x 1024, 1024 q-bins over the network's
+# q range, until 2^19 pipeline curves (half of the 2^20-curve training set)
+PIPELINE = dict(N=512, T=1024, NB=1024, kmin=4.0, kmax=60.0, max_curves=1 << 19)
+
+
+def fit_benchmark(n_eval=100000, n_train=1 << 19, n_videos=2000, epochs=8, oracle_sample=256, pipeline=PIPELINE,
+                  heldout_videos=24):
     """q-fits/s of the batched LM on held-out q-curves: plain (the reference's
     start strategy), surrogate-seeded, and surrogate-seeded with the plain
     strategy as fallback; the surrogate trained here on the GPU (analytic
@@ -533,7 +539,7 @@ def run_surrogate(args, rank, world, dist):
     import torch
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
     half = 1 << 19
-    pipe = dict(N=512, T=1024, NB=1024, kmin=4.0, kmax=60.0, max_curves=half)
+    pipe = PIPELINE
     t0 = time.perf_counter()
     fit = fit_benchmark(n_train=half, n_videos=args.videos or 2000, pipeline=pipe, heldout_videos=24)
     if rank == 0:

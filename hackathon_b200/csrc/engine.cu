@@ -30,6 +30,7 @@ thread_local std::string g_create_error;
 struct ddm_engine {
   ddm_geometry g{};
   int NH = 0, NHB = 0, modes = 0, chunk = 0, chunk_cap = 0, unit_size = 0, variant = 0;
+  bool sparse_enabled = true;  // the sparse-mask temporal kernel for masks with few zeros
   int device = 0;
   std::string err;
   int64_t launches = 0, throttled = 0;
@@ -653,6 +654,15 @@ static int temporal_impl(ddm_engine *h, const uint32_t *order, const float *mask
   tp.tw = h->d_tw_t;
   tp.tw16 = h->d_tw_t16;
   tp.variant = h->variant;
+  {  // a 0/1 mask with few zeros: A + B from prefix sums (temporal_sparse_kernel)
+    int nz = 0;
+    bool binary = true;
+    for (int j = 0; j < T; j++) {
+      nz += mask[j] == 0.f;
+      binary = binary && (mask[j] == 0.f || mask[j] == 1.f);
+    }
+    tp.sparse = h->sparse_enabled && binary && nz <= SPARSE_ZMAX && temporal_sparse_ok(TPAD) ? 1 : 0;
+  }
   tp.unit_counter = h->d_counter;
   tp.err = h->d_err;
   tp.T = T;
@@ -670,7 +680,7 @@ static int temporal_impl(ddm_engine *h, const uint32_t *order, const float *mask
     tp.outD = h->d_fullD;
     tp.outC = h->d_fullC;
     tp.outP = h->d_fullP;
-    const int grid = std::min(temporal_max_grid(TPAD, T, L, true), h->nunits_full);
+    const int grid = std::min(temporal_max_grid(TPAD, T, L, true, 0, tp.sparse != 0), h->nunits_full);
     CK(cudaMemsetAsync(h->d_counter, 0, sizeof(int), st));
     CKL(launch_temporal(TPAD, L, true, tp, std::max(grid, 1), st));
     RadialFullParams rp{};
@@ -691,7 +701,7 @@ static int temporal_impl(ddm_engine *h, const uint32_t *order, const float *mask
     tp.units = h->d_units;
     tp.nunits = h->nunits;
     tp.partials = h->d_partials;
-    const int grid = std::min(temporal_max_grid(TPAD, T, L, false, h->variant), h->nunits);
+    const int grid = std::min(temporal_max_grid(TPAD, T, L, false, h->variant, tp.sparse != 0), h->nunits);
     CK(cudaMemsetAsync(h->d_counter, 0, sizeof(int), st));
     if (h->nunits > 0) CKL(launch_temporal(TPAD, L, false, tp, std::max(grid, 1), st));
     ReduceParams rp{};
@@ -1318,6 +1328,12 @@ extern "C" int ddm_autotune(ddm_engine *h, char *report, int32_t report_len) {
     report[report_len - 1] = 0;
   }
   return check_device_error(h);
+}
+
+extern "C" int ddm_set_sparse(ddm_engine *h, int32_t enable) {
+  if (!h) return DDM_ERR_ARG;
+  h->sparse_enabled = enable != 0;
+  return DDM_OK;
 }
 
 extern "C" int ddm_get_tuning(const ddm_engine *h, int32_t *chunk, int32_t *unit_size, int32_t *variant) {

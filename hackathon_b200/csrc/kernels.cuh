@@ -73,7 +73,11 @@ struct TemporalParams {
   int T, L;                // single video; batched: the largest T and L
   const VideoDesc* videos; // nullptr: one video (the fields above); else units[u].w indexes it
   int variant;             // 0: one-group radix-8 kernel; 1: two-group radix-16 (TPAD 1024..4096)
+  int sparse;              // 1: single video whose mask has <= SPARSE_ZMAX zeros: A+B from
+                           // prefix sums (temporal_sparse_kernel); 0: by transforms
 };
+
+constexpr int SPARSE_ZMAX = 64;  // masked time indices the sparse temporal kernel takes
 
 struct ReduceParams {
   const double* partials;
@@ -126,9 +130,11 @@ cudaError_t launch_cols(int N, const ColParams& p, cudaStream_t s);
 int frames_per_col_cta(int N);
 cudaError_t launch_temporal(int TPAD, int L, bool full, const TemporalParams& p, int grid,
                             cudaStream_t s);
-int temporal_max_grid(int TPAD, int T, int L, bool full, int variant = 0);
+int temporal_max_grid(int TPAD, int T, int L, bool full, int variant = 0, bool sparse = false);
 // whether the two-group radix-16 variant exists for this TPAD (fused path)
 bool temporal_has_variant16(int TPAD);
+// TPAD sizes the sparse-mask temporal kernel serves
+bool temporal_sparse_ok(int TPAD);
 cudaError_t launch_reduce(const ReduceParams& p, cudaStream_t s);
 cudaError_t launch_radial_full(const RadialFullParams& p, cudaStream_t s);
 cudaError_t launch_lm(const LmParams& p, cudaStream_t s);

@@ -787,6 +787,338 @@ __global__ void __launch_bounds__(NP / 16, 1) temporal_big_kernel(TemporalParams
   }
 }
 
+// ---------------------------------------------------------------------------
+// Sparse-mask variant (one video whose binary mask drops at most SPARSE_ZMAX
+// time indices, as in a recording with a few missing frames): A + B comes
+// from the time domain instead of a transform. With p(t) = m(t)|x(t)|^2 (zero
+// at the masked t, and zero outside [0, T)) and S(n) = sum_{t<n} p(t),
+//   A(tau) = sum_t m(t+tau) p(t) = S(T - tau) - sum_{d in Z} p(d - tau)
+//   B(tau) = sum_t m(t) p(t+tau) = S(T) - S(tau) - sum_{d in Z} p(d + tau)
+// over the masked set Z -- exact, and cheaper than FFT(p) and the inverse
+// transform of conj(M) P while |Z| is small. The two modes of a pair then
+// share ONE inverse transform, of |Y_a|^2 + i |Y_b|^2 (both real, so
+// W = n (G_a + i G_b) splits by W(tau) +- conj W(-tau)): three transforms per
+// pair instead of five, 1.5 per mode. Same staging, unit scheduling and
+// epilogues as temporal_kernel.
+// Layout: p of the pair interleaved (p_a, p_b) in a zero-padded shared row
+// (PADL zeros either side, PADL >= every lag a thread touches), so each
+// correction term is one unconditional 8-byte load serving both modes and
+// summed in FP32 (at most 2 SPARSE_ZMAX terms); S in FP64, scanned per pair
+// into the exchange buffer the inverse transform leaves free (2 T doubles
+// <= TPAD float2 as T <= TPAD / 2).
+__host__ __device__ constexpr int sparse_padl(int NP, int L, int LPT) {
+  return L > LPT * (NP / 8) ? L : LPT * (NP / 8);
+}
+
+template <int NP, int LPT, bool FULL>
+__global__ void __launch_bounds__(NP / 8, TemporalBounds<NP>::MIN_BLOCKS)
+    temporal_sparse_kernel(TemporalParams p) {
+  constexpr int NT = NP / 8;
+  constexpr int PN = padded(NP);
+  constexpr int WARPS = NT / 32;
+  static_assert(NT % 32 == 0 && WARPS >= 1, "whole warps (TPAD >= 256)");
+  extern __shared__ __align__(16) float2 sm[];
+  float2* bufA = sm;
+  float2* bufB = sm + PN;
+  __shared__ __align__(8) uint64_t mbar[2];
+  __shared__ int s_next, s_nz;
+  __shared__ int s_zero[SPARSE_ZMAX];
+  __shared__ double s_wt[2][WARPS];
+  const int t = threadIdx.x;
+  const int TS = p.T;                              // the video's T (single video)
+  const VideoDesc vd = video_of(p, 0);
+  const int L = vd.L, T = vd.T;
+  const int PADL = sparse_padl(NP, L, LPT);
+  float2* stage = sm + 2 * PN;                     // [2 buffers][2 rows][TS]
+  float2* s_tw = stage + 4 * TS;                   // per-stage twiddle blocks
+  float2* s_pp = s_tw + tw_size(NP);               // [PADL + TS + PADL] (p_a, p_b)
+  float* s_np = (float*)(s_pp + TS + 2 * PADL);    // N(tau), tau < L
+  float2* pz = s_pp + PADL;                        // pz[j] = p at time index j
+  const float invn = 0.5f / NP;
+  for (int i = t; i < tw_size(NP); i += NT) s_tw[i] = p.tw[i];
+  for (int i = t; i < TS + 2 * PADL; i += NT) s_pp[i] = make_float2(0.f, 0.f);
+  const float np0 = vd.npairs[0];
+  for (int i = t; i < L; i += NT) s_np[i] = vd.npairs[i];
+  uint32_t ord[4];
+  float msk[4];
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const int i = t + q * NT;
+    ord[q] = i < T ? __ldg(&vd.order[i]) : 0u;
+    msk[q] = i < T ? __ldg(&vd.mask[i]) : 0.f;
+  }
+  if (t < 32) {  // the masked time indices, ascending (one warp, ballots)
+    int nz = 0;
+    for (int j0 = 0; j0 < T; j0 += 32) {
+      const bool z = j0 + t < T && __ldg(&vd.mask[j0 + t]) == 0.f;
+      const unsigned b = __ballot_sync(0xffffffffu, z);
+      if (z) {
+        const int at = nz + __popc(b & ((1u << t) - 1u));
+        if (at < SPARSE_ZMAX) s_zero[at] = j0 + t;
+      }
+      nz += __popc(b);
+    }
+    if (t == 0) s_nz = nz < SPARSE_ZMAX ? nz : SPARSE_ZMAX;
+  }
+  if (t == 0) {
+    mbar_init(&mbar[0], 1);
+    mbar_init(&mbar[1], 1);
+    fence_barrier_init();
+    s_next = atomicAdd(p.unit_counter, 1);
+  }
+  __syncthreads();
+  const int nz = s_nz;
+  int u = s_next;
+  __syncthreads();
+  if (t == 0) {
+    s_next = atomicAdd(p.unit_counter, 1);
+    if (u < p.nunits) issue_pair(p, u, 0, stage, TS, &mbar[0]);
+  }
+  __syncthreads();
+  int unext = s_next;
+  int k = 0, buf = 0;
+  uint32_t phase = 0;
+  double acc[LPT][PFIELDS];
+  double accP = 0.0;
+#pragma unroll
+  for (int r = 0; r < LPT; r++)
+#pragma unroll
+    for (int c = 0; c < PFIELDS; c++) acc[r][c] = 0.0;
+
+  while (u < p.nunits) {
+    const int4 U = p.units[u];
+    int nu = u, nk = k + 2;
+    if (nk >= U.y) {
+      nu = unext;
+      nk = 0;
+    }
+    const bool prefetched = nu < p.nunits;
+    if (t == 0 && prefetched) issue_pair(p, nu, nk, stage + (buf ^ 1) * 2 * TS, TS, &mbar[buf ^ 1]);
+    if (!mbar_wait(&mbar[buf], (phase >> buf) & 1u, p.err, 1)) {
+      if (prefetched) mbar_wait(&mbar[buf ^ 1], (phase >> (buf ^ 1)) & 1u, p.err, 1);
+      return;
+    }
+    phase ^= 1u << buf;
+    const float2* rowa = stage + buf * 2 * TS;
+    const float2* rowb = rowa + TS;
+    const bool hasb = k + 1 < U.y;
+    const int4 ea = load_item(vd.items, U.x + k);
+    const int4 eb = hasb ? load_item(vd.items, U.x + k + 1) : ea;
+    float2 v[8];
+    float pa[4], sa[8];
+    // mode a: p_a(t) and Y_a = FFT(x_a); |Y_a|^2 kept in registers
+    gather<NP>(v, rowa, ord, msk);
+#pragma unroll
+    for (int q = 0; q < 4; q++) pa[q] = fmaf(v[q].x, v[q].x, v[q].y * v[q].y);
+    {
+      const float2* Y = fft<NP, false, true>(v, t, bufA, bufB, s_tw);
+#pragma unroll
+      for (int q = 0; q < 8; q++) {
+        const float2 y = Y[pad(t + q * NT)];
+        sa[q] = fmaf(y.x, y.x, y.y * y.y);
+      }
+    }
+    __syncthreads();  // Y_a read before the next transform writes the buffers
+    // mode b (zeros for the odd last mode of a unit)
+    if (hasb)
+      gather<NP>(v, rowb, ord, msk);
+    else
+#pragma unroll
+      for (int q = 0; q < 8; q++) v[q] = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int j = t + q * NT;
+      if (j < T) pz[j] = make_float2(pa[q], fmaf(v[q].x, v[q].x, v[q].y * v[q].y));
+    }
+    {
+      const float2* Y = fft<NP, false, true>(v, t, bufA, bufB, s_tw);
+#pragma unroll
+      for (int q = 0; q < 8; q++) {
+        const float2 y = Y[pad(t + q * NT)];
+        v[q] = make_float2(sa[q], fmaf(y.x, y.x, y.y * y.y));
+      }
+    }
+    __syncthreads();
+    const float2* W = fft<NP, true, true>(v, t, bufA, bufB, s_tw);
+    // S(j + 1) of both modes at Sd[j]: thread t sums time indices 4t..4t+3,
+    // warps scan, warp totals combine through shared memory
+    double2* Sd = reinterpret_cast<double2*>(W == bufA ? bufB : bufA);
+    {
+      double2 loc[4];
+      double ra = 0.0, rb = 0.0;
+#pragma unroll
+      for (int e = 0; e < 4; e++) {
+        const int j = 4 * t + e;
+        const float2 pv = j < T ? pz[j] : make_float2(0.f, 0.f);
+        ra += (double)pv.x;
+        rb += (double)pv.y;
+        loc[e] = make_double2(ra, rb);
+      }
+      double ta = ra, tb = rb;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const double ya = __shfl_up_sync(0xffffffffu, ta, o);
+        const double yb = __shfl_up_sync(0xffffffffu, tb, o);
+        if ((t & 31) >= o) {
+          ta += ya;
+          tb += yb;
+        }
+      }
+      if ((t & 31) == 31) {
+        s_wt[0][t >> 5] = ta;
+        s_wt[1][t >> 5] = tb;
+      }
+      __syncthreads();
+      double ba = ta - ra, bb = tb - rb;  // inclusive scan minus this thread's own sums
+      for (int w = 0; w < (t >> 5); w++) {
+        ba += s_wt[0][w];
+        bb += s_wt[1][w];
+      }
+#pragma unroll
+      for (int e = 0; e < 4; e++) {
+        const int j = 4 * t + e;
+        if (j < T) Sd[j] = make_double2(ba + loc[e].x, bb + loc[e].y);
+      }
+      __syncthreads();
+    }
+    const double2 ST = Sd[T - 1];
+    // E(tau) = A + B of both modes
+    auto base_of = [&](int tau) {
+      const double2 s1 = tau > 0 ? Sd[tau - 1] : make_double2(0.0, 0.0);
+      const double2 s2 = T - tau > 0 ? Sd[T - tau - 1] : make_double2(0.0, 0.0);
+      return make_double2(ST.x - s1.x + s2.x, ST.y - s1.y + s2.y);
+    };
+    // G of mode s from the shared transform: W = n (G_a + i G_b)
+    auto G_of = [&](int s, int tau, float& gx, float& gy) {
+      const float2 w0 = W[pad(tau)];
+      const float2 w1 = W[pad((NP - tau) & (NP - 1))];
+      if (s == 0) {
+        gx = (w0.x + w1.x) * invn;
+        gy = (w0.y - w1.y) * invn;
+      } else {
+        gx = (w0.y + w1.y) * invn;
+        gy = (w1.x - w0.x) * invn;
+      }
+    };
+    if (FULL) {
+      for (int tau = t; tau < L; tau += NT) {
+        float2 cr = make_float2(0.f, 0.f);
+        for (int z = 0; z < nz; z++) {
+          const int d = s_zero[z];
+          const float2 lo = pz[d - tau], hi = pz[d + tau];
+          cr.x += lo.x + hi.x;
+          cr.y += lo.y + hi.y;
+        }
+        const double2 E0 = base_of(tau);
+        const float np = s_np[tau];
+        const float inv = np > 0.5f ? 1.f / np : 0.f;
+#pragma unroll
+        for (int s = 0; s < 2; s++) {
+          if (s == 1 && !hasb) break;
+          const size_t mode = (size_t)(s ? eb : ea).x;
+          const double E = s ? E0.y - (double)cr.y : E0.x - (double)cr.x;
+          float gx, gy;
+          G_of(s, tau, gx, gy);
+          p.outD[mode * L + tau] = (float)((E - 2.0 * gx) * inv);
+          p.outC[mode * L + tau] = make_float2(gx * inv, gy * inv);
+        }
+      }
+      if (t == 0) {
+        p.outP[(size_t)ea.x] = np0 > 0.5f ? (float)(ST.x / np0) : 0.f;
+        if (hasb) p.outP[(size_t)eb.x] = np0 > 0.5f ? (float)(ST.y / np0) : 0.f;
+      }
+    } else {
+      float2 cr[LPT];
+#pragma unroll
+      for (int r = 0; r < LPT; r++) cr[r] = make_float2(0.f, 0.f);
+      for (int z = 0; z < nz; z++) {
+        const int d = s_zero[z];
+        const float2* lo = pz + (d - t);  // lo[-r NT] = p(d - tau)
+        const float2* hi = pz + (d + t);  // hi[r NT] = p(d + tau)
+#pragma unroll
+        for (int r = 0; r < LPT; r++) {
+          const float2 a = lo[-r * NT], b = hi[r * NT];
+          cr[r].x += a.x + b.x;
+          cr[r].y += a.y + b.y;
+        }
+      }
+      double2 E[LPT];
+#pragma unroll
+      for (int r = 0; r < LPT; r++) {
+        const int tau = t + r * NT;
+        const double2 E0 = base_of(tau < L ? tau : 0);
+        E[r] = make_double2(E0.x - (double)cr[r].x, E0.y - (double)cr[r].y);
+      }
+#pragma unroll 1
+      for (int s = 0; s < 2; s++) {
+        if (s == 1 && !hasb) break;
+        const int4 e = s ? eb : ea;
+        const double kx = e.y, ky = e.z;
+#pragma unroll
+        for (int r = 0; r < LPT; r++) {
+          const int tau = t + r * NT;
+          if (tau < L) {
+            const float n0 = s_np[tau];
+            const float inp = n0 > 0.5f ? 1.f / n0 : 0.f;
+            float gx, gy;
+            G_of(s, tau, gx, gy);
+            acc[r][0] += ((s ? E[r].y : E[r].x) - 2.0 * gx) * (double)inp;
+            if (tau + 1 < L) {
+              const float n1 = s_np[tau + 1];
+              const float inp1 = n1 > 0.5f ? 1.f / n1 : 0.f;
+              float g1x, g1y;
+              G_of(s, tau + 1, g1x, g1y);
+              const float cx = gx * inp, cy = gy * inp;
+              const float c1x = g1x * inp1, c1y = g1y * inp1;
+              const float zr = fmaf(c1x, cx, c1y * cy);  // C(tau+1) conj C(tau)
+              const float zi = fmaf(c1y, cx, -c1x * cy);
+              const float w = sqrtf(fmaf(zr, zr, zi * zi));
+              if (w > 0.f) {
+                const double wd = w, ph = atan2f(zi, zr);
+                acc[r][1] += wd;
+                acc[r][2] += wd * kx * kx;
+                acc[r][3] += wd * kx * ky;
+                acc[r][4] += wd * ky * ky;
+                acc[r][5] += wd * kx * ph;
+                acc[r][6] += wd * ky * ph;
+                acc[r][7] += wd * ph * ph;
+                acc[r][8] += 1.0;
+              }
+            }
+          }
+        }
+        accP += np0 > 0.5f ? (double)(float)((s ? ST.y : ST.x) / np0) : 0.0;
+      }
+    }
+    if (k + 2 >= U.y) {
+      if (!FULL) {
+        const int ul = u - vd.unit0;
+#pragma unroll
+        for (int r = 0; r < LPT; r++) {
+          const int tau = t + r * NT;
+          if (tau < L)
+#pragma unroll
+            for (int c = 0; c < PFIELDS; c++) {
+              vd.partials[((size_t)ul * PFIELDS + c) * L + tau] = acc[r][c];
+              acc[r][c] = 0.0;
+            }
+        }
+        if (t == 0) vd.partials[(size_t)vd.nunits * PFIELDS * L + ul] = accP;
+        accP = 0.0;
+      }
+      u = unext;
+      k = 0;
+      if (t == 0) s_next = atomicAdd(p.unit_counter, 1);
+    } else {
+      k += 2;
+    }
+    buf ^= 1;
+    fence_proxy_async_smem();  // this CTA's reads of the staged rows before the next TMA write
+    __syncthreads();           // also: the epilogue is done with W, Sd and pz before the next pair
+    unext = s_next;
+  }
+}
+
 // Sums the unit partials of each bin in unit order (deterministic), divides
 // D and P by the bin's mode count (ddm_ref.js:404-412) and writes the
 // reference's Radial layout: D[b*L+tau], P[b], drift[(b*L+tau)*8+c].
@@ -898,6 +1230,16 @@ static int lpt_big(int TPAD, int L) {
   return r <= 1 ? 1 : r <= 2 ? 2 : r <= 4 ? 4 : 8;
 }
 
+// the sparse-mask kernel: whole warps per transform group and room for its
+// buffers (TPAD 256..4096)
+__host__ __device__ constexpr bool sparse_ok(int NP) { return NP >= 256 && NP <= 4096; }
+
+template <int NP>
+static size_t temporal_sparse_smem(int T, int L, int LPT) {
+  return sizeof(float2) * (2 * (size_t)padded(NP) + 5 * (size_t)T + tw_size(NP) + 2 * (size_t)sparse_padl(NP, L, LPT)) +
+         sizeof(float) * (size_t)L;
+}
+
 template <int NP, int LPT, bool FULL>
 static cudaError_t launch_k(const TemporalParams& p, int grid, cudaStream_t s) {
   if constexpr (use_big(NP)) {
@@ -907,6 +1249,15 @@ static cudaError_t launch_k(const TemporalParams& p, int grid, cudaStream_t s) {
     k<<<grid, NP / 16, sm, s>>>(p);
     return cudaGetLastError();
   } else {
+    if constexpr (sparse_ok(NP)) {
+      if (p.sparse) {
+        auto k = temporal_sparse_kernel<NP, LPT, FULL>;
+        const size_t sm = temporal_sparse_smem<NP>(p.T, p.L, LPT);
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        k<<<grid, NP / 8, sm, s>>>(p);
+        return cudaGetLastError();
+      }
+    }
     if constexpr (use16(NP, FULL)) {
       if (p.variant == 1) {
         auto k = temporal16_kernel<NP, LPT>;
@@ -935,10 +1286,13 @@ static int occupancy_grid(K k, int threads, size_t smem) {
 }
 
 template <int NP, int LPT, bool FULL>
-static int grid_of(int T, int L, int variant) {
+static int grid_of(int T, int L, int variant, bool sparse) {
   if constexpr (use_big(NP)) {
     return occupancy_grid(temporal_big_kernel<NP, LPT, FULL>, NP / 16, temporal_big_smem<NP>(T, L));
   } else {
+    if constexpr (sparse_ok(NP))
+      if (sparse)
+        return occupancy_grid(temporal_sparse_kernel<NP, LPT, FULL>, NP / 8, temporal_sparse_smem<NP>(T, L, LPT));
     if constexpr (use16(NP, FULL))
       if (variant == 1) return occupancy_grid(temporal16_kernel<NP, LPT>, NP / 8, temporal16_smem<NP>(T, L));
     return occupancy_grid(temporal_kernel<NP, LPT, FULL>, NP / 8, temporal_smem<NP>(T, L));
@@ -947,66 +1301,68 @@ static int grid_of(int T, int L, int variant) {
 
 template <int NP>
 static cudaError_t dispatch_np(int T, int L, bool full, const TemporalParams* p, int grid,
-                               cudaStream_t s, int* grid_out, int variant) {
+                               cudaStream_t s, int* grid_out, int variant, bool sparse) {
   if (full) {
-    if (grid_out) *grid_out = grid_of<NP, 1, true>(T, L, variant);
+    if (grid_out) *grid_out = grid_of<NP, 1, true>(T, L, variant, sparse);
     return p ? launch_k<NP, 1, true>(*p, grid, s) : cudaSuccess;
   }
   if constexpr (use_big(NP)) {
     switch (lpt_big(NP, L)) {
       case 1:
-        if (grid_out) *grid_out = grid_of<NP, 1, false>(T, L, variant);
+        if (grid_out) *grid_out = grid_of<NP, 1, false>(T, L, variant, sparse);
         return p ? launch_k<NP, 1, false>(*p, grid, s) : cudaSuccess;
       case 2:
-        if (grid_out) *grid_out = grid_of<NP, 2, false>(T, L, variant);
+        if (grid_out) *grid_out = grid_of<NP, 2, false>(T, L, variant, sparse);
         return p ? launch_k<NP, 2, false>(*p, grid, s) : cudaSuccess;
       case 4:
-        if (grid_out) *grid_out = grid_of<NP, 4, false>(T, L, variant);
+        if (grid_out) *grid_out = grid_of<NP, 4, false>(T, L, variant, sparse);
         return p ? launch_k<NP, 4, false>(*p, grid, s) : cudaSuccess;
       default:
-        if (grid_out) *grid_out = grid_of<NP, 8, false>(T, L, variant);
+        if (grid_out) *grid_out = grid_of<NP, 8, false>(T, L, variant, sparse);
         return p ? launch_k<NP, 8, false>(*p, grid, s) : cudaSuccess;
     }
   }
   switch (lpt_of(NP, L)) {
     case 1:
-      if (grid_out) *grid_out = grid_of<NP, 1, false>(T, L, variant);
+      if (grid_out) *grid_out = grid_of<NP, 1, false>(T, L, variant, sparse);
       return p ? launch_k<NP, 1, false>(*p, grid, s) : cudaSuccess;
     case 2:
-      if (grid_out) *grid_out = grid_of<NP, 2, false>(T, L, variant);
+      if (grid_out) *grid_out = grid_of<NP, 2, false>(T, L, variant, sparse);
       return p ? launch_k<NP, 2, false>(*p, grid, s) : cudaSuccess;
     default:
-      if (grid_out) *grid_out = grid_of<NP, 4, false>(T, L, variant);
+      if (grid_out) *grid_out = grid_of<NP, 4, false>(T, L, variant, sparse);
       return p ? launch_k<NP, 4, false>(*p, grid, s) : cudaSuccess;
   }
 }
 
 static cudaError_t dispatch(int TPAD, int T, int L, bool full, const TemporalParams* p, int grid,
-                            cudaStream_t s, int* grid_out, int variant) {
+                            cudaStream_t s, int* grid_out, int variant, bool sparse) {
   switch (TPAD) {
-    case 128: return dispatch_np<128>(T, L, full, p, grid, s, grid_out, variant);
-    case 256: return dispatch_np<256>(T, L, full, p, grid, s, grid_out, variant);
-    case 512: return dispatch_np<512>(T, L, full, p, grid, s, grid_out, variant);
-    case 1024: return dispatch_np<1024>(T, L, full, p, grid, s, grid_out, variant);
-    case 2048: return dispatch_np<2048>(T, L, full, p, grid, s, grid_out, variant);
-    case 4096: return dispatch_np<4096>(T, L, full, p, grid, s, grid_out, variant);
-    case 8192: return dispatch_np<8192>(T, L, full, p, grid, s, grid_out, variant);
+    case 128: return dispatch_np<128>(T, L, full, p, grid, s, grid_out, variant, sparse);
+    case 256: return dispatch_np<256>(T, L, full, p, grid, s, grid_out, variant, sparse);
+    case 512: return dispatch_np<512>(T, L, full, p, grid, s, grid_out, variant, sparse);
+    case 1024: return dispatch_np<1024>(T, L, full, p, grid, s, grid_out, variant, sparse);
+    case 2048: return dispatch_np<2048>(T, L, full, p, grid, s, grid_out, variant, sparse);
+    case 4096: return dispatch_np<4096>(T, L, full, p, grid, s, grid_out, variant, sparse);
+    case 8192: return dispatch_np<8192>(T, L, full, p, grid, s, grid_out, variant, sparse);
     default: return cudaErrorInvalidValue;
   }
 }
 
 cudaError_t launch_temporal(int TPAD, int L, bool full, const TemporalParams& p, int grid,
                             cudaStream_t s) {
-  return dispatch(TPAD, p.T, L, full, &p, grid, s, nullptr, p.variant);
+  return dispatch(TPAD, p.T, L, full, &p, grid, s, nullptr, p.variant, p.sparse != 0);
 }
 
-int temporal_max_grid(int TPAD, int T, int L, bool full, int variant) {
+int temporal_max_grid(int TPAD, int T, int L, bool full, int variant, bool sparse) {
   int g = 0;
-  dispatch(TPAD, T, L, full, nullptr, 0, nullptr, &g, variant);
+  dispatch(TPAD, T, L, full, nullptr, 0, nullptr, &g, variant, sparse);
   return g;
 }
 
 bool temporal_has_variant16(int TPAD) { return use16(TPAD, false); }
+
+bool temporal_sparse_ok(int TPAD) { return sparse_ok(TPAD); }
 
 cudaError_t launch_reduce(const ReduceParams& p, cudaStream_t s) {
   const int threads = p.L >= 256 ? 256 : ((p.L + 31) / 32) * 32;

@@ -250,6 +250,12 @@ class DdmEngine:
         self._alive()
         self._check(self._lib.ddm_set_tuning(self._h, int(chunk), int(unit_size), int(variant)))
 
+    def set_sparse(self, enable=True):
+        """Sparse-mask temporal kernel for masks with at most 64 zeros
+        (ddm_set_sparse); False keeps the transform path for every mask."""
+        self._alive()
+        self._check(self._lib.ddm_set_sparse(self._h, 1 if enable else 0))
+
     @property
     def tuning(self):
         c, u, v = C.c_int32(), C.c_int32(), C.c_int32()

@@ -144,6 +144,31 @@ def test_radial_fused_parity(harness):
     assert np.allclose(rf.drift, rg.drift, rtol=1e-4, atol=1e-6 * np.abs(rg.drift).max())
 
 
+def test_radial_transform_path_parity(harness):
+    """The harness mask drops 37 frames, so computeTemporal takes the
+    sparse-mask kernel (A + B from prefix sums, 1.5 transforms per mode);
+    with it disabled the transform path (2.5 per mode) must meet the same
+    bounds against analyzeRadial, and the two paths agree closely."""
+    eng = harness["eng"]
+    order, mask = harness["order"], harness["mask"]
+    bins = O.make_bins(256, 32, 4, 100)
+    ro = O.analyze_radial(harness["hist"], order, mask, bins, 128)
+    try:
+        eng.set_sparse(False)
+        eng.compute_temporal(order, mask)
+        rt = eng.read_radial()
+    finally:
+        eng.set_sparse(True)
+    _radial_check(rt, ro, bins)
+    eng.compute_temporal(order, mask)
+    rs = eng.read_radial()
+    _radial_check(rs, ro, bins)
+    Dt, Ds = rt.D2(), rs.D2()
+    for b in range(rt.NB):
+        sc = np.abs(Dt[b]).max()
+        assert np.abs(Ds[b] - Dt[b]).max() <= 1e-5 * sc, b
+
+
 def test_verdict_parity(harness):
     """The motility analysis on GPU radial data matches the FP64 pipeline
     (harness.ts:154-178 thresholds)."""

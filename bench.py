@@ -720,18 +720,22 @@ def main():
         s["frac"] = s["GBps"] / peak
     # FP32 work, 5 n log2 n per complex FFT of n points
     fl_sp = T * (N // 2 + N // 2 + 1) * 5 * N * np.log2(N)
-    fl_tm = nbinned * 2.5 * 5 * TPAD * np.log2(TPAD)
+    # transforms per mode of the kernel that ran: 2.5 (masked WK by
+    # transforms), 1.5 (sparse-mask kernel: A + B from prefix sums)
+    tk = eng.last_temporal_kernel
+    fl_tm = nbinned * (1.5 if tk == "temporal_sparse_kernel" else 2.5) * 5 * TPAD * np.log2(TPAD)
     stages["spatial"]["gflop"] = fl_sp / 1e9
     stages["temporal"]["gflop"] = fl_tm / 1e9
-    # dominant kernel: temporal_kernel (one launch per step, the largest
-    # single kernel; the spatial stage is 2 kernels x 37 chunk launches)
+    stages["temporal"]["kernel"] = tk
+    # dominant kernel: the temporal kernel (one launch per step, the largest
+    # single kernel; the spatial stage is 3 kernels x 16 chunk launches)
     traffic = _profile_traffic() or {}
     tm = stages["temporal"]
-    roof = {"bound": "hbm", "kernel": "temporal_kernel", "achieved": tm["GBps"], "peak": peak,
+    roof = {"bound": "hbm", "kernel": tk, "achieved": tm["GBps"], "peak": peak,
             "unit": "GB/s", "frac": tm["frac"], "peak_source": peak_kind,
-            "traffic": traffic.get("temporal_kernel_bytes_per_launch"),
+            "traffic": traffic.get(f"{tk}_bytes_per_launch"),
             "algorithmic_bytes": tm["bytes"],
-            "timed_span": "temporal stage on the engine stream: meta upload + temporal_kernel + reduce_kernel",
+            "timed_span": f"temporal stage on the engine stream: meta upload + {tk} + reduce_kernel",
             "fp32_tflops": tm["gflop"] / tm["ms"], "fp32_frac_of_nominal": tm["gflop"] / tm["ms"] / FP32_NOMINAL_TFLOPS,
             "pipeline_GBps": (sp_bytes + tm_bytes) / (ms_step * 1e6),
             "pipeline_frac": (sp_bytes + tm_bytes) / (ms_step * 1e6) / peak,

@@ -31,6 +31,7 @@ struct ddm_engine {
   ddm_geometry g{};
   int NH = 0, NHB = 0, modes = 0, chunk = 0, chunk_cap = 0, unit_size = 0, variant = 0;
   bool sparse_enabled = true;  // the sparse-mask temporal kernel for masks with few zeros
+  int last_tk = -1;             // DDM_TK_* of the last temporal launch
   int device = 0;
   std::string err;
   int64_t launches = 0, throttled = 0;
@@ -663,6 +664,7 @@ static int temporal_impl(ddm_engine *h, const uint32_t *order, const float *mask
     }
     tp.sparse = h->sparse_enabled && binary && nz <= SPARSE_ZMAX && temporal_sparse_ok(TPAD) ? 1 : 0;
   }
+  h->last_tk = temporal_kernel_id(TPAD, full, h->variant, tp.sparse != 0);
   tp.unit_counter = h->d_counter;
   tp.err = h->d_err;
   tp.T = T;
@@ -1335,6 +1337,8 @@ extern "C" int ddm_set_sparse(ddm_engine *h, int32_t enable) {
   h->sparse_enabled = enable != 0;
   return DDM_OK;
 }
+
+extern "C" int ddm_last_temporal_kernel(const ddm_engine *h) { return h ? h->last_tk : DDM_ERR_ARG; }
 
 extern "C" int ddm_get_tuning(const ddm_engine *h, int32_t *chunk, int32_t *unit_size, int32_t *variant) {
   if (!h) return DDM_ERR_ARG;

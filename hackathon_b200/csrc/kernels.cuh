@@ -135,6 +135,8 @@ int temporal_max_grid(int TPAD, int T, int L, bool full, int variant = 0, bool s
 bool temporal_has_variant16(int TPAD);
 // TPAD sizes the sparse-mask temporal kernel serves
 bool temporal_sparse_ok(int TPAD);
+// which temporal kernel launch_temporal runs for these settings (DDM_TK_*)
+int temporal_kernel_id(int TPAD, bool full, int variant, bool sparse);
 cudaError_t launch_reduce(const ReduceParams& p, cudaStream_t s);
 cudaError_t launch_radial_full(const RadialFullParams& p, cudaStream_t s);
 cudaError_t launch_lm(const LmParams& p, cudaStream_t s);

@@ -33,6 +33,7 @@
 #include <cstdint>
 
 #include "async_copy.cuh"
+#include "ddm_b200.h"
 #include "fft_block.cuh"
 #include "kernels.cuh"
 
@@ -807,8 +808,12 @@ __global__ void __launch_bounds__(NP / 16, 1) temporal_big_kernel(TemporalParams
 // into the exchange buffer the inverse transform leaves free (2 T doubles
 // <= TPAD float2 as T <= TPAD / 2).
 __host__ __device__ constexpr int sparse_padl(int NP, int L, int LPT) {
-  return L > LPT * (NP / 8) ? L : LPT * (NP / 8);
+  return ((L > LPT * (NP / 8) ? L : LPT * (NP / 8)) + 1) & ~1;  // even: pz stays 16-byte aligned
 }
+// Slot of S(j + 1) in the scan buffer: a permutation inside aligned groups of
+// four, so the scan's stores (thread t: j = 4t + e) hit eight distinct 16-byte
+// bank groups per quarter-warp while consecutive-j reads stay conflict-free.
+__device__ __forceinline__ int sparse_sidx(int j) { return j ^ ((j >> 3) & 3); }
 
 template <int NP, int LPT, bool FULL>
 __global__ void __launch_bounds__(NP / 8, TemporalBounds<NP>::MIN_BLOCKS)
@@ -940,18 +945,24 @@ __global__ void __launch_bounds__(NP / 8, TemporalBounds<NP>::MIN_BLOCKS)
     }
     __syncthreads();
     const float2* W = fft<NP, true, true>(v, t, bufA, bufB, s_tw);
-    // S(j + 1) of both modes at Sd[j]: thread t sums time indices 4t..4t+3,
-    // warps scan, warp totals combine through shared memory
+    // S(j + 1) of both modes at Sd[sparse_sidx(j)] (slots < T rounded up to
+    // 4 <= TPAD / 2): thread t sums time indices 4t..4t+3, warps scan, warp
+    // totals combine through shared memory
     double2* Sd = reinterpret_cast<double2*>(W == bufA ? bufB : bufA);
     {
       double2 loc[4];
       double ra = 0.0, rb = 0.0;
+      // four consecutive (p_a, p_b) as two 16-byte loads (T even: a pair is
+      // either inside [0, T) or wholly beyond it)
+      float4 q2[2];
+#pragma unroll
+      for (int h = 0; h < 2; h++)
+        q2[h] = 4 * t + 2 * h < T ? reinterpret_cast<const float4*>(pz)[2 * t + h] : make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
       for (int e = 0; e < 4; e++) {
-        const int j = 4 * t + e;
-        const float2 pv = j < T ? pz[j] : make_float2(0.f, 0.f);
-        ra += (double)pv.x;
-        rb += (double)pv.y;
+        const float4 q = q2[e >> 1];
+        ra += (double)((e & 1) ? q.z : q.x);
+        rb += (double)((e & 1) ? q.w : q.y);
         loc[e] = make_double2(ra, rb);
       }
       double ta = ra, tb = rb;
@@ -977,15 +988,15 @@ __global__ void __launch_bounds__(NP / 8, TemporalBounds<NP>::MIN_BLOCKS)
 #pragma unroll
       for (int e = 0; e < 4; e++) {
         const int j = 4 * t + e;
-        if (j < T) Sd[j] = make_double2(ba + loc[e].x, bb + loc[e].y);
+        if (j < T) Sd[sparse_sidx(j)] = make_double2(ba + loc[e].x, bb + loc[e].y);
       }
       __syncthreads();
     }
-    const double2 ST = Sd[T - 1];
+    const double2 ST = Sd[sparse_sidx(T - 1)];
     // E(tau) = A + B of both modes
     auto base_of = [&](int tau) {
-      const double2 s1 = tau > 0 ? Sd[tau - 1] : make_double2(0.0, 0.0);
-      const double2 s2 = T - tau > 0 ? Sd[T - tau - 1] : make_double2(0.0, 0.0);
+      const double2 s1 = tau > 0 ? Sd[sparse_sidx(tau - 1)] : make_double2(0.0, 0.0);
+      const double2 s2 = T - tau > 0 ? Sd[sparse_sidx(T - tau - 1)] : make_double2(0.0, 0.0);
       return make_double2(ST.x - s1.x + s2.x, ST.y - s1.y + s2.y);
     };
     // G of mode s from the shared transform: W = n (G_a + i G_b)
@@ -1122,24 +1133,30 @@ __global__ void __launch_bounds__(NP / 8, TemporalBounds<NP>::MIN_BLOCKS)
 // Sums the unit partials of each bin in unit order (deterministic), divides
 // D and P by the bin's mode count (ddm_ref.js:404-412) and writes the
 // reference's Radial layout: D[b*L+tau], P[b], drift[(b*L+tau)*8+c].
+// Grid (lag blocks, bins), one thread per (bin, lag): the unit loop is
+// unrolled so several units' loads are in flight (the sums still add in
+// unit order).
 __global__ void reduce_kernel(ReduceParams p) {
-  const int b = blockIdx.x;
+  const int b = blockIdx.y;
   const int L = p.L;
+  const int tau = blockIdx.x * blockDim.x + threadIdx.x;
   const int u0 = p.bin_units[b], u1 = p.bin_units[b + 1];
   const double n = (double)p.nmodes[b];
   const double inv = n > 0 ? 1.0 / n : 0.0;
-  for (int tau = threadIdx.x; tau < L; tau += blockDim.x) {
+  if (tau < L) {
     double s[PFIELDS];
 #pragma unroll
     for (int c = 0; c < PFIELDS; c++) s[c] = 0.0;
+    const double* __restrict__ src = p.partials + tau;
+#pragma unroll 4
     for (int u = u0; u < u1; u++)
 #pragma unroll
-      for (int c = 0; c < PFIELDS; c++) s[c] += p.partials[((size_t)u * PFIELDS + c) * L + tau];
+      for (int c = 0; c < PFIELDS; c++) s[c] += __ldg(&src[((size_t)u * PFIELDS + c) * L]);
     p.D[(size_t)b * L + tau] = s[0] * inv;
 #pragma unroll
     for (int c = 0; c < DRIFT; c++) p.drift[((size_t)b * L + tau) * DRIFT + c] = s[c + 1];
   }
-  if (threadIdx.x == 0) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
     double s = 0.0;
     for (int u = u0; u < u1; u++) s += p.partials[(size_t)p.nunits * PFIELDS * L + u];
     p.P[b] = s * inv;
@@ -1364,9 +1381,16 @@ bool temporal_has_variant16(int TPAD) { return use16(TPAD, false); }
 
 bool temporal_sparse_ok(int TPAD) { return sparse_ok(TPAD); }
 
+int temporal_kernel_id(int TPAD, bool full, int variant, bool sparse) {
+  if (use_big(TPAD)) return DDM_TK_BIG;
+  if (sparse && sparse_ok(TPAD)) return DDM_TK_SPARSE;
+  if (use16(TPAD, full) && variant == 1) return DDM_TK_RADIX16;
+  return DDM_TK_RADIX8;
+}
+
 cudaError_t launch_reduce(const ReduceParams& p, cudaStream_t s) {
-  const int threads = p.L >= 256 ? 256 : ((p.L + 31) / 32) * 32;
-  reduce_kernel<<<p.NB, threads, 0, s>>>(p);
+  const int threads = p.L >= 128 ? 128 : ((p.L + 31) / 32) * 32;
+  reduce_kernel<<<dim3((p.L + threads - 1) / threads, p.NB), threads, 0, s>>>(p);
   return cudaGetLastError();
 }
 

@@ -256,6 +256,16 @@ class DdmEngine:
         self._alive()
         self._check(self._lib.ddm_set_sparse(self._h, 1 if enable else 0))
 
+    TEMPORAL_KERNELS = {0: "temporal_kernel", 1: "temporal16_kernel", 2: "temporal_sparse_kernel",
+                        3: "temporal_big_kernel"}
+
+    @property
+    def last_temporal_kernel(self):
+        """Name of the temporal kernel the last computeTemporal ran (None
+        before the first one)."""
+        self._alive()
+        return self.TEMPORAL_KERNELS.get(self._lib.ddm_last_temporal_kernel(self._h))
+
     @property
     def tuning(self):
         c, u, v = C.c_int32(), C.c_int32(), C.c_int32()

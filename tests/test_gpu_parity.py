@@ -157,11 +157,13 @@ def test_radial_transform_path_parity(harness):
         eng.set_sparse(False)
         eng.compute_temporal(order, mask)
         rt = eng.read_radial()
+        assert eng.last_temporal_kernel in ("temporal_kernel", "temporal16_kernel")
     finally:
         eng.set_sparse(True)
     _radial_check(rt, ro, bins)
     eng.compute_temporal(order, mask)
     rs = eng.read_radial()
+    assert eng.last_temporal_kernel == "temporal_sparse_kernel"
     _radial_check(rs, ro, bins)
     Dt, Ds = rt.D2(), rs.D2()
     for b in range(rt.NB):
@@ -234,6 +236,55 @@ def test_temporal_edge_cases(case):
     rg = eng.read_radial()
     ro = O.analyze_radial(hist, order, mask.astype(np.float64), bins, L, TPAD=eng.TPAD)
     # radial D against D's natural scale 2P (harness.ts:147), P relative
+    pscale = max(ro["P"].max(), 1e-30)
+    assert np.abs(rg.D.reshape(-1, L) - ro["D"]).max() <= 1e-4 * 2 * pscale
+    assert np.abs(rg.P - ro["P"]).max() <= 1e-5 * pscale
+    eng.destroy()
+
+
+@pytest.mark.parametrize("case", ["none", "ends", "run", "zmax", "zmax_plus1", "shuffled"])
+def test_temporal_sparse_edges(case):
+    """The sparse-mask kernel (0/1 masks with at most 64 zeros, TPAD >= 256)
+    against the FP64 oracle: no zeros, zeros at both ends of the series (the
+    corrections' zero padding), one run of 40 consecutive zeros, exactly 64
+    zeros, 65 zeros (the transform path takes over), a shuffled order; full
+    per-mode outputs and the fused radial path."""
+    N, T, L = 64, 128, 100
+    rng = np.random.default_rng(11)
+    frames = rng.integers(0, 65536, (T, N, N)).astype(np.uint16)
+    eng = _engine(N=N, T=T, L=L, NB=16, kmin=2, kmax=30)
+    assert eng.TPAD == 256
+    slots = np.arange(T, dtype=np.int32)
+    eng.ingest_frames(frames, slots, 1.0 / 65535)
+    hist = O.history_ingest(frames.astype(np.float64) / 65535, slots, T)
+    order = np.arange(T, dtype=np.uint32)
+    mask = np.ones(T, np.float32)
+    if case == "ends":
+        mask[[0, 1, 5, 60, T - 2, T - 1]] = 0
+    elif case == "run":
+        mask[30:70] = 0
+    elif case in ("zmax", "zmax_plus1"):
+        mask[rng.choice(T, 64 if case == "zmax" else 65, replace=False)] = 0
+    elif case == "shuffled":
+        mask[rng.choice(T, 30, replace=False)] = 0
+        order, m64 = O.shuffle_order(order, mask.astype(np.float64), 99)
+        mask = m64.astype(np.float32)
+    want = "temporal_kernel" if case == "zmax_plus1" else "temporal_sparse_kernel"
+    eng.compute_temporal(order, mask, full=True)
+    assert eng.last_temporal_kernel == want
+    g = eng.read_temporal_full()
+    M = eng.modes
+    D, Cm, P = O.analyze_modes(hist, order, mask.astype(np.float64), L, np.arange(M, dtype=np.int32),
+                               TPAD=eng.TPAD)
+    ok = P > 0
+    sc = P[ok].max()
+    assert np.abs(g["P"][ok] - P[ok]).max() / sc < 1e-5
+    assert np.abs(g["D"][ok] - D[ok]).max() / (2 * sc) < 1e-4
+    assert np.abs(g["C"][ok] - Cm[ok]).max() / sc < 1e-4
+    eng.compute_temporal(order, mask, full=False)
+    assert eng.last_temporal_kernel == want
+    rg = eng.read_radial()
+    ro = O.analyze_radial(hist, order, mask.astype(np.float64), O.make_bins(N, 16, 2, 30), L, TPAD=eng.TPAD)
     pscale = max(ro["P"].max(), 1e-30)
     assert np.abs(rg.D.reshape(-1, L) - ro["D"]).max() <= 1e-4 * 2 * pscale
     assert np.abs(rg.P - ro["P"]).max() <= 1e-5 * pscale
@@ -349,10 +400,12 @@ def test_radial_both_temporal_variants(variant):
     idx = np.nonzero(valid)[0]
     eng = _engine(N=N, T=T, L=L, NB=12, kmin=2, kmax=28)
     eng.set_tuning(0, 0, variant)
+    eng.set_sparse(False)  # 23 dropped frames would take the sparse-mask kernel
     assert eng.tuning["variant"] == variant
     eng.ingest_frames(frames[idx], idx)
     order, mask = O.linear_order(valid)
     eng.compute_temporal(order, mask)
+    assert eng.last_temporal_kernel == ("temporal_kernel", "temporal16_kernel")[variant]
     rg = eng.read_radial()
     hist = O.history_ingest(O.luma_of(frames[idx]), idx.astype(np.int32), T)
     ro = O.analyze_radial(hist, order, mask, O.make_bins(N, 12, 2, 28), L)

@@ -472,6 +472,7 @@ static int launch_chunk(ddm_engine *h, const void *dframes, int dtype, int n, co
   rp.err = h->d_err;
   CK(cudaMemsetAsync(h->d_framesum, 0, sizeof(double) * n, h->stream));
   CKL(launch_rows(N, dtype, rp, h->stream));
+  if (n > 0) h->launches++;  // launch_rows also runs cref_kernel (the frames' reference levels)
   ColParams cp{};
   cp.rows = h->d_rows;
   cp.framec = h->d_rowc;

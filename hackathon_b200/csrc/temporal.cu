@@ -837,13 +837,16 @@ __global__ void __launch_bounds__(NP / 8, TemporalBounds<NP>::MIN_BLOCKS)
   float2* stage = sm + 2 * PN;                     // [2 buffers][2 rows][TS]
   float2* s_tw = stage + 4 * TS;                   // per-stage twiddle blocks
   float2* s_pp = s_tw + tw_size(NP);               // [PADL + TS + PADL] (p_a, p_b)
-  float* s_np = (float*)(s_pp + TS + 2 * PADL);    // N(tau), tau < L
+  float* s_inp = (float*)(s_pp + TS + 2 * PADL);   // 1 / N(tau) (0 where N = 0), tau < L
   float2* pz = s_pp + PADL;                        // pz[j] = p at time index j
   const float invn = 0.5f / NP;
   for (int i = t; i < tw_size(NP); i += NT) s_tw[i] = p.tw[i];
   for (int i = t; i < TS + 2 * PADL; i += NT) s_pp[i] = make_float2(0.f, 0.f);
   const float np0 = vd.npairs[0];
-  for (int i = t; i < L; i += NT) s_np[i] = vd.npairs[i];
+  for (int i = t; i < L; i += NT) {
+    const float n = vd.npairs[i];
+    s_inp[i] = n > 0.5f ? 1.f / n : 0.f;
+  }
   uint32_t ord[4];
   float msk[4];
 #pragma unroll
@@ -1021,8 +1024,7 @@ __global__ void __launch_bounds__(NP / 8, TemporalBounds<NP>::MIN_BLOCKS)
           cr.y += lo.y + hi.y;
         }
         const double2 E0 = base_of(tau);
-        const float np = s_np[tau];
-        const float inv = np > 0.5f ? 1.f / np : 0.f;
+        const float inv = s_inp[tau];
 #pragma unroll
         for (int s = 0; s < 2; s++) {
           if (s == 1 && !hasb) break;
@@ -1069,14 +1071,12 @@ __global__ void __launch_bounds__(NP / 8, TemporalBounds<NP>::MIN_BLOCKS)
         for (int r = 0; r < LPT; r++) {
           const int tau = t + r * NT;
           if (tau < L) {
-            const float n0 = s_np[tau];
-            const float inp = n0 > 0.5f ? 1.f / n0 : 0.f;
+            const float inp = s_inp[tau];
             float gx, gy;
             G_of(s, tau, gx, gy);
             acc[r][0] += ((s ? E[r].y : E[r].x) - 2.0 * gx) * (double)inp;
             if (tau + 1 < L) {
-              const float n1 = s_np[tau + 1];
-              const float inp1 = n1 > 0.5f ? 1.f / n1 : 0.f;
+              const float inp1 = s_inp[tau + 1];
               float g1x, g1y;
               G_of(s, tau + 1, g1x, g1y);
               const float cx = gx * inp, cy = gy * inp;

@@ -511,6 +511,7 @@ def run_batch(args, rank, world, dist):
                 "config": {"workload": BATCH_WORKLOAD, "videos": nvid, "frames_per_step": total,
                            "sizes": {str(n): sum(v["N"] == n for v in vids) for n in (256, 384, 512, 768)},
                            "l2": "inputs larger than L2", "generation_s": t_gen,
+                           "temporal_kernel": engines[0].last_temporal_kernel,
                            "autotuned": {str(n): {k: t[k] for k in ("best_chunk", "best_unit", "best_variant")}
                                          for n, t in tuned.items()}},
                 "e2e": {"value": None, "unit": "frames/s",

@@ -732,8 +732,10 @@ static int check_device_error(ddm_engine *h) {
   if (e) {
     CK(cudaMemset(h->d_err, 0, sizeof(int)));
     h->radial_valid = h->full_valid = false;
-    return fail(h, DDM_ERR_CUDA,
-                "a staged copy did not complete in time (code %d: 1 temporal, 2 row, 3 column kernel)", e);
+    return fail(h, DDM_ERR_CUDA, "%s (code %d)",
+                e == 4 ? "the sparse-mask temporal kernel met more masked time indices than it holds"
+                       : "a staged copy did not complete in time (1 temporal, 2 row, 3 column kernel)",
+                e);
   }
   return DDM_OK;
 }
@@ -1114,6 +1116,16 @@ extern "C" int ddm_batch_enqueue_temporal(ddm_batch *b) {
   tp.tw = b->d_tw;
   tp.tw16 = b->d_tw16;
   tp.variant = b->e[0]->variant;
+  {  // every video's 0/1 mask within SPARSE_ZMAX zeros: the sparse-mask kernel
+    const float *hm = (const float *)(b->h_meta + sizeof(uint32_t) * nv * (size_t)b->Tmax);
+    bool sparse = b->e[0]->sparse_enabled && temporal_sparse_ok(b->TPAD);
+    for (int i = 0; sparse && i < nv; i++) {
+      int nz = 0;
+      for (int j = 0; j < b->e[i]->g.T; j++) nz += hm[(size_t)i * b->Tmax + j] == 0.f;
+      sparse = nz <= SPARSE_ZMAX;
+    }
+    tp.sparse = sparse ? 1 : 0;
+  }
   tp.units = b->d_units;
   tp.nunits = b->nunits;
   tp.unit_counter = b->d_counter;
@@ -1123,10 +1135,13 @@ extern "C" int ddm_batch_enqueue_temporal(ddm_batch *b) {
   tp.videos = b->d_videos;
   BCK(cudaMemsetAsync(b->d_counter, 0, sizeof(int), b->stream));
   if (b->nunits > 0) {
-    const int grid = std::min(temporal_max_grid(b->TPAD, b->Tmax, b->Lmax, false, tp.variant), b->nunits);
+    const int grid =
+        std::min(temporal_max_grid(b->TPAD, b->Tmax, b->Lmax, false, tp.variant, tp.sparse != 0), b->nunits);
     BCK(launch_temporal(b->TPAD, b->Lmax, false, tp, std::max(grid, 1), b->stream));
   }
+  const int tk = temporal_kernel_id(b->TPAD, false, tp.variant, tp.sparse != 0);
   for (ddm_engine *h : b->e) {
+    h->last_tk = tk;
     ReduceParams rp{};
     rp.partials = h->d_partials;
     rp.bin_units = h->d_bin_units;
@@ -1159,7 +1174,11 @@ extern "C" int ddm_batch_sync(ddm_batch *b) {
   }
   if (e) {
     cudaMemset(b->d_err, 0, sizeof(int));
-    return bfail(b, DDM_ERR_CUDA, "a staged copy did not complete in time (code %d)", e);
+    return bfail(b, DDM_ERR_CUDA, "%s (code %d)",
+                 e == 4 ? "a mask changed since the launch was recorded has more masked time indices than the "
+                          "sparse-mask kernel holds"
+                        : "a staged copy did not complete in time",
+                 e);
   }
   return DDM_OK;
 }

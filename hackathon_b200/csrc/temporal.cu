@@ -789,8 +789,8 @@ __global__ void __launch_bounds__(NP / 16, 1) temporal_big_kernel(TemporalParams
 }
 
 // ---------------------------------------------------------------------------
-// Sparse-mask variant (one video whose binary mask drops at most SPARSE_ZMAX
-// time indices, as in a recording with a few missing frames): A + B comes
+// Sparse-mask variant (videos whose binary masks drop at most SPARSE_ZMAX
+// time indices each, as recordings with a few missing frames): A + B comes
 // from the time domain instead of a transform. With p(t) = m(t)|x(t)|^2 (zero
 // at the masked t, and zero outside [0, T)) and S(n) = sum_{t<n} p(t),
 //   A(tau) = sum_t m(t+tau) p(t) = S(T - tau) - sum_{d in Z} p(d - tau)
@@ -800,7 +800,8 @@ __global__ void __launch_bounds__(NP / 16, 1) temporal_big_kernel(TemporalParams
 // share ONE inverse transform, of |Y_a|^2 + i |Y_b|^2 (both real, so
 // W = n (G_a + i G_b) splits by W(tau) +- conj W(-tau)): three transforms per
 // pair instead of five, 1.5 per mode. Same staging, unit scheduling and
-// epilogues as temporal_kernel.
+// epilogues as temporal_kernel; in batched launches a CTA reloads the video's
+// tables (zero list, 1/N(tau), order and mask) when its unit changes video.
 // Layout: p of the pair interleaved (p_a, p_b) in a zero-padded shared row
 // (PADL zeros either side, PADL >= every lag a thread touches), so each
 // correction term is one unconditional 8-byte load serving both modes and
@@ -830,10 +831,8 @@ __global__ void __launch_bounds__(NP / 8, TemporalBounds<NP>::MIN_BLOCKS)
   __shared__ int s_zero[SPARSE_ZMAX];
   __shared__ double s_wt[2][WARPS];
   const int t = threadIdx.x;
-  const int TS = p.T;                              // the video's T (single video)
-  const VideoDesc vd = video_of(p, 0);
-  const int L = vd.L, T = vd.T;
-  const int PADL = sparse_padl(NP, L, LPT);
+  const int TS = p.T;                              // staging stride: the (largest) T
+  const int PADL = sparse_padl(NP, p.L, LPT);      // p.L: the (largest) L
   float2* stage = sm + 2 * PN;                     // [2 buffers][2 rows][TS]
   float2* s_tw = stage + 4 * TS;                   // per-stage twiddle blocks
   float2* s_pp = s_tw + tw_size(NP);               // [PADL + TS + PADL] (p_a, p_b)
@@ -841,33 +840,55 @@ __global__ void __launch_bounds__(NP / 8, TemporalBounds<NP>::MIN_BLOCKS)
   float2* pz = s_pp + PADL;                        // pz[j] = p at time index j
   const float invn = 0.5f / NP;
   for (int i = t; i < tw_size(NP); i += NT) s_tw[i] = p.tw[i];
-  for (int i = t; i < TS + 2 * PADL; i += NT) s_pp[i] = make_float2(0.f, 0.f);
-  const float np0 = vd.npairs[0];
-  for (int i = t; i < L; i += NT) {
-    const float n = vd.npairs[i];
-    s_inp[i] = n > 0.5f ? 1.f / n : 0.f;
-  }
+
+  // per-video state: tables in shared memory, the slot and mask of this
+  // thread's samples, the masked time indices
+  const int4* v_items = nullptr;
+  double* v_partials = nullptr;
+  int cur_v = -1, L = 0, T = 0, v_unit0 = 0, v_nunits = 0, nz = 0;
+  float np0 = 0.f;
   uint32_t ord[4];
   float msk[4];
-#pragma unroll
-  for (int q = 0; q < 4; q++) {
-    const int i = t + q * NT;
-    ord[q] = i < T ? __ldg(&vd.order[i]) : 0u;
-    msk[q] = i < T ? __ldg(&vd.mask[i]) : 0.f;
-  }
-  if (t < 32) {  // the masked time indices, ascending (one warp, ballots)
-    int nz = 0;
-    for (int j0 = 0; j0 < T; j0 += 32) {
-      const bool z = j0 + t < T && __ldg(&vd.mask[j0 + t]) == 0.f;
-      const unsigned b = __ballot_sync(0xffffffffu, z);
-      if (z) {
-        const int at = nz + __popc(b & ((1u << t) - 1u));
-        if (at < SPARSE_ZMAX) s_zero[at] = j0 + t;
-      }
-      nz += __popc(b);
+  auto load_video = [&](int vi) {  // between two CTA barriers
+    const VideoDesc vd = video_of(p, vi);
+    cur_v = vi;
+    L = vd.L;
+    T = vd.T;
+    v_items = vd.items;
+    v_partials = vd.partials;
+    v_unit0 = vd.unit0;
+    v_nunits = vd.nunits;
+    np0 = vd.npairs[0];
+    for (int i = t; i < TS + 2 * PADL; i += NT) s_pp[i] = make_float2(0.f, 0.f);
+    for (int i = t; i < L; i += NT) {
+      const float n = vd.npairs[i];
+      s_inp[i] = n > 0.5f ? 1.f / n : 0.f;
     }
-    if (t == 0) s_nz = nz < SPARSE_ZMAX ? nz : SPARSE_ZMAX;
-  }
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int i = t + q * NT;
+      ord[q] = i < T ? __ldg(&vd.order[i]) : 0u;
+      msk[q] = i < T ? __ldg(&vd.mask[i]) : 0.f;
+    }
+    if (t < 32) {  // the masked time indices, ascending (one warp, ballots)
+      int n = 0;
+      for (int j0 = 0; j0 < T; j0 += 32) {
+        const bool z = j0 + t < T && __ldg(&vd.mask[j0 + t]) == 0.f;
+        const unsigned b = __ballot_sync(0xffffffffu, z);
+        if (z) {
+          const int at = n + __popc(b & ((1u << t) - 1u));
+          if (at < SPARSE_ZMAX) s_zero[at] = j0 + t;
+        }
+        n += __popc(b);
+      }
+      if (t == 0) {
+        // the host picks this kernel for masks within SPARSE_ZMAX zeros; a
+        // replayed launch whose tables changed since is reported, not run
+        if (n > SPARSE_ZMAX) atomicExch(p.err, 4);
+        s_nz = n > SPARSE_ZMAX ? -1 : n;
+      }
+    }
+  };
   if (t == 0) {
     mbar_init(&mbar[0], 1);
     mbar_init(&mbar[1], 1);
@@ -875,7 +896,6 @@ __global__ void __launch_bounds__(NP / 8, TemporalBounds<NP>::MIN_BLOCKS)
     s_next = atomicAdd(p.unit_counter, 1);
   }
   __syncthreads();
-  const int nz = s_nz;
   int u = s_next;
   __syncthreads();
   if (t == 0) {
@@ -895,6 +915,17 @@ __global__ void __launch_bounds__(NP / 8, TemporalBounds<NP>::MIN_BLOCKS)
 
   while (u < p.nunits) {
     const int4 U = p.units[u];
+    const int vi = p.videos ? U.w : 0;
+    if (vi != cur_v) {
+      __syncthreads();  // the previous video's shared tables are no longer read
+      load_video(vi);
+      __syncthreads();
+      nz = s_nz;
+      if (nz < 0) {  // more masked indices than the kernel holds: stop (reported)
+        if (t == 0) mbar_wait(&mbar[buf], (phase >> buf) & 1u, nullptr, 0);  // the copy in flight
+        return;
+      }
+    }
     int nu = u, nk = k + 2;
     if (nk >= U.y) {
       nu = unext;
@@ -910,8 +941,8 @@ __global__ void __launch_bounds__(NP / 8, TemporalBounds<NP>::MIN_BLOCKS)
     const float2* rowa = stage + buf * 2 * TS;
     const float2* rowb = rowa + TS;
     const bool hasb = k + 1 < U.y;
-    const int4 ea = load_item(vd.items, U.x + k);
-    const int4 eb = hasb ? load_item(vd.items, U.x + k + 1) : ea;
+    const int4 ea = load_item(v_items, U.x + k);
+    const int4 eb = hasb ? load_item(v_items, U.x + k + 1) : ea;
     float2 v[8];
     float pa[4], sa[8];
     // mode a: p_a(t) and Y_a = FFT(x_a); |Y_a|^2 kept in registers
@@ -1103,18 +1134,18 @@ __global__ void __launch_bounds__(NP / 8, TemporalBounds<NP>::MIN_BLOCKS)
     }
     if (k + 2 >= U.y) {
       if (!FULL) {
-        const int ul = u - vd.unit0;
+        const int ul = u - v_unit0;
 #pragma unroll
         for (int r = 0; r < LPT; r++) {
           const int tau = t + r * NT;
           if (tau < L)
 #pragma unroll
             for (int c = 0; c < PFIELDS; c++) {
-              vd.partials[((size_t)ul * PFIELDS + c) * L + tau] = acc[r][c];
+              v_partials[((size_t)ul * PFIELDS + c) * L + tau] = acc[r][c];
               acc[r][c] = 0.0;
             }
         }
-        if (t == 0) vd.partials[(size_t)vd.nunits * PFIELDS * L + ul] = accP;
+        if (t == 0) v_partials[(size_t)v_nunits * PFIELDS * L + ul] = accP;
         accP = 0.0;
       }
       u = unext;

@@ -119,3 +119,55 @@ def test_batch_small_video_against_oracle():
     batch.destroy()
     e1.destroy()
     e2.destroy()
+
+
+def test_batch_sparse_kernel_and_replay_guard():
+    """Every video's mask within 64 zeros: the batched launch takes the
+    sparse-mask kernel (per-video zero lists), equal to the transform path;
+    a recorded launch replayed after a mask grew past 64 zeros reports the
+    error instead of a wrong record."""
+    vids = _make(seed=31)
+    rng = np.random.default_rng(5)
+    orders = [np.arange(v["geo"][1], dtype=np.uint32) for v in vids]
+    masks = []
+    for v in vids:
+        m = np.ones(v["geo"][1], np.float32)
+        m[rng.choice(v["geo"][1], 25, replace=False)] = 0
+        masks.append(m)
+    slots = [np.arange(v["geo"][1], dtype=np.int32) for v in vids]
+    scales = [1.0 / 65535] * len(vids)
+    engines = [_engine(v["geo"]) for v in vids]
+    batch = DdmBatch(engines)
+    batch.ingest([v["frames"] for v in vids], slots, scales)
+    batch.compute_temporal(orders, masks)
+    sparse = batch.read_radials()
+    assert all(e.last_temporal_kernel == "temporal_sparse_kernel" for e in engines)
+    engines[0].set_sparse(False)  # the batch follows its first engine's setting
+    batch.compute_temporal(orders, masks)
+    dense = batch.read_radials()
+    assert all(e.last_temporal_kernel in ("temporal_kernel", "temporal16_kernel") for e in engines)
+    engines[0].set_sparse(True)
+    for a, b in zip(sparse, dense):
+        _close(a, b)
+    # record the step with the sparse kernel, then refresh the tables with a
+    # mask of 100 zeros (the direct launch takes the transform path) and replay
+    batch.compute_temporal(orders, masks)
+    batch.capture([v["frames"] for v in vids], slots, scales)
+    batch.launch_graph()
+    rep = batch.read_radials()
+    for a, b in zip(rep, sparse):
+        _close(a, b)
+    many = [m.copy() for m in masks]
+    many[0][:100] = 0
+    batch.compute_temporal(orders, many)
+    batch.sync()
+    assert engines[0].last_temporal_kernel != "temporal_sparse_kernel"
+    batch.launch_graph()
+    with pytest.raises(H.DdmError, match="sparse-mask kernel"):
+        batch.sync()
+    batch.compute_temporal(orders, masks)  # usable again
+    for a, b in zip(batch.read_radials(), sparse):
+        _close(a, b)
+    batch.destroy()
+    for e in engines:
+        e.destroy()

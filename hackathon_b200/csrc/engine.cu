@@ -663,7 +663,7 @@ static int temporal_impl(ddm_engine *h, const uint32_t *order, const float *mask
       nz += mask[j] == 0.f;
       binary = binary && (mask[j] == 0.f || mask[j] == 1.f);
     }
-    tp.sparse = h->sparse_enabled && binary && nz <= SPARSE_ZMAX && temporal_sparse_ok(TPAD) ? 1 : 0;
+    tp.sparse = h->sparse_enabled && binary && nz <= temporal_sparse_limit(TPAD, T, L, full) ? 1 : 0;
   }
   h->last_tk = temporal_kernel_id(TPAD, full, h->variant, tp.sparse != 0);
   tp.unit_counter = h->d_counter;
@@ -1118,11 +1118,12 @@ extern "C" int ddm_batch_enqueue_temporal(ddm_batch *b) {
   tp.variant = b->e[0]->variant;
   {  // every video's 0/1 mask within SPARSE_ZMAX zeros: the sparse-mask kernel
     const float *hm = (const float *)(b->h_meta + sizeof(uint32_t) * nv * (size_t)b->Tmax);
-    bool sparse = b->e[0]->sparse_enabled && temporal_sparse_ok(b->TPAD);
+    const int limit = temporal_sparse_limit(b->TPAD, b->Tmax, b->Lmax, false);
+    bool sparse = b->e[0]->sparse_enabled && limit > 0;
     for (int i = 0; sparse && i < nv; i++) {
       int nz = 0;
       for (int j = 0; j < b->e[i]->g.T; j++) nz += hm[(size_t)i * b->Tmax + j] == 0.f;
-      sparse = nz <= SPARSE_ZMAX;
+      sparse = nz <= limit;
     }
     tp.sparse = sparse ? 1 : 0;
   }

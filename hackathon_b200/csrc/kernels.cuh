@@ -78,6 +78,7 @@ struct TemporalParams {
 };
 
 constexpr int SPARSE_ZMAX = 64;  // masked time indices the sparse temporal kernel takes
+constexpr int SPARSE_ZMAX_BIG = 256;  // ... and its TPAD 8192 variant (zero-list capacity)
 
 struct ReduceParams {
   const double* partials;
@@ -135,6 +136,8 @@ int temporal_max_grid(int TPAD, int T, int L, bool full, int variant = 0, bool s
 bool temporal_has_variant16(int TPAD);
 // TPAD sizes the sparse-mask temporal kernel serves
 bool temporal_sparse_ok(int TPAD);
+// most masked time indices the sparse path takes for this geometry (0: none)
+int temporal_sparse_limit(int TPAD, int T, int L, bool full);
 // which temporal kernel launch_temporal runs for these settings (DDM_TK_*)
 int temporal_kernel_id(int TPAD, bool full, int variant, bool sparse);
 cudaError_t launch_reduce(const ReduceParams& p, cudaStream_t s);

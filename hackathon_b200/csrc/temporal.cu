@@ -1161,6 +1161,370 @@ __global__ void __launch_bounds__(NP / 8, TemporalBounds<NP>::MIN_BLOCKS)
   }
 }
 
+// ---------------------------------------------------------------------------
+// Sparse-mask variant of temporal_big_kernel (TPAD 8192; same A + B from
+// prefix sums and shared inverse transform as temporal_sparse_kernel). One
+// group of TPAD/16 = 512 threads, 16 points per thread, in-place radix-16
+// transforms in ONE 64 KB buffer:
+//   Y_a = FFT(x_a) (|Y_a|^2 kept in registers); Y_b = FFT(x_b);
+//   W = IFFT(|Y_a|^2 + i |Y_b|^2)
+// -- three transforms per pair instead of five. The whole scan S does not
+// fit beside the 64 KB staged pair, so only the values the lags use are
+// kept: S(n) for n <= L (head) and n >= T - L (tail). Up to
+// SPARSE_ZMAX_BIG masked indices (the host also bounds zeros x lags per
+// thread, the corrections' cost).
+__host__ __device__ constexpr int sparse_padl_big(int NP, int L, int LPT) {
+  return ((L > LPT * (NP / 16) ? L : LPT * (NP / 16)) + 1) & ~1;
+}
+
+template <int NP, int LPT, bool FULL>
+__global__ void __launch_bounds__(NP / 16, 1) temporal_sparse_big_kernel(TemporalParams p) {
+  constexpr int NTH = NP / 16;
+  constexpr int WARPS = NTH / 32;
+  extern __shared__ __align__(16) float2 sm[];
+  float2* bufF = sm;
+  __shared__ __align__(8) uint64_t mbar;
+  __shared__ int s_next, s_nz;
+  __shared__ int s_zero[SPARSE_ZMAX_BIG];
+  __shared__ double s_wt[2][WARPS];
+  const int t = threadIdx.x;
+  const float invn = 0.5f / NP;
+  const float2* __restrict__ tw = p.tw16;
+  const int TS = p.T;                              // staging stride: the (largest) T
+  const int LM = p.L;                              // the (largest) L
+  const int PADL = sparse_padl_big(NP, LM, LPT);
+  float2* stage = sm + NP;                         // [2 rows][TS]
+  float2* s_pp = stage + 2 * TS;                   // [PADL + TS + PADL] (p_a, p_b)
+  float2* pz = s_pp + PADL;
+  double2* Sh = reinterpret_cast<double2*>(s_pp + TS + 2 * PADL);  // S(n), n <= L
+  double2* St = Sh + (LM + 1);                                     // S(T - L + m), m <= L
+  float* s_inp = reinterpret_cast<float*>(St + (LM + 1));          // 1 / N(tau)
+
+  const int4* v_items = nullptr;
+  double* v_partials = nullptr;
+  int cur_v = -1, L = 0, T = 0, v_unit0 = 0, v_nunits = 0, nz = 0;
+  float np0 = 0.f;
+  int om[8];  // slot of each of this thread's samples, -1 where masked or beyond T
+  auto load_video = [&](int vi) {  // between two CTA barriers
+    const VideoDesc vd = video_of(p, vi);
+    cur_v = vi;
+    L = vd.L;
+    T = vd.T;
+    v_items = vd.items;
+    v_partials = vd.partials;
+    v_unit0 = vd.unit0;
+    v_nunits = vd.nunits;
+    np0 = vd.npairs[0];
+    for (int i = t; i < TS + 2 * PADL; i += NTH) s_pp[i] = make_float2(0.f, 0.f);
+    for (int i = t; i < L; i += NTH) {
+      const float n = vd.npairs[i];
+      s_inp[i] = n > 0.5f ? 1.f / n : 0.f;
+    }
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      const int i = t + q * NTH;
+      om[q] = (i < T && __ldg(&vd.mask[i]) != 0.f) ? (int)__ldg(&vd.order[i]) : -1;
+    }
+    if (t < 32) {  // the masked time indices, ascending (one warp, ballots)
+      int n = 0;
+      for (int j0 = 0; j0 < T; j0 += 32) {
+        const bool z = j0 + t < T && __ldg(&vd.mask[j0 + t]) == 0.f;
+        const unsigned b = __ballot_sync(0xffffffffu, z);
+        if (z) {
+          const int at = n + __popc(b & ((1u << t) - 1u));
+          if (at < SPARSE_ZMAX_BIG) s_zero[at] = j0 + t;
+        }
+        n += __popc(b);
+      }
+      if (t == 0) {
+        if (n > SPARSE_ZMAX_BIG) atomicExch(p.err, 4);  // see temporal_sparse_kernel
+        s_nz = n > SPARSE_ZMAX_BIG ? -1 : n;
+      }
+    }
+  };
+  if (t == 0) {
+    mbar_init(&mbar, 1);
+    fence_barrier_init();
+    s_next = atomicAdd(p.unit_counter, 1);
+  }
+  __syncthreads();
+  int u = s_next;
+  __syncthreads();
+  if (t == 0) {
+    s_next = atomicAdd(p.unit_counter, 1);
+    if (u < p.nunits) issue_pair(p, u, 0, stage, TS, &mbar);
+  }
+  __syncthreads();
+  int unext = s_next;
+  uint32_t phase = 0;
+  int k = 0;
+  double acc[LPT][PFIELDS];
+  double accP = 0.0;
+#pragma unroll
+  for (int r = 0; r < LPT; r++)
+#pragma unroll
+    for (int c = 0; c < PFIELDS; c++) acc[r][c] = 0.0;
+
+  while (u < p.nunits) {
+    const int4 U = p.units[u];
+    const int vi = p.videos ? U.w : 0;
+    if (vi != cur_v) {
+      __syncthreads();
+      load_video(vi);
+      __syncthreads();
+      nz = s_nz;
+      if (nz < 0) {  // more masked indices than the kernel holds: stop (reported)
+        if (t == 0) mbar_wait(&mbar, phase, nullptr, 0);  // the copy in flight
+        return;
+      }
+    }
+    if (!mbar_wait(&mbar, phase, p.err, 1)) return;  // nothing else is in flight
+    phase ^= 1u;
+    const bool hasb = k + 1 < U.y;
+    const int4 ea = load_item(v_items, U.x + k);
+    const int4 eb = hasb ? load_item(v_items, U.x + k + 1) : ea;
+    const float2* rowa = stage;
+    const float2* rowb = stage + TS;
+    float2 v[16];
+    float sa[16];
+    float* pzf = reinterpret_cast<float*>(pz);  // p_a at 2j, p_b at 2j + 1
+    // mode a: p_a straight to shared memory (registers are short here) and
+    // Y_a; |Y_a|^2 kept in registers
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      v[q] = om[q] >= 0 ? rowa[om[q]] : make_float2(0.f, 0.f);
+      const int j = t + q * NTH;
+      if (j < T) pzf[2 * j] = fmaf(v[q].x, v[q].x, v[q].y * v[q].y);
+    }
+#pragma unroll
+    for (int q = 8; q < 16; q++) v[q] = make_float2(0.f, 0.f);
+    fft16<NP, false>(v, t, bufF, tw, 0);  // ends with a barrier after its last store
+#pragma unroll
+    for (int q = 0; q < 16; q++) {
+      const float2 y = bufF[pad16(t + q * NTH)];
+      sa[q] = fmaf(y.x, y.x, y.y * y.y);
+    }
+    // mode b: the pair's last gather, then the stage takes the next pair
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      v[q] = hasb && om[q] >= 0 ? rowb[om[q]] : make_float2(0.f, 0.f);
+      const int j = t + q * NTH;
+      if (j < T) pzf[2 * j + 1] = fmaf(v[q].x, v[q].x, v[q].y * v[q].y);
+    }
+#pragma unroll
+    for (int q = 8; q < 16; q++) v[q] = make_float2(0.f, 0.f);
+    fence_proxy_async_smem();
+    __syncthreads();
+    {
+      int nu = u, nk = k + 2;
+      if (nk >= U.y) {
+        nu = unext;
+        nk = 0;
+      }
+      if (t == 0 && nu < p.nunits) issue_pair(p, nu, nk, stage, TS, &mbar);
+    }
+    // the first store of each transform waits for the group: the reads of
+    // the buffer before it are done by then
+    fft16<NP, false>(v, t, bufF, tw, 0);
+#pragma unroll
+    for (int q = 0; q < 16; q++) {
+      const float2 y = bufF[pad16(t + q * NTH)];
+      v[q] = make_float2(sa[q], fmaf(y.x, y.x, y.y * y.y));
+    }
+    fft16<NP, true>(v, t, bufF, tw, 0);
+    const float2* W = bufF;
+    // S(n) of both modes at the head (n <= L) and tail (n >= T - L): thread
+    // t sums time indices 8t..8t+7, warps scan, warp totals combine
+    {
+      // pass 1: this thread's sums; pass 2 (threads whose indices reach the
+      // head or the tail) re-reads its 8 values to write the S(n) kept
+      double ra = 0.0, rb = 0.0;
+#pragma unroll
+      for (int h = 0; h < 4; h++) {
+        const float4 q = 8 * t + 2 * h < T ? reinterpret_cast<const float4*>(pz)[4 * t + h]
+                                           : make_float4(0.f, 0.f, 0.f, 0.f);
+        ra += (double)q.x;
+        rb += (double)q.y;
+        ra += (double)q.z;
+        rb += (double)q.w;
+      }
+      double ta = ra, tb = rb;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const double ya = __shfl_up_sync(0xffffffffu, ta, o);
+        const double yb = __shfl_up_sync(0xffffffffu, tb, o);
+        if ((t & 31) >= o) {
+          ta += ya;
+          tb += yb;
+        }
+      }
+      if ((t & 31) == 31) {
+        s_wt[0][t >> 5] = ta;
+        s_wt[1][t >> 5] = tb;
+      }
+      __syncthreads();
+      if (8 * t + 1 <= L || 8 * t + 8 >= T - L) {
+        double ba = ta - ra, bb = tb - rb;  // exclusive prefix of this thread's indices
+        for (int w = 0; w < (t >> 5); w++) {
+          ba += s_wt[0][w];
+          bb += s_wt[1][w];
+        }
+#pragma unroll
+        for (int e = 0; e < 8; e++) {
+          const int j = 8 * t + e;  // S(j + 1) = S(j) + p(j)
+          if (j < T) {
+            const float2 pv = pz[j];
+            ba += (double)pv.x;
+            bb += (double)pv.y;
+            const int n = j + 1;
+            const double2 sv = make_double2(ba, bb);
+            if (n <= L) Sh[n] = sv;
+            if (n >= T - L) St[n - (T - L)] = sv;
+          }
+        }
+      }
+      if (t == 0) {
+        Sh[0] = make_double2(0.0, 0.0);
+        if (T == L) St[0] = make_double2(0.0, 0.0);
+      }
+      __syncthreads();
+    }
+    const double2 ST = St[L];
+    auto base_of = [&](int tau) {  // S(T) - S(tau) + S(T - tau), tau < L
+      const double2 s1 = Sh[tau], s2 = St[L - tau];
+      return make_double2(ST.x - s1.x + s2.x, ST.y - s1.y + s2.y);
+    };
+    auto G_of = [&](int s, int tau, float& gx, float& gy) {
+      const float2 w0 = W[pad16(tau)];
+      const float2 w1 = W[pad16((NP - tau) & (NP - 1))];
+      if (s == 0) {
+        gx = (w0.x + w1.x) * invn;
+        gy = (w0.y - w1.y) * invn;
+      } else {
+        gx = (w0.y + w1.y) * invn;
+        gy = (w1.x - w0.x) * invn;
+      }
+    };
+    if (FULL) {
+      for (int tau = t; tau < L; tau += NTH) {
+        float2 cr = make_float2(0.f, 0.f);
+#pragma unroll 4
+        for (int z = 0; z < nz; z++) {
+          const int d = s_zero[z];
+          const float2 lo = pz[d - tau], hi = pz[d + tau];
+          cr.x += lo.x + hi.x;
+          cr.y += lo.y + hi.y;
+        }
+        const double2 E0 = base_of(tau);
+        const float inv = s_inp[tau];
+#pragma unroll
+        for (int s = 0; s < 2; s++) {
+          if (s == 1 && !hasb) break;
+          const size_t mode = (size_t)(s ? eb : ea).x;
+          const double E = s ? E0.y - (double)cr.y : E0.x - (double)cr.x;
+          float gx, gy;
+          G_of(s, tau, gx, gy);
+          p.outD[mode * L + tau] = (float)((E - 2.0 * gx) * inv);
+          p.outC[mode * L + tau] = make_float2(gx * inv, gy * inv);
+        }
+      }
+      if (t == 0) {
+        p.outP[(size_t)ea.x] = np0 > 0.5f ? (float)(ST.x / np0) : 0.f;
+        if (hasb) p.outP[(size_t)eb.x] = np0 > 0.5f ? (float)(ST.y / np0) : 0.f;
+      }
+    } else {
+      double2 E[LPT];
+#pragma unroll
+      for (int r = 0; r < LPT; r++) E[r] = make_double2(0.0, 0.0);
+      if (t < L) {  // threads without a lag skip the corrections
+        float2 cr[LPT];
+#pragma unroll
+        for (int r = 0; r < LPT; r++) cr[r] = make_float2(0.f, 0.f);
+#pragma unroll 2
+        for (int z = 0; z < nz; z++) {
+          const int d = s_zero[z];
+          const float2* lo = pz + (d - t);
+          const float2* hi = pz + (d + t);
+#pragma unroll
+          for (int r = 0; r < LPT; r++) {
+            const float2 a = lo[-r * NTH], b = hi[r * NTH];
+            cr[r].x += a.x + b.x;
+            cr[r].y += a.y + b.y;
+          }
+        }
+#pragma unroll
+        for (int r = 0; r < LPT; r++) {
+          const int tau = t + r * NTH;
+          const double2 E0 = base_of(tau < L ? tau : 0);
+          E[r] = make_double2(E0.x - (double)cr[r].x, E0.y - (double)cr[r].y);
+        }
+      }
+#pragma unroll 1
+      for (int s = 0; s < 2; s++) {
+        if (s == 1 && !hasb) break;
+        const int4 e = s ? eb : ea;
+        const double kx = e.y, ky = e.z;
+#pragma unroll
+        for (int r = 0; r < LPT; r++) {
+          const int tau = t + r * NTH;
+          if (tau < L) {
+            const float inp = s_inp[tau];
+            float gx, gy;
+            G_of(s, tau, gx, gy);
+            acc[r][0] += ((s ? E[r].y : E[r].x) - 2.0 * gx) * (double)inp;
+            if (tau + 1 < L) {
+              const float inp1 = s_inp[tau + 1];
+              float g1x, g1y;
+              G_of(s, tau + 1, g1x, g1y);
+              const float cx = gx * inp, cy = gy * inp;
+              const float c1x = g1x * inp1, c1y = g1y * inp1;
+              const float zr = fmaf(c1x, cx, c1y * cy);  // C(tau+1) conj C(tau)
+              const float zi = fmaf(c1y, cx, -c1x * cy);
+              const float w = sqrtf(fmaf(zr, zr, zi * zi));
+              if (w > 0.f) {
+                const double wd = w, ph = atan2f(zi, zr);
+                acc[r][1] += wd;
+                acc[r][2] += wd * kx * kx;
+                acc[r][3] += wd * kx * ky;
+                acc[r][4] += wd * ky * ky;
+                acc[r][5] += wd * kx * ph;
+                acc[r][6] += wd * ky * ph;
+                acc[r][7] += wd * ph * ph;
+                acc[r][8] += 1.0;
+              }
+            }
+          }
+        }
+        accP += np0 > 0.5f ? (double)(float)((s ? ST.y : ST.x) / np0) : 0.0;
+      }
+    }
+    if (k + 2 >= U.y) {
+      if (!FULL) {
+        const int ul = u - v_unit0;
+#pragma unroll
+        for (int r = 0; r < LPT; r++) {
+          const int tau = t + r * NTH;
+          if (tau < L)
+#pragma unroll
+            for (int c = 0; c < PFIELDS; c++) {
+              v_partials[((size_t)ul * PFIELDS + c) * L + tau] = acc[r][c];
+              acc[r][c] = 0.0;
+            }
+        }
+        if (t == 0) v_partials[(size_t)v_nunits * PFIELDS * L + ul] = accP;
+        accP = 0.0;
+      }
+      u = unext;
+      k = 0;
+      if (t == 0) s_next = atomicAdd(p.unit_counter, 1);
+    } else {
+      k += 2;
+    }
+    __syncthreads();  // the epilogue is done with W, S and pz; s_next is complete
+    unext = s_next;
+  }
+}
+
 // Sums the unit partials of each bin in unit order (deterministic), divides
 // D and P by the bin's mode count (ddm_ref.js:404-412) and writes the
 // reference's Radial layout: D[b*L+tau], P[b], drift[(b*L+tau)*8+c].
@@ -1271,6 +1635,12 @@ static size_t temporal_big_smem(int T, int L) {
   return sizeof(float2) * (2 * (size_t)NP + 2 * (size_t)T) + sizeof(float) * (size_t)L;
 }
 
+template <int NP>
+static size_t temporal_sparse_big_smem(int T, int L, int LPT) {
+  return sizeof(float2) * ((size_t)NP + 3 * (size_t)T + 2 * (size_t)sparse_padl_big(NP, L, LPT)) +
+         sizeof(double2) * 2 * ((size_t)L + 1) + sizeof(float) * (size_t)L;
+}
+
 // lags per thread of the big kernel (NP/16 threads)
 static int lpt_big(int TPAD, int L) {
   const int NTH = TPAD / 16;
@@ -1291,6 +1661,13 @@ static size_t temporal_sparse_smem(int T, int L, int LPT) {
 template <int NP, int LPT, bool FULL>
 static cudaError_t launch_k(const TemporalParams& p, int grid, cudaStream_t s) {
   if constexpr (use_big(NP)) {
+    if (p.sparse) {
+      auto k = temporal_sparse_big_kernel<NP, LPT, FULL>;
+      const size_t sm = temporal_sparse_big_smem<NP>(p.T, p.L, LPT);
+      cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+      k<<<grid, NP / 16, sm, s>>>(p);
+      return cudaGetLastError();
+    }
     auto k = temporal_big_kernel<NP, LPT, FULL>;
     const size_t sm = temporal_big_smem<NP>(p.T, p.L);
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
@@ -1336,6 +1713,9 @@ static int occupancy_grid(K k, int threads, size_t smem) {
 template <int NP, int LPT, bool FULL>
 static int grid_of(int T, int L, int variant, bool sparse) {
   if constexpr (use_big(NP)) {
+    if (sparse)
+      return occupancy_grid(temporal_sparse_big_kernel<NP, LPT, FULL>, NP / 16,
+                            temporal_sparse_big_smem<NP>(T, L, LPT));
     return occupancy_grid(temporal_big_kernel<NP, LPT, FULL>, NP / 16, temporal_big_smem<NP>(T, L));
   } else {
     if constexpr (sparse_ok(NP))
@@ -1410,10 +1790,19 @@ int temporal_max_grid(int TPAD, int T, int L, bool full, int variant, bool spars
 
 bool temporal_has_variant16(int TPAD) { return use16(TPAD, false); }
 
-bool temporal_sparse_ok(int TPAD) { return sparse_ok(TPAD); }
+bool temporal_sparse_ok(int TPAD) { return sparse_ok(TPAD) || use_big(TPAD); }
+
+int temporal_sparse_limit(int TPAD, int T, int L, bool full) {
+  if (sparse_ok(TPAD)) return SPARSE_ZMAX;
+  if (TPAD != 8192) return 0;
+  // the corrections cost zeros x lags per thread: bound their product
+  const int lpt = full ? 1 : lpt_big(TPAD, L);
+  if (temporal_sparse_big_smem<8192>(T, L, lpt) > 225 * 1024) return 0;  // with the static tables
+  return SPARSE_ZMAX_BIG / lpt;
+}
 
 int temporal_kernel_id(int TPAD, bool full, int variant, bool sparse) {
-  if (use_big(TPAD)) return DDM_TK_BIG;
+  if (use_big(TPAD)) return sparse ? DDM_TK_SPARSE_BIG : DDM_TK_BIG;
   if (sparse && sparse_ok(TPAD)) return DDM_TK_SPARSE;
   if (use16(TPAD, full) && variant == 1) return DDM_TK_RADIX16;
   return DDM_TK_RADIX8;

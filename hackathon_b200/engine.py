@@ -257,7 +257,7 @@ class DdmEngine:
         self._check(self._lib.ddm_set_sparse(self._h, 1 if enable else 0))
 
     TEMPORAL_KERNELS = {0: "temporal_kernel", 1: "temporal16_kernel", 2: "temporal_sparse_kernel",
-                        3: "temporal_big_kernel"}
+                        3: "temporal_big_kernel", 4: "temporal_sparse_big_kernel"}
 
     @property
     def last_temporal_kernel(self):

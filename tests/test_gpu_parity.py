@@ -432,6 +432,10 @@ def test_temporal_tpad8192(N, L, NB, kmax):
     order, mask = O.linear_order(valid)
     order, mask = O.shuffle_order(order, mask, 7) if L > 2048 else (order, mask)
     eng.compute_temporal(order, mask)
+    # 81 dropped frames: the sparse-mask kernel at 128 lags; at 2100 lags the
+    # corrections would cost more than the transforms they replace
+    want = "temporal_sparse_big_kernel" if L <= 512 else "temporal_big_kernel"
+    assert eng.last_temporal_kernel == want
     rg = eng.read_radial()
     hist = O.history_ingest(O.luma_of(frames[idx]), idx.astype(np.int32), T)
     bins = O.make_bins(N, NB, 2, kmax)
@@ -442,8 +446,18 @@ def test_temporal_tpad8192(N, L, NB, kmax):
         if sc > 0:
             assert np.abs(D[b] - ro["D"][b]).max() <= 1e-4 * sc, b
     assert np.allclose(rg.P, ro["P"], rtol=1e-5, atol=0)
+    if want == "temporal_sparse_big_kernel":  # the transform kernel on the same analysis
+        eng.set_sparse(False)
+        eng.compute_temporal(order, mask)
+        assert eng.last_temporal_kernel == "temporal_big_kernel"
+        D2 = eng.read_radial().D2()
+        eng.set_sparse(True)
+        for b in range(NB):
+            sc = np.abs(D2[b]).max()
+            assert np.abs(D[b] - D2[b]).max() <= 1e-5 * sc, b
     if L <= 2048:
         eng.compute_temporal(order, mask, full=True)
+        assert eng.last_temporal_kernel == want
         g = eng.read_temporal_full()
         modes = np.unique(bins["binModes"][:, 0])[::7].astype(np.int32)
         Do, Co, Po = O.analyze_modes(hist, order, mask, L, modes)

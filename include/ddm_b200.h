@@ -168,12 +168,15 @@ int ddm_set_stream(ddm_engine *h, void *stream);
  * before ingesting and before ddm_batch_create over the engine. `report`
  * (may be NULL) receives a JSON summary of every candidate's time. */
 int ddm_autotune(ddm_engine *h, char *report, int32_t report_len);
-/* The temporal pass of an analysis whose mask drops at most 64 time indices
+/* The temporal pass of an analysis whose 0/1 mask drops few time indices
  * (a recording with a few missing frames) computes A + B of the masked
- * Wiener-Khinchin formula from exact FP64 prefix sums and the masked set
- * instead of two transforms, and pairs the modes' |Y|^2 in one inverse
- * transform: 1.5 transforms per mode instead of 2.5 (TPAD 256..4096, single
- * engine). enable = 0 keeps the transform path for every mask. Default 1. */
+ * Wiener-Khinchin formula from FP64 prefix sums and the masked set instead
+ * of two transforms, and pairs the modes' |Y|^2 in one inverse transform:
+ * 1.5 transforms per mode instead of 2.5. "Few": at most 64 zeros for TPAD
+ * 256..4096; at TPAD 8192, 256 divided by the lags per thread (L/512 rounded
+ * up to 1, 2, 4 or 8) while the tables fit shared memory. A batch takes it
+ * when every video qualifies and its first engine has it enabled. enable = 0
+ * keeps the transform path for every mask. Default 1. */
 int ddm_set_sparse(ddm_engine *h, int32_t enable);
 /* The temporal kernel of the engine's last computeTemporal: DDM_TK_RADIX8
  * (one-group radix-8 transforms), DDM_TK_RADIX16 (two-group radix-16),

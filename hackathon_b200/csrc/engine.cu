@@ -1308,9 +1308,25 @@ extern "C" int ddm_autotune(ddm_engine *h, char *report, int32_t report_len) {
   int best_u = h->unit_size, best_var = h->variant;
   float best_tu = 1e30f;
   bool first = true;
+  // the transform kernels (masks with many zeros) pick the variant and, when
+  // the sparse path is off, the unit; an all-ones mask then times the
+  // sparse-mask kernel, whose best unit wins when it is on (the common case:
+  // a recording with few dropped frames)
+  const bool sparse_was = h->sparse_enabled;
+  const bool sparse_on = sparse_was && temporal_sparse_limit(h->g.TPAD, T, h->g.L, false) > 0;
+  h->sparse_enabled = false;
   const int nvar = temporal_has_variant16(h->g.TPAD) ? 2 : 1;
-  for (int cand = 0; cand < 6 * nvar && !rc; cand++) {
-    const int U = 8 << (cand % 6), var = cand / 6;
+  const int ncand = 6 * nvar + (sparse_on ? 6 : 0);
+  int best_su = 0;
+  float best_ts = 1e30f;
+  for (int cand = 0; cand < ncand && !rc; cand++) {
+    const bool sp = cand >= 6 * nvar;
+    const int U = 8 << (cand % 6), var = sp ? best_var : cand / 6;
+    if (sp && cand == 6 * nvar) {
+      h->sparse_enabled = true;
+      rep += "}, \"sparse_unit\": {";
+      first = true;
+    }
     h->variant = var;
     if ((rc = build_units(h, U))) break;
     float t[3];
@@ -1327,12 +1343,18 @@ extern "C" int ddm_autotune(ddm_engine *h, char *report, int32_t report_len) {
     if (rc) break;
     const float ms = med3(t[0], t[1], t[2]);
     char b[64];
-    snprintf(b, sizeof b, "%s\"%s%d\": %.4f", first ? "" : ", ", var ? "r16:" : "", U, ms);
+    snprintf(b, sizeof b, "%s\"%s%d\": %.4f", first ? "" : ", ", !sp && var ? "r16:" : "", U, ms);
     rep += b;
     first = false;
-    if (ms < best_tu) best_tu = ms, best_u = U, best_var = var;
+    if (sp) {
+      if (ms < best_ts) best_ts = ms, best_su = U;
+    } else if (ms < best_tu) {
+      best_tu = ms, best_u = U, best_var = var;
+    }
   }
+  h->sparse_enabled = sparse_was;
   h->variant = best_var;
+  if (best_su > 0) best_u = best_su, best_tu = best_ts;
   if (!rc) rc = build_units(h, best_u);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);

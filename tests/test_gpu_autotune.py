@@ -1,5 +1,6 @@
 """The autotuner (ddm_autotune) picks its spatial chunk, temporal unit size
-and temporal kernel variant from timed candidates, and the tuned engine
+(on the sparse-mask kernel when that path is on) and temporal kernel variant
+(on the transform kernels) from timed candidates, and the tuned engine
 computes the same radial record as an untuned one (unit size regroups FP64
 partial sums, the variant changes the FFT plan's FP32 rounding: agreement to
 1e-5 of each bin's scale, the FP32 transforms' accuracy)."""
@@ -31,6 +32,9 @@ def test_autotune_report_and_results_unchanged():
             assert key in rep["temporal_unit"] and t["unit_size"] == rep["best_unit"]
             assert t["variant"] == rep["best_variant"]
             assert any(k.startswith("r16:") for k in rep["temporal_unit"])  # TPAD 1024 has both variants
+            # the sparse-mask kernel's sweep picks the unit (the path this mask takes)
+            su = rep["sparse_unit"]
+            assert su[str(t["unit_size"])] == min(su.values())
             assert min(rep["spatial_chunk"].values()) == pytest.approx(rep["us_per_frame"], rel=1e-3)
         e.ingest_frames(frames, slots, 1 / 65535)
         e.compute_temporal(order, mask)

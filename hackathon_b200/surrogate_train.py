@@ -240,12 +240,27 @@ def compare_fits(net, data, bnds, max_iter=200, tol=1e-10, nrefine=3):
     for name in ("seeded", "fallback"):
         r = res[name]
         equal = r["cost"] <= p["cost"] * (1 + 1e-3) + 1e-30
+        ratio = r["cost"] / np.maximum(p["cost"], 1e-300)
         summary.update({f"{name}_qfits_per_s": r["qfits_per_s"],
                         f"{name}_speedup": r["qfits_per_s"] / p["qfits_per_s"],
                         f"{name}_mean_iters": float(r["iters"].mean()),
                         f"{name}_mean_evals": float(r["evals"].mean()),
                         f"{name}_frac_equal_or_better": float(equal.mean()),
+                        f"{name}_cost_ratio_p50_p90_p99": [float(np.quantile(ratio, q)) for q in (0.5, 0.9, 0.99)],
                         f"{name}_frac_fallback": float(((r["status"] >> 1) & 1).mean())})
+    # fit error against the curves' labels (the generator's parameters for
+    # analytic and "truth"-labelled pipeline curves): D (every curve) and
+    # vbar (curves whose label has a motile fraction >= 0.2)
+    lab = np.asarray(data["theta"], np.float64)
+    motile = lab[:, 2] >= 0.2
+    for name in ("plain", "seeded", "fallback"):
+        th = res[name]["theta"]
+        eD = np.abs(np.exp(th[:, 5]) / lab[:, 5] - 1)
+        ev = np.abs(np.exp(th[:, 3]) / lab[:, 3] - 1)[motile]
+        summary.update({f"{name}_D_relerr_p50": float(np.median(eD)),
+                        f"{name}_frac_D_within_10pct": float((eD <= 0.1).mean()),
+                        f"{name}_vbar_relerr_p50": float(np.median(ev)) if ev.size else None,
+                        f"{name}_frac_vbar_within_10pct": float((ev <= 0.1).mean()) if ev.size else None})
     return summary, res
 
 

@@ -671,6 +671,8 @@ def main():
     # take videos in turn (a user with a stream of videos): while one
     # video's temporal analysis runs, the next video's frames already cross
     # PCIe into the other engine; every video's radial record is read back.
+    # (Two host threads, one per engine, measured slower: 45 GB/s over the
+    # link against 50.5 GB/s, the two engines' copies then overlapping.)
     host = frames.view(torch.int16).cpu().pin_memory()
     rad_bytes = 8 * (NB * L + NB + NB * L * 8)
     eng.set_stream(stream.cuda_stream)
@@ -708,6 +710,17 @@ def main():
     eng2.destroy()
     ms_e2e = R.max_over_ranks(ms_e2e, dist, device="cuda")
     e2e = R.weak_scaling_throughput(T * args.e2e_steps, ms_e2e, world)
+    # the link's ceiling for context: one plain pinned host->device copy of a video
+    dev_copy = torch.empty_like(host, device="cuda")
+    c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    dev_copy.copy_(host, non_blocking=True)
+    torch.cuda.synchronize()
+    c0.record(stream)
+    dev_copy.copy_(host, non_blocking=True)
+    c1.record(stream)
+    torch.cuda.synchronize()
+    h2d_gbps = host.numel() * 2 / (c0.elapsed_time(c1) * 1e6)
+    del dev_copy
 
     # ---------------- roofline of the dominant stage
     peak, peak_kind = _peaks()
@@ -764,6 +777,8 @@ def main():
                            "autotuned": {"chunk": tune["best_chunk"], "unit": tune["best_unit"],
                                          "temporal_variant": tune["best_variant"]}},
                 "e2e": {"value": e2e, "unit": "frames/s", "pipeline": "two engines take videos in turn",
+                        "h2d_GBps": host.numel() * 2 * args.e2e_steps / (ms_e2e * 1e6),
+                        "h2d_GBps_plain_copy": h2d_gbps,
                         "h2d_bytes_per_step": int(host.numel() * 2),
                         "d2h_bytes_per_step": rad_bytes},
                 "gpu_launches": int(launches),

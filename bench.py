@@ -743,6 +743,50 @@ def main():
     stages["spatial"]["gflop"] = fl_sp / 1e9
     stages["temporal"]["gflop"] = fl_tm / 1e9
     stages["temporal"]["kernel"] = tk
+    # a library reference point for the temporal stage's transform work:
+    # cuFFT (torch.fft) running just the same number of TPAD-point complex
+    # transforms over device-resident series (one forward per mode from T
+    # samples, plus the inverse transforms: one per mode pair for the
+    # sparse-mask kernel, 1.5 per mode for the transform kernels), with none
+    # of the masked Wiener-Khinchin arithmetic or the radial epilogue
+    lib = None
+    try:
+        x = torch.randn((nbinned, T), dtype=torch.complex64, device="cuda")
+        n_inv = nbinned // 2 if tk == "temporal_sparse_kernel" else (3 * nbinned) // 2
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        times = []
+        for r in range(4):
+            torch.cuda.synchronize()
+            f0.record()
+            y = torch.fft.fft(x, n=TPAD, dim=1)
+            z = torch.fft.ifft(y[:n_inv] if n_inv <= nbinned else torch.cat([y, y[:n_inv - nbinned]]), dim=1)
+            f1.record()
+            torch.cuda.synchronize()
+            if r:
+                times.append(f0.elapsed_time(f1))
+            del y, z
+        lib = {"temporal": {"what": f"torch.fft (cuFFT): {nbinned} forward + {n_inv} inverse {TPAD}-point C2C "
+                                    "transforms, device-resident, no other work",
+                            "ms": statistics.median(times)}}
+        del x
+        # and the spatial stage's: a 2D real-to-half-plane FFT of every frame
+        # already in FP32 (no conversion, window, mean or transposed store)
+        x = torch.randn((T, N, N), dtype=torch.float32, device="cuda")
+        times = []
+        for r in range(4):
+            torch.cuda.synchronize()
+            f0.record()
+            y = torch.fft.rfft2(x)
+            f1.record()
+            torch.cuda.synchronize()
+            if r:
+                times.append(f0.elapsed_time(f1))
+            del y
+        lib["spatial"] = {"what": f"torch.fft.rfft2 (cuFFT) of {T} FP32 {N}x{N} frames, device-resident, no other work",
+                          "ms": statistics.median(times)}
+        del x
+    except RuntimeError as e:  # e.g. out of memory on a shared device
+        lib = {"unavailable": str(e)[:120]}
     # dominant kernel: the temporal kernel (one launch per step, the largest
     # single kernel; the spatial stage is 3 kernels x 16 chunk launches)
     traffic = _profile_traffic() or {}
@@ -753,6 +797,7 @@ def main():
             "algorithmic_bytes": tm["bytes"],
             "timed_span": f"temporal stage on the engine stream: meta upload + {tk} + reduce_kernel",
             "fp32_tflops": tm["gflop"] / tm["ms"], "fp32_frac_of_nominal": tm["gflop"] / tm["ms"] / FP32_NOMINAL_TFLOPS,
+            "library_fft_reference": lib,
             "pipeline_GBps": (sp_bytes + tm_bytes) / (ms_step * 1e6),
             "pipeline_frac": (sp_bytes + tm_bytes) / (ms_step * 1e6) / peak,
             "stages": stages}

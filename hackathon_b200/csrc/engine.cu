@@ -1116,7 +1116,7 @@ extern "C" int ddm_batch_enqueue_temporal(ddm_batch *b) {
   tp.tw = b->d_tw;
   tp.tw16 = b->d_tw16;
   tp.variant = b->e[0]->variant;
-  {  // every video's 0/1 mask within SPARSE_ZMAX zeros: the sparse-mask kernel
+  {  // every video's (binarised) mask within the sparse path's zero limit: the sparse-mask kernel
     const float *hm = (const float *)(b->h_meta + sizeof(uint32_t) * nv * (size_t)b->Tmax);
     const int limit = temporal_sparse_limit(b->TPAD, b->Tmax, b->Lmax, false);
     bool sparse = b->e[0]->sparse_enabled && limit > 0;

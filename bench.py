@@ -671,8 +671,10 @@ def main():
     # take videos in turn (a user with a stream of videos): while one
     # video's temporal analysis runs, the next video's frames already cross
     # PCIe into the other engine; every video's radial record is read back.
-    # (Two host threads, one per engine, measured slower: 45 GB/s over the
-    # link against 50.5 GB/s, the two engines' copies then overlapping.)
+    # (Measured alternatives, no faster: two host threads, one per engine;
+    # ddm_ingest_frames_async with the host's set-up overlapping the copies;
+    # four staging buffers instead of two. The link carries ~50 GB/s here
+    # against ~55 GB/s for one plain pinned copy.)
     host = frames.view(torch.int16).cpu().pin_memory()
     rad_bytes = 8 * (NB * L + NB + NB * L * 8)
     eng.set_stream(stream.cuda_stream)

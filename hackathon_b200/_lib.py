@@ -69,6 +69,8 @@ _SIGS = {
     "ddm_ingest_luma": (C.c_int, [_vp, _vp, _i32, C.POINTER(_i32)]),
     "ddm_ingest_frames": (C.c_int, [_vp, _vp, _i32, _i32, _vp, C.c_float]),
     "ddm_ingest_frames_device": (C.c_int, [_vp, _vp, _i32, _i32, _vp, C.c_float]),
+    "ddm_ingest_frames_async": (C.c_int, [_vp, _vp, _i32, _i32, _vp, C.c_float]),
+    "ddm_ingest_wait": (C.c_int, [_vp]),
     "ddm_set_spatial_mask": (C.c_int, [_vp, _vp]),
     "ddm_compute_temporal": (C.c_int, [_vp, _vp, _vp, _i32]),
     "ddm_compute_temporal_async": (C.c_int, [_vp, _vp, _vp, _i32]),

@@ -134,11 +134,13 @@ static void release(ddm_engine *h) {
   if (h->ana_stream) cudaStreamSynchronize(h->ana_stream);
   void *dev[] = {h->d_hist, h->d_rows, h->d_rowc, h->d_framesum, h->d_means, h->d_win, h->d_wys, h->d_ninv,
                  h->d_invtot, h->d_tw_s, h->d_tw_t, h->d_tw_t16, h->d_wcorr4, h->d_wcorr_full, h->d_smask,
-                 h->d_stage[0], h->d_stage[1], h->d_order, h->d_mask, h->d_npairs,
+                 h->d_order, h->d_mask, h->d_npairs,
                  h->d_mspec, h->d_items, h->d_units, h->d_bin_units, h->d_offsets, h->d_nmodes,
                  h->d_units_full, h->d_counter, h->d_err, h->d_partials, h->d_radD, h->d_radP,
                  h->d_radDrift, h->d_fullD, h->d_fullP, h->d_fullC};
   for (void *p : dev)
+    if (p) cudaFree(p);
+  for (void *p : h->d_stage)
     if (p) cudaFree(p);
   if (h->h_meta) cudaFreeHost(h->h_meta);
   for (int i = 0; i < NSTAGE; i++) {
@@ -373,13 +375,13 @@ extern "C" int ddm_create(const ddm_geometry *geometry, ddm_engine **out) {
       (rc = dalloc(h, &h->d_invtot, 1)) || (rc = dalloc(h, &h->d_tw_s, N)) ||
       (rc = dalloc(h, &h->d_tw_t, g.TPAD)) || (rc = dalloc(h, &h->d_tw_t16, g.TPAD)) ||
       (rc = dalloc(h, &h->d_wcorr4, 4)) ||
-      (rc = dalloc(h, (char **)&h->d_stage[0], h->stage_bytes)) ||
-      (rc = dalloc(h, (char **)&h->d_stage[1], h->stage_bytes)) ||
       (rc = dalloc(h, &h->d_order, g.T)) || (rc = dalloc(h, &h->d_mask, g.T)) ||
       (rc = dalloc(h, &h->d_npairs, g.L)) || (rc = dalloc(h, &h->d_mspec, g.TPAD)) ||
       (rc = dalloc(h, &h->d_radD, (size_t)g.NB * g.L)) || (rc = dalloc(h, &h->d_radP, g.NB)) ||
       (rc = dalloc(h, &h->d_radDrift, (size_t)g.NB * g.L * DRIFT)))
     return bail(rc);
+  for (void *&p : h->d_stage)
+    if ((rc = dalloc(h, (char **)&p, h->stage_bytes))) return bail(rc);
   h->meta_bytes = sizeof(uint32_t) * g.T + sizeof(float) * g.T + sizeof(float) * g.L +
                   sizeof(float2) * g.TPAD;
   if (cudaHostAlloc((void **)&h->h_meta, h->meta_bytes, cudaHostAllocDefault) != cudaSuccess) {
@@ -532,7 +534,7 @@ static void note_inflight(ddm_engine *h) {
 static int dtype_size(int dtype) { return dtype == 0 ? 1 : dtype == 1 ? 2 : 4; }
 
 static int ingest_impl(ddm_engine *h, const void *frames, int dtype, int n, const int32_t *slots,
-                       float scale, bool device) {
+                       float scale, bool device, bool wait_copies = true) {
   cudaSetDevice(h->device);
   int rc = check_frames_args(h, frames, dtype, n, slots);
   if (rc) return rc;
@@ -559,8 +561,9 @@ static int ingest_impl(ddm_engine *h, const void *frames, int dtype, int n, cons
     if ((rc = launch_chunk(h, src, dtype, m, slots + c0, scale))) return rc;
     if (!device) CK(cudaEventRecord(h->free_ev[ci % NSTAGE], h->stream));
   }
-  // the caller's host buffer is free once the copies have run
-  CK(cudaStreamSynchronize(h->copy_stream));
+  // the caller's host buffer is free once the copies have run (the async
+  // entry point leaves that wait to ddm_ingest_wait)
+  if (wait_copies) CK(cudaStreamSynchronize(h->copy_stream));
   note_inflight(h);
   if (!h->radial_from_live) h->radial_valid = false;  // a live snapshot stays readable
   return DDM_OK;
@@ -576,6 +579,19 @@ extern "C" int ddm_ingest_frames_device(ddm_engine *h, const void *frames, int32
                                         const int32_t *slots, float scale) {
   if (!h) return DDM_ERR_ARG;
   return ingest_impl(h, frames, dtype, n, slots, scale, true);
+}
+
+extern "C" int ddm_ingest_frames_async(ddm_engine *h, const void *frames, int32_t dtype, int32_t n,
+                                       const int32_t *slots, float scale) {
+  if (!h) return DDM_ERR_ARG;
+  return ingest_impl(h, frames, dtype, n, slots, scale, false, false);
+}
+
+extern "C" int ddm_ingest_wait(ddm_engine *h) {
+  if (!h) return DDM_ERR_ARG;
+  cudaSetDevice(h->device);
+  CK(cudaStreamSynchronize(h->copy_stream));
+  return DDM_OK;
 }
 
 static int prune_inflight(ddm_engine *h) {

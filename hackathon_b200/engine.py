@@ -59,6 +59,7 @@ class DdmEngine:
         self.modes = self.N * self.NH
         self.bins = self._read_bins()
         self._destroyed = False
+        self._pending_host = []  # host buffers of asynchronous ingests still being copied
 
     # ------------------------------------------------------------ lifetime
     @classmethod
@@ -80,7 +81,8 @@ class DdmEngine:
         """DdmEngine.destroy (ddm-engine.ts:421-425)."""
         if not self._destroyed:
             self._destroyed = True
-            self._lib.ddm_destroy(self._h)
+            self._lib.ddm_destroy(self._h)  # waits for the copies in flight
+            self._pending_host.clear()
 
     def __enter__(self):
         return self
@@ -142,10 +144,13 @@ class DdmEngine:
         self._check(self._lib.ddm_ingest_luma(self._h, _ptr(a), int(slot), C.byref(ok)))
         return bool(ok.value)
 
-    def ingest_frames(self, frames, slots, scale=None):
+    def ingest_frames(self, frames, slots, scale=None, wait=True):
         """Raw frames [n, N, N] (numpy, or torch CPU/CUDA tensor) into ring slots
         `slots[i] % T`. luma = value * scale; scale defaults to 1/255 for u8
-        (lumaOf, test/sim.mjs:189-193), 1/65535 for u16 and 1 for f32."""
+        (lumaOf, test/sim.mjs:189-193), 1/65535 for u16 and 1 for f32.
+        wait=False (host frames): return once the copies are queued
+        (ddm_ingest_frames_async); the engine keeps a reference to the host
+        buffer until ingest_wait() -- do not change it before then."""
         self._alive()
         slots = np.ascontiguousarray(slots, dtype=np.int32).reshape(-1)
         dev_ptr = None
@@ -187,11 +192,23 @@ class DdmEngine:
         if dev_ptr is not None:
             rc = self._lib.ddm_ingest_frames_device(self._h, C.c_void_p(dev_ptr), code, n, _ptr(slots),
                                                     float(scale))
+        elif not wait:
+            rc = self._lib.ddm_ingest_frames_async(self._h, C.c_void_p(host_ptr), code, n, _ptr(slots),
+                                                   float(scale))
+            self._pending_host.append(keep)
         else:
             rc = self._lib.ddm_ingest_frames(self._h, C.c_void_p(host_ptr), code, n, _ptr(slots),
                                              float(scale))
+            self._pending_host.clear()  # the synchronous ingest waited for every earlier copy
         del keep
         self._check(rc)
+
+    def ingest_wait(self):
+        """Wait until every earlier ingest's frames are off the host buffers
+        (ddm_ingest_wait)."""
+        self._alive()
+        self._check(self._lib.ddm_ingest_wait(self._h))
+        self._pending_host.clear()
 
     def set_spatial_mask(self, mask):
         """Extension: N x N ROI mask (nonzero = used), or None."""
@@ -311,6 +328,7 @@ class DdmEngine:
     def idle(self):
         """idle (ddm-engine.ts:417-419)."""
         self._check(self._lib.ddm_idle(self._h))
+        self._pending_host.clear()
 
     # ------------------------------------------------------------ plumbing
     def set_stream(self, stream_ptr):

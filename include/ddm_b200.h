@@ -102,6 +102,18 @@ int ddm_ingest_frames(ddm_engine *h, const void *frames, int32_t dtype,
  * buffer must stay valid until it runs. */
 int ddm_ingest_frames_device(ddm_engine *h, const void *frames, int32_t dtype,
                              int32_t n, const int32_t *slots, float scale);
+/* ddm_ingest_frames without the final wait (no counterpart in the reference,
+ * whose writeBuffer copies at call time): returns once the copies and
+ * transforms are queued, so a host with a stream of videos keeps the PCIe
+ * link busy while it prepares the next call. The host buffer must stay
+ * unchanged until ddm_ingest_wait returns (or a later synchronous ingest,
+ * ddm_idle or ddm_destroy). Pinned memory is needed for the copies to be
+ * asynchronous at all. */
+int ddm_ingest_frames_async(ddm_engine *h, const void *frames, int32_t dtype,
+                            int32_t n, const int32_t *slots, float scale);
+/* Waits until the frames of every earlier ingest have been copied off the
+ * caller's buffers. */
+int ddm_ingest_wait(ddm_engine *h);
 
 /* Spatial ROI mask (extension; the reference has none): N*N bytes, 1 = pixel
  * used. Masked pixels are excluded from the frame mean and zeroed before the

@@ -289,13 +289,25 @@ class DdmEngine:
         self._check(self._lib.ddm_get_tuning(self._h, C.byref(c), C.byref(u), C.byref(v)))
         return dict(chunk=c.value, unit_size=u.value, variant=v.value)
 
-    def read_radial(self):
-        """readRadial (ddm-engine.ts:391-395) -> Radial (ddm_ref.js:336-348)."""
+    def read_radial(self, out=None):
+        """readRadial (ddm-engine.ts:391-395) -> Radial (ddm_ref.js:336-348).
+        out: optional (D, P, drift) float64 arrays of NB*L, NB and NB*L*8
+        values that receive the record (the Radial returned uses them), e.g.
+        pinned host memory reused across videos: the copy back then runs at
+        the link's rate instead of through the driver's pageable path."""
         self._alive()
         NB, L = self.NB, self.L
-        D = np.empty(NB * L)
-        P = np.empty(NB)
-        drift = np.empty(NB * L * 8)
+        if out is None:
+            D = np.empty(NB * L)
+            P = np.empty(NB)
+            drift = np.empty(NB * L * 8)
+        else:
+            D, P, drift = out
+            for a, n in ((D, NB * L), (P, NB), (drift, NB * L * 8)):
+                if not (isinstance(a, np.ndarray) and a.dtype == np.float64 and a.size == n
+                        and a.flags.c_contiguous and a.flags.writeable):
+                    raise DdmArgError(_lib.DDM_ERR_ARG, f"read_radial out: need writable contiguous float64 "
+                                                        f"arrays of {NB * L}, {NB}, {NB * L * 8} values")
         self._check(self._lib.ddm_read_radial(self._h, _ptr(D), _ptr(P), _ptr(drift)))
         b = self.bins
         return Radial(N=self.N, NB=NB, L=L, kCenter=b["kCenter"].copy(), kNodes=b["kNodes"].copy(),

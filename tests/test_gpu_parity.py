@@ -498,7 +498,7 @@ def test_radial_mixed_radix_size():
 def test_async_ingest_matches_sync():
     """ddm_ingest_frames_async (copies queued, no wait) then the analysis:
     the same radial record, bit for bit, as the synchronous ingest; pinned
-    and pageable host buffers alike."""
+    and pageable host buffers alike; read_radial into caller-owned buffers."""
     import torch
     N, T, L = 64, 128, 40
     rng = np.random.default_rng(3)
@@ -517,6 +517,12 @@ def test_async_ingest_matches_sync():
         r = e.read_radial()
         e.ingest_wait()
         out.append((r.D.copy(), r.P.copy(), r.drift.copy()))
+        # the same record into caller-owned (pinned) buffers
+        bufs = [torch.empty(k, dtype=torch.float64).pin_memory().numpy() for k in (12 * L, 12, 12 * L * 8)]
+        r2 = e.read_radial(out=bufs)
+        assert r2.D is bufs[0] and np.array_equal(r2.D, r.D) and np.array_equal(r2.drift, r.drift)
+        with pytest.raises(H.DdmArgError):
+            e.read_radial(out=[np.empty(3), bufs[1], bufs[2]])
         e.destroy()
     for o in out[1:]:
         for a, b in zip(out[0], o):

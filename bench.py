@@ -564,7 +564,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--e2e-steps", type=int, default=6)
+    ap.add_argument("--e2e-steps", type=int, default=12)
     ap.add_argument("--no-fit", action="store_true", help="skip the q-fits/s (surrogate + LM) section")
     ap.add_argument("--tuning", default="", help="chunk,unit[,variant]: apply instead of autotuning")
     ap.add_argument("--workload", default="config2", choices=["config2", "large", "batch", "surrogate"],

@@ -32,6 +32,7 @@ struct ddm_engine {
   int NH = 0, NHB = 0, modes = 0, chunk = 0, chunk_cap = 0, unit_size = 0, variant = 0;
   bool sparse_enabled = true;  // the sparse-mask temporal kernel for masks with few zeros
   int last_tk = -1;             // DDM_TK_* of the last temporal launch
+  std::vector<float> meta_mask, meta_npairs, meta_mspec;  // temporal_meta of the last mask
   int device = 0;
   std::string err;
   int64_t launches = 0, throttled = 0;
@@ -644,8 +645,13 @@ static int temporal_impl(ddm_engine *h, const uint32_t *order, const float *mask
   if (!order || !mask) return fail(h, DDM_ERR_ARG, "computeTemporal: order/mask must have length %d", T);
   for (int j = 0; j < T; j++)
     if (order[j] >= (uint32_t)T) return fail(h, DDM_ERR_ARG, "order[%d] = %u is not a slot < %d", j, order[j], T);
-  std::vector<float> npairs, mspec;
-  temporal_meta(mask, T, TPAD, L, npairs, mspec);
+  // N(tau) and the mask spectrum depend on the mask alone: reused while the
+  // mask is the previous analysis' (a stream of videos with the same drops)
+  if (h->meta_mask.size() != (size_t)T || memcmp(h->meta_mask.data(), mask, sizeof(float) * T) != 0) {
+    temporal_meta(mask, T, TPAD, L, h->meta_npairs, h->meta_mspec);
+    h->meta_mask.assign(mask, mask + T);
+  }
+  const std::vector<float> &npairs = h->meta_npairs, &mspec = h->meta_mspec;
   // the pinned staging may still be read by the previous analysis' copies
   CK(cudaEventSynchronize(h->meta_ev));
   char *p = h->h_meta;

@@ -50,7 +50,8 @@ struct ddm_engine {
   BinTable bins;
   float2 *d_hist = nullptr;            // [modes][T]
   float2 *d_rows = nullptr;            // [chunk][NHB][KB][N]
-  float *d_rowc = nullptr;             // [chunk] frame reference levels c_f
+  float *d_rowc = nullptr;             // [rowc_cap] frame reference levels c_f
+  size_t rowc_cap = 0;                 // c_f slots: a chunk's, or a whole device ingest's up to this
   double *d_framesum = nullptr;        // [chunk] pixel sums
   double *d_means = nullptr;           // [chunk]
   float *d_win = nullptr, *d_wys = nullptr;
@@ -367,9 +368,10 @@ extern "C" int ddm_create(const ddm_geometry *geometry, ddm_engine **out) {
   cudaEventCreateWithFlags(&h->ingest_ev, cudaEventDisableTiming);
   const int N = g.N;
   h->stage_bytes = (size_t)h->chunk_cap * N * N * sizeof(float);
+  h->rowc_cap = std::max<size_t>((size_t)h->chunk_cap * N, (size_t)g.T);
   if ((rc = dalloc(h, &h->d_hist, (size_t)h->modes * g.T)) ||
       (rc = dalloc(h, &h->d_rows, (size_t)h->chunk_cap * h->NHB * N * KB)) ||
-      (rc = dalloc(h, &h->d_rowc, (size_t)h->chunk_cap * N)) ||
+      (rc = dalloc(h, &h->d_rowc, h->rowc_cap)) ||
       (rc = dalloc(h, &h->d_framesum, (size_t)h->chunk_cap)) ||
       (rc = dalloc(h, &h->d_means, (size_t)h->chunk_cap)) || (rc = dalloc(h, &h->d_win, N)) ||
       (rc = dalloc(h, &h->d_wys, N)) || (rc = dalloc(h, &h->d_ninv, N)) ||
@@ -457,8 +459,10 @@ extern "C" int ddm_set_stream(ddm_engine *h, void *stream) {
 extern "C" int64_t ddm_kernel_launches(const ddm_engine *h) { return h ? h->launches : 0; }
 
 // Rows + columns for one chunk of frames already in device memory.
+// framec: the chunk's c_f already computed for the whole call (device frames),
+// or nullptr: cref_kernel runs with the rows kernel for this chunk
 static int launch_chunk(ddm_engine *h, const void *dframes, int dtype, int n, const int32_t *slots,
-                        float scale) {
+                        float scale, float *framec = nullptr) {
   const int N = h->g.N;
   // w(y) * scale for this call's scale
   RowParams rp{};
@@ -470,15 +474,16 @@ static int launch_chunk(ddm_engine *h, const void *dframes, int dtype, int n, co
   rp.smask = h->d_smask;
   rp.tw = h->d_tw_s;
   rp.rows = h->d_rows;
-  rp.framec = h->d_rowc;
+  rp.framec = framec ? framec : h->d_rowc;
+  rp.framec_ready = framec != nullptr;
   rp.framesum = h->d_framesum;
   rp.err = h->d_err;
   CK(cudaMemsetAsync(h->d_framesum, 0, sizeof(double) * n, h->stream));
   CKL(launch_rows(N, dtype, rp, h->stream));
-  if (n > 0) h->launches++;  // launch_rows also runs cref_kernel (the frames' reference levels)
+  if (n > 0 && !framec) h->launches++;  // launch_rows also ran cref_kernel (the frames' reference levels)
   ColParams cp{};
   cp.rows = h->d_rows;
-  cp.framec = h->d_rowc;
+  cp.framec = rp.framec;
   cp.framesum = h->d_framesum;
   cp.inv_total = h->d_invtot;
   cp.w2d = h->d_smask ? h->d_wcorr_full : nullptr;
@@ -544,6 +549,10 @@ static int ingest_impl(ddm_engine *h, const void *frames, int dtype, int n, cons
   if ((rc = set_scale(h, scale))) return rc;
   const int N = h->g.N;
   const size_t fbytes = (size_t)N * N * dtype_size(dtype);
+  // device frames: every frame's reference level in one launch ahead of the
+  // chunks (host frames arrive chunk by chunk: per chunk with the rows kernel)
+  const bool cref_all = device && n > 0 && (size_t)n <= h->rowc_cap;
+  if (cref_all) CKL(launch_cref(N, dtype, frames, (long long)N * N, n, h->d_rowc, h->stream));
   for (int c0 = 0, ci = 0; c0 < n; c0 += h->chunk, ci++) {
     const int m = std::min(h->chunk, n - c0);
     const void *src;
@@ -559,7 +568,7 @@ static int ingest_impl(ddm_engine *h, const void *frames, int dtype, int n, cons
       CK(cudaStreamWaitEvent(h->stream, h->ready_ev[s], 0));
       src = h->d_stage[s];
     }
-    if ((rc = launch_chunk(h, src, dtype, m, slots + c0, scale))) return rc;
+    if ((rc = launch_chunk(h, src, dtype, m, slots + c0, scale, cref_all ? h->d_rowc + c0 : nullptr))) return rc;
     if (!device) CK(cudaEventRecord(h->free_ev[ci % NSTAGE], h->stream));
   }
   // the caller's host buffer is free once the copies have run (the async

@@ -23,6 +23,7 @@ struct RowParams {
   float* framec;           // [nframes] frame reference level c_f (raw units, out)
   double* framesum;        // [nframes] masked pixel sums (zeroed before launch)
   int* err;                // error word (bounded waits that timed out), or nullptr
+  int framec_ready;        // 1: framec already holds these frames' c_f (launch_cref ran for the call)
 };
 
 struct ColParams {
@@ -126,6 +127,10 @@ struct LmParams {
 // launchers (return cudaGetLastError())
 cudaError_t launch_rows(int N, int dtype, const RowParams& p, cudaStream_t s);
 cudaError_t launch_cols(int N, const ColParams& p, cudaStream_t s);
+// the frames' reference levels c_f of nframes device frames (cref_kernel),
+// for a whole ingest call at once
+cudaError_t launch_cref(int N, int dtype, const void* frames, long long frame_stride, int nframes, float* framec,
+                        cudaStream_t s);
 // frames handled by one column-kernel CTA (one per FFT group); ingest chunks
 // are multiples of it
 int frames_per_col_cta(int N);

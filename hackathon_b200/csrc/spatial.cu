@@ -592,7 +592,8 @@ static cudaError_t rows_n(const RowParams& p, cudaStream_t s) {
   auto k = rows_kernel<N, Tin>;
   const size_t sm = fft_smem<N>() + N * sizeof(float) + (size_t)ROW_STAGES * 2 * G * N * (sizeof(Tin) + 1);
   const int grid = persistent_grid(k, G * (N / pts(N)), sm, (npairs + G - 1) / G);
-  if (p.nframes > 0) cref_kernel<N, Tin><<<p.nframes, CREF, 0, s>>>((const Tin*)p.frames, p.frame_stride, p.framec);
+  if (p.nframes > 0 && !p.framec_ready)
+    cref_kernel<N, Tin><<<p.nframes, CREF, 0, s>>>((const Tin*)p.frames, p.frame_stride, p.framec);
   k<<<grid, G * (N / pts(N)), sm, s>>>(p);
   return cudaGetLastError();
 }
@@ -603,6 +604,33 @@ static cudaError_t rows_dt(int dtype, const RowParams& p, cudaStream_t s) {
     case 0: return rows_n<N, uint8_t>(p, s);
     case 1: return rows_n<N, uint16_t>(p, s);
     case 2: return rows_n<N, float>(p, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+template <int N>
+static cudaError_t cref_n(int dtype, const void* frames, long long stride, int n, float* framec, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  switch (dtype) {
+    case 0: cref_kernel<N, uint8_t><<<n, CREF, 0, s>>>((const uint8_t*)frames, stride, framec); break;
+    case 1: cref_kernel<N, uint16_t><<<n, CREF, 0, s>>>((const uint16_t*)frames, stride, framec); break;
+    case 2: cref_kernel<N, float><<<n, CREF, 0, s>>>((const float*)frames, stride, framec); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_cref(int N, int dtype, const void* frames, long long stride, int n, float* framec,
+                        cudaStream_t s) {
+  switch (N) {
+    case 64: return cref_n<64>(dtype, frames, stride, n, framec, s);
+    case 128: return cref_n<128>(dtype, frames, stride, n, framec, s);
+    case 256: return cref_n<256>(dtype, frames, stride, n, framec, s);
+    case 384: return cref_n<384>(dtype, frames, stride, n, framec, s);
+    case 512: return cref_n<512>(dtype, frames, stride, n, framec, s);
+    case 768: return cref_n<768>(dtype, frames, stride, n, framec, s);
+    case 1024: return cref_n<1024>(dtype, frames, stride, n, framec, s);
+    case 2048: return cref_n<2048>(dtype, frames, stride, n, framec, s);
     default: return cudaErrorInvalidValue;
   }
 }

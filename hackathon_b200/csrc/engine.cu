@@ -1087,9 +1087,18 @@ extern "C" int ddm_batch_ingest(ddm_batch *b, const void *const *frames, const i
     cudaStream_t keep = h->stream;
     h->stream = b->stream;
     const size_t fbytes = (size_t)h->g.N * h->g.N * dtype_size(dtypes[i]);
+    // the video's frame reference levels in one launch (as ingest_impl)
+    const bool cref_all = n[i] > 0 && (size_t)n[i] <= h->rowc_cap;
+    if (cref_all) {
+      const cudaError_t e = launch_cref(h->g.N, dtypes[i], frames[i], (long long)h->g.N * h->g.N, n[i], h->d_rowc,
+                                        h->stream);
+      h->launches++;
+      if (e != cudaSuccess) rc = fail(h, DDM_ERR_CUDA, "launch_cref failed: %s", cudaGetErrorString(e));
+    }
     for (int c0 = 0; c0 < n[i] && !rc; c0 += h->chunk) {
       const int m = std::min(h->chunk, n[i] - c0);
-      rc = launch_chunk(h, (const char *)frames[i] + (size_t)c0 * fbytes, dtypes[i], m, slots[i] + c0, scales[i]);
+      rc = launch_chunk(h, (const char *)frames[i] + (size_t)c0 * fbytes, dtypes[i], m, slots[i] + c0, scales[i],
+                        cref_all ? h->d_rowc + c0 : nullptr);
     }
     h->stream = keep;
     if (rc) return bfail(b, rc, "video %zu: %s", i, h->err.c_str());

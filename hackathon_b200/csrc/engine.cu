@@ -334,15 +334,18 @@ extern "C" int ddm_create(const ddm_geometry *geometry, ddm_engine **out) {
   h->modes = g.N * h->NH;
   {
     const size_t per = (size_t)h->NHB * g.N * KB * sizeof(float2);
-    const size_t target = 32u << 20;  // rows scratch stays L2-resident
+    // default chunk: ~128 MB of row spectra (at 512^2 x 1024 the autotuner's
+    // choice is larger still: fewer launches and persistent-grid tails
+    // outweigh the scratch no longer fitting L2)
+    const size_t target = 128u << 20;
     const int fg = frames_per_col_cta(g.N);
     size_t c = std::max<size_t>(1, target / per);
     c = std::min<size_t>(MAX_CHUNK, std::max<size_t>(c, fg));
     h->chunk = (int)(c / fg * fg);  // whole column-kernel frame groups
     // buffers hold up to chunk_cap frames, so the autotuner may pick larger
     // chunks (at N >= 1024 one frame's scratch is 4 MB or more and a chunk
-    // of four, the column kernel's tile, already passes the L2 target)
-    const size_t cap_bytes = g.N >= 1024 ? (288u << 20) : (96u << 20);
+    // of four, the column kernel's tile, is already 17 MB)
+    const size_t cap_bytes = g.N >= 1024 ? (288u << 20) : (256u << 20);
     h->chunk_cap = std::max(h->chunk, std::min<int>(MAX_CHUNK, (int)std::max<size_t>(fg, cap_bytes / per)) / fg * fg);
   }
   h->bins = make_bins(g.N, g.NB, g.kmin, g.kmax, g.knodes);
@@ -383,8 +386,6 @@ extern "C" int ddm_create(const ddm_geometry *geometry, ddm_engine **out) {
       (rc = dalloc(h, &h->d_radD, (size_t)g.NB * g.L)) || (rc = dalloc(h, &h->d_radP, g.NB)) ||
       (rc = dalloc(h, &h->d_radDrift, (size_t)g.NB * g.L * DRIFT)))
     return bail(rc);
-  for (void *&p : h->d_stage)
-    if ((rc = dalloc(h, (char **)&p, h->stage_bytes))) return bail(rc);
   h->meta_bytes = sizeof(uint32_t) * g.T + sizeof(float) * g.T + sizeof(float) * g.L +
                   sizeof(float2) * g.TPAD;
   if (cudaHostAlloc((void **)&h->h_meta, h->meta_bytes, cudaHostAllocDefault) != cudaSuccess) {
@@ -549,6 +550,11 @@ static int ingest_impl(ddm_engine *h, const void *frames, int dtype, int n, cons
   if ((rc = set_scale(h, scale))) return rc;
   const int N = h->g.N;
   const size_t fbytes = (size_t)N * N * dtype_size(dtype);
+  // the host-frame staging buffers exist from the first host ingest on
+  // (engines fed from device memory never hold them)
+  if (!device && n > 0)
+    for (void *&p : h->d_stage)
+      if (!p && (rc = dalloc(h, (char **)&p, h->stage_bytes))) return rc;
   // device frames: every frame's reference level in one launch ahead of the
   // chunks (host frames arrive chunk by chunk: per chunk with the rows kernel)
   const bool cref_all = device && n > 0 && (size_t)n <= h->rowc_cap;

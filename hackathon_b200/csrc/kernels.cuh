@@ -9,7 +9,7 @@ namespace ddm {
 constexpr int KB = 2;       // kx columns per block of the row-spectrum scratch
 constexpr int DRIFT = 8;    // drift fields per (bin, lag) (ddm_ref.js:28)
 constexpr int PFIELDS = 9;  // D + 8 drift sums per lag in a partial record
-constexpr int MAX_CHUNK = 64;  // frames per spatial launch (slots travel as a kernel parameter)
+constexpr int MAX_CHUNK = 256;  // frames per spatial launch (slots travel as a kernel parameter)
 
 struct RowParams {
   const void* frames;      // [nframes][N][N] u8 / u16 / f32 (16-byte aligned)

@@ -345,7 +345,7 @@ extern "C" int ddm_create(const ddm_geometry *geometry, ddm_engine **out) {
     // buffers hold up to chunk_cap frames, so the autotuner may pick larger
     // chunks (at N >= 1024 one frame's scratch is 4 MB or more and a chunk
     // of four, the column kernel's tile, is already 17 MB)
-    const size_t cap_bytes = g.N >= 1024 ? (288u << 20) : (256u << 20);
+    const size_t cap_bytes = g.N >= 1024 ? (size_t(1) << 30) : (256u << 20);
     h->chunk_cap = std::max(h->chunk, std::min<int>(MAX_CHUNK, (int)std::max<size_t>(fg, cap_bytes / per)) / fg * fg);
   }
   h->bins = make_bins(g.N, g.NB, g.kmin, g.kmax, g.knodes);

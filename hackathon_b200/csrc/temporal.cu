@@ -1093,23 +1093,30 @@ __global__ void __launch_bounds__(NP / 8, TemporalBounds<NP>::MIN_BLOCKS)
         const double2 E0 = base_of(tau < L ? tau : 0);
         E[r] = make_double2(E0.x - (double)cr[r].x, E0.y - (double)cr[r].y);
       }
-#pragma unroll 1
-      for (int s = 0; s < 2; s++) {
-        if (s == 1 && !hasb) break;
-        const int4 e = s ? eb : ea;
-        const double kx = e.y, ky = e.z;
+      // lag-major: W(tau), W(-tau) (and at tau + 1) are read once for both
+      // modes of the pair; per lag the modes still add in the order a, b
 #pragma unroll
-        for (int r = 0; r < LPT; r++) {
-          const int tau = t + r * NT;
-          if (tau < L) {
-            const float inp = s_inp[tau];
-            float gx, gy;
-            G_of(s, tau, gx, gy);
+      for (int r = 0; r < LPT; r++) {
+        const int tau = t + r * NT;
+        if (tau < L) {
+          const float inp = s_inp[tau];
+          const bool next = tau + 1 < L;
+          const float inp1 = next ? s_inp[tau + 1] : 0.f;
+          const float2 w0 = W[pad(tau)], w1 = W[pad((NP - tau) & (NP - 1))];
+          const float2 u0 = next ? W[pad(tau + 1)] : make_float2(0.f, 0.f);
+          const float2 u1 = next ? W[pad((NP - tau - 1) & (NP - 1))] : make_float2(0.f, 0.f);
+#pragma unroll 1
+          for (int s = 0; s < 2; s++) {
+            if (s == 1 && !hasb) break;
+            const int4 e = s ? eb : ea;
+            const double kx = e.y, ky = e.z;
+            // G of mode s from the shared transform: W = n (G_a + i G_b)
+            const float gx = (s ? w0.y + w1.y : w0.x + w1.x) * invn;
+            const float gy = (s ? w1.x - w0.x : w0.y - w1.y) * invn;
             acc[r][0] += ((s ? E[r].y : E[r].x) - 2.0 * gx) * (double)inp;
-            if (tau + 1 < L) {
-              const float inp1 = s_inp[tau + 1];
-              float g1x, g1y;
-              G_of(s, tau + 1, g1x, g1y);
+            if (next) {
+              const float g1x = (s ? u0.y + u1.y : u0.x + u1.x) * invn;
+              const float g1y = (s ? u1.x - u0.x : u0.y - u1.y) * invn;
               const float cx = gx * inp, cy = gy * inp;
               const float c1x = g1x * inp1, c1y = g1y * inp1;
               const float zr = fmaf(c1x, cx, c1y * cy);  // C(tau+1) conj C(tau)
@@ -1129,8 +1136,9 @@ __global__ void __launch_bounds__(NP / 8, TemporalBounds<NP>::MIN_BLOCKS)
             }
           }
         }
-        accP += np0 > 0.5f ? (double)(float)((s ? ST.y : ST.x) / np0) : 0.0;
       }
+      accP += np0 > 0.5f ? (double)(float)(ST.x / np0) : 0.0;
+      if (hasb) accP += np0 > 0.5f ? (double)(float)(ST.y / np0) : 0.0;
     }
     if (k + 2 >= U.y) {
       if (!FULL) {

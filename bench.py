@@ -15,6 +15,12 @@ analyzeRadial, motility-ddm/src/ddm_ref.js:196-206, 425-437).
 Under torchrun each rank analyses its own video (weak scaling, no collective
 on the data path).
 
+  roofline  the dominant kernel (the temporal kernel the engine ran: with 2 %
+         dropped frames the sparse-mask kernel) against the HBM peak, with
+         its FP32 rate beside it, both stages' figures, and cuFFT running just
+         the stages' transforms on device-resident data as a library
+         reference point
+
   fit    (rank 0) q-fits/s of the batched GPU LM on 10^5 held-out q-curves:
          plain (the reference's start strategy), seeded by the tensor-core
          surrogate (trained in the run on 2^20 curves: 2^19 analytic + 2^19

@@ -152,34 +152,91 @@ def _profile_traffic():
     return out
 
 
-def cpu_baseline(frames_u16, valid, sample_frames=24, sample_modes=6144, threads=None):
-    """Times the FP64 oracle (the reference's CPU algorithm restated in C) on
-    a bounded sample of the workload and scales it to frames/s of the whole
-    video: spatial time per frame x T + temporal time per mode x binned modes."""
+# the CPU baseline's temporal sample: the modes of every CPU_BIN_STRIDE-th
+# q-bin from bin 3 on (25.2 % of the binned modes at 256 bins), on the
+# video's real history
+CPU_BIN_STRIDE = 4
+
+
+def _sampled_bins(bins, stride):
+    off = bins["binOffsets"]
+    sel = np.arange(stride - 1, bins["NB"], stride)
+    rows = [bins["binModes"][off[b]:off[b + 1]] for b in sel]
+    sub = dict(bins)
+    sub.update(NB=len(sel), binModes=np.ascontiguousarray(np.concatenate(rows)),
+               binOffsets=np.concatenate([[0], np.cumsum([len(r) for r in rows])]).astype(np.uint32),
+               nModes=np.ascontiguousarray(bins["nModes"][sel]).astype(np.uint32))
+    return sel, sub
+
+
+def cpu_baseline(frames_u16, valid, roi, threads=None, gpu_radial=None, one_core=False, reps=1):
+    """The reference's CPU algorithm (its FP64 C restatement, oracle/) on this
+    very video, timed on the host cores. Both arms call it with the same
+    sample:
+      spatial   every valid frame of the video (History.ingest,
+                ddm_ref.js:196-206, with the ROI pixel mask the engine applies)
+                -- the real history, not a sample;
+      temporal  the masked Wiener-Khinchin analysis and radial sums
+                (analyzeRadial, ddm_ref.js:425-437) of every CPU_BIN_STRIDE-th
+                q-bin's modes of that history, scaled to all binned modes.
+    frames/s = T / (spatial time + temporal time / sampled share of modes);
+    `reps` timings, the median kept. With gpu_radial, the sampled bins' radial
+    D is compared with the GPU's record (max |dD| / bin scale); one_core adds
+    a single-thread figure from 16 frames and every 16th sampled mode."""
     import oracle as O
     threads = threads or os.cpu_count()
     os.environ["OMP_NUM_THREADS"] = str(threads)
-    fr = frames_u16[:sample_frames].astype(np.float64) * (1.0 / 65535)
-    t0 = time.perf_counter()
-    hist = O.history_ingest(fr, np.arange(sample_frames, dtype=np.int32), T)
-    t_sp = (time.perf_counter() - t0) / sample_frames
+    idx = np.nonzero(valid)[0]
+    order, mask = O.linear_order(valid)
     bins = O.make_bins(N, NB, KMIN, KMAX)
     nbinned = int(bins["binOffsets"][-1])
-    rng = np.random.default_rng(0)
-    pick = np.sort(rng.choice(nbinned, size=min(sample_modes, nbinned), replace=False))
-    modes = bins["binModes"][pick, 0].astype(np.int32)
-    # synthetic full-length series for the sampled modes (timing only)
-    h = np.zeros((N * (N // 2 + 1), T), np.complex128)
-    h[modes] = rng.standard_normal((modes.size, T)) + 1j * rng.standard_normal((modes.size, T))
-    order, mask = O.linear_order(valid)
-    t0 = time.perf_counter()
-    O.analyze_modes(h, order, mask, L, modes, TPAD=TPAD, threads=threads)
-    t_tm = (time.perf_counter() - t0) / modes.size
-    del hist, h
-    t_frame = t_sp + t_tm * nbinned / T
-    return {"value": 1.0 / t_frame, "unit": "frames/s", "cores": threads, "kind": "port",
-            "sample": f"{sample_frames} frames of the spatial FFT + {modes.size} of {nbinned} binned "
-                      f"modes of the TPAD={TPAD} masked WK, FP64, scaled to the {T}-frame video"}
+    sel, sub = _sampled_bins(bins, CPU_BIN_STRIDE)
+    frac = sub["binModes"].shape[0] / nbinned
+    runs = []
+    hist = ro = None
+    for _ in range(reps):
+        hist = np.zeros((N * (N // 2 + 1), T), np.complex128)
+        t0 = time.perf_counter()
+        for c in range(0, idx.size, 64):
+            k = idx[c:c + 64]
+            O.history_ingest(frames_u16[k].astype(np.float64) * (1.0 / 65535), k.astype(np.int32), T, hist=hist,
+                             smask=roi)
+        t_sp = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        ro = O.analyze_radial(hist, order, mask, sub, L, TPAD=TPAD, threads=threads)
+        t_tm = time.perf_counter() - t0
+        runs.append((T / (t_sp + t_tm / frac), t_sp, t_tm))
+    runs.sort()
+    v, t_sp, t_tm = runs[len(runs) // 2]
+    out = {"value": v, "unit": "frames/s", "cores": threads, "kind": "port",
+           "sample": f"spatial: all {idx.size} valid frames of the video; temporal: the {sub['binModes'].shape[0]} "
+                     f"modes of every {CPU_BIN_STRIDE}th q-bin ({frac:.1%} of the {nbinned} binned modes) on the "
+                     f"video's own FP64 history, scaled to all binned modes; TPAD={TPAD}, L={L}, FP64",
+           "sample_mode_frac": frac, "spatial_s": t_sp, "temporal_s_sampled": t_tm, "reps": reps}
+    if gpu_radial is not None:
+        Dg = gpu_radial.D2()[sel]
+        sc = np.where(ro["D"].max(axis=1) > 0, ro["D"].max(axis=1), 1)
+        out["agreement"] = {"what": "GPU radial record vs this run's FP64 radial, sampled bins",
+                            "bins": int(len(sel)),
+                            "D_max_rel_to_bin_scale": float((np.abs(Dg - ro["D"]).max(axis=1) / sc).max()),
+                            "P_max_rel": float(np.abs(gpu_radial.P[sel] / np.where(ro["P"] > 0, ro["P"], 1) - 1).max())}
+    if one_core:
+        os.environ["OMP_NUM_THREADS"] = "1"
+        k = idx[:16]
+        h1 = np.zeros((N * (N // 2 + 1), T), np.complex128)
+        t0 = time.perf_counter()
+        O.history_ingest(frames_u16[k].astype(np.float64) * (1.0 / 65535), k.astype(np.int32), T, hist=h1, smask=roi)
+        sp1 = (time.perf_counter() - t0) / k.size
+        del h1
+        m1 = sub["binModes"][::16, 0].astype(np.int32)
+        t0 = time.perf_counter()
+        O.analyze_modes(hist, order, mask, L, m1, TPAD=TPAD, threads=1)
+        tm1 = (time.perf_counter() - t0) / m1.size
+        out["value_1core"] = 1.0 / (sp1 * idx.size / T + tm1 * nbinned / T)
+        out["sample_1core"] = f"{k.size} frames + {m1.size} modes on one thread, scaled to the video"
+        os.environ["OMP_NUM_THREADS"] = str(threads)
+    del hist
+    return out
 
 
 # the surrogate's training videos: 512^2 x 1024, 1024 q-bins over the network's
@@ -244,12 +301,14 @@ def run_reference(args, rank, world):
     spec = synth.config2(seed=1)
     frames, valid, _ = synth.generate(spec, device="cuda" if torch.cuda.is_available() else "cpu")
     fr = frames.view(torch.int16).cpu().numpy().view(np.uint16)
+    roi = synth.roi_mask(spec)
+    del frames
     for _ in range(args.warmup):
-        cpu_baseline(fr, valid, sample_frames=8, sample_modes=1024)
+        cpu_baseline(fr, valid, roi)
     vals = []
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        vals.append(cpu_baseline(fr, valid, sample_frames=8, sample_modes=2048))
+        vals.append(cpu_baseline(fr, valid, roi))
     wall = time.perf_counter() - t0
     v = statistics.median(x["value"] for x in vals)
     line = {"metric": METRIC, "value": v, "unit": "frames/s", "impl": "reference", "n_gpus": world,
@@ -257,10 +316,11 @@ def run_reference(args, rank, world):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "config": {"workload": WORKLOAD},
             "cpu_baseline": {"value": v, "unit": "frames/s", "cores": vals[0]["cores"], "kind": "port",
-                             "sample": vals[0]["sample"]},
+                             "sample": vals[0]["sample"], "sample_mode_frac": vals[0]["sample_mode_frac"]},
             "e2e": {"value": v, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "note": "the reference path is JavaScript (motility-ddm/src/ddm_ref.js, fft.js); no JS "
-                    "runtime exists on this box, so its FP64 C restatement runs on the host cores"}
+                    "runtime exists on this box, so its FP64 C restatement runs on the host cores; "
+                    "each step is the same measurement as the GPU arm's cpu_baseline"}
     print(json.dumps(line), flush=True)
 
 
@@ -814,6 +874,22 @@ def main():
             "pipeline_frac": (sp_bytes + tm_bytes) / (ms_step * 1e6) / peak,
             "stages": stages}
 
+    # full-size checks on this video (outside the timed regions): the fused
+    # radial record equals the record of the full per-mode outputs, D(q, 0) = 0,
+    # everything finite; the CPU baseline below adds the FP64 comparison
+    eng.compute_temporal(order, tmask, full=False)
+    fused = eng.read_radial()
+    eng.compute_temporal(order, tmask, full=True)
+    fullr = eng.read_radial()
+    D1, D2 = fused.D2(), fullr.D2()
+    sc = np.abs(D1).max(axis=1, keepdims=True)
+    checks = {"finite": bool(np.isfinite(D1).all() and np.isfinite(fused.P).all() and np.isfinite(fused.drift).all()),
+              "fused_vs_full_D_max_rel": float((np.abs(D1 - D2) / np.where(sc > 0, sc, 1)).max()),
+              "fused_vs_full_P_max_rel": float(np.abs(fused.P / np.where(fullr.P > 0, fullr.P, 1) - 1)[fullr.P > 0].max()),
+              "D0_max_rel": float((np.abs(D1[:, 0:1]) / np.where(sc > 0, sc, 1)).max()),
+              "kernel": eng.last_temporal_kernel}
+    del fullr
+
     fit = None
     if rank == 0 and not args.no_fit:
         fit = fit_benchmark()
@@ -821,7 +897,7 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         fr = frames.view(torch.int16).cpu().numpy().view(np.uint16)
-        cpu = cpu_baseline(fr, valid)
+        cpu = cpu_baseline(fr, valid, mask_roi, gpu_radial=radial, one_core=True, reps=3)
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": world,
@@ -842,6 +918,7 @@ def main():
                 "roofline": roof,
                 "clocks": clk,
                 "cpu_baseline": cpu,
+                "checks": checks,
                 "binned_modes": nbinned,
                 "fit": fit}
         print(json.dumps(line), flush=True)

@@ -120,6 +120,7 @@ _SIGS = {
     "ddm_mlp_train_step": (C.c_int, [_vp, _vp, _vp, _i32, C.c_float, _vp, _vp]),
     "ddm_mlp_sync": (C.c_int, [_vp, _vp]),
     "ddm_spectra_noalloc": (C.c_int, [_vp, _i32, _i32, _i32, _i32, _vp, C.c_float, _vp, _vp]),
+    "ddm_spectra_noalloc_status": (C.c_int, [_vp]),
 }
 
 _lib = None

@@ -27,6 +27,14 @@
 // device addresses of the arrays (cudaGetSymbolAddress) and fills the tables;
 // make that first call before any stream capture. A later call with another N
 // or scale refills the tables, ordered on the caller's stream.
+//
+// Errors on the device: the row and column kernels wait for their staged
+// copies with bounded waits. A wait that gives up leaves part of the ring
+// unwritten and records a code in g_err, a file-scope device word that each
+// call zeroes on its stream before its kernels run. The call itself returns
+// once the work is queued; ddm_spectra_noalloc_status(stream) waits for the
+// stream, reads the word (a copy from the symbol, no allocation) and turns
+// a recorded code into DDM_ERR_CUDA.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -55,6 +63,7 @@ static __device__ __align__(256) float g_wys[NOALLOC_MAX_N];
 static __device__ __align__(256) float2 g_tw[NOALLOC_MAX_N];
 static __device__ __align__(256) float2 g_wcorr4[4];
 static __device__ __align__(256) double g_invtot[1];
+static __device__ __align__(256) int g_err[1];  // 0, or the code of a bounded wait that gave up
 
 struct DeviceState {
   bool ready = false;
@@ -67,6 +76,7 @@ struct DeviceState {
   float2* tw = nullptr;
   float2* wcorr4 = nullptr;
   double* invtot = nullptr;
+  int* err = nullptr;
   int N = 0;
   float scale = 0.f;
 };
@@ -118,7 +128,8 @@ extern "C" int ddm_spectra_noalloc(const void* frames, int32_t dtype, int32_t n,
       if (lookup(g_rows_scratch, (void**)&d.rows) || lookup(g_rowc, (void**)&d.rowc) ||
           lookup(g_framesum, (void**)&d.framesum) || lookup(g_means, (void**)&d.means) ||
           lookup(g_win, (void**)&d.win) || lookup(g_wys, (void**)&d.wys) || lookup(g_tw, (void**)&d.tw) ||
-          lookup(g_wcorr4, (void**)&d.wcorr4) || lookup(g_invtot, (void**)&d.invtot))
+          lookup(g_wcorr4, (void**)&d.wcorr4) || lookup(g_invtot, (void**)&d.invtot) ||
+          lookup(g_err, (void**)&d.err))
         return nf_fail(DDM_ERR_CUDA, "ddm_spectra_noalloc: cudaGetSymbolAddress failed");
       d.ready = true;
     }
@@ -155,6 +166,8 @@ extern "C" int ddm_spectra_noalloc(const void* frames, int32_t dtype, int32_t n,
     st = d;
   }
   const size_t fbytes = (size_t)N * N * (dtype == 0 ? 1 : dtype == 1 ? 2 : 4);
+  if (cudaMemsetAsync(st.err, 0, sizeof(int), s) != cudaSuccess)
+    return nf_fail(DDM_ERR_CUDA, "ddm_spectra_noalloc: cudaMemsetAsync failed");
   for (int c0 = 0; c0 < n; c0 += chunk) {
     const int m = std::min(chunk, n - c0);
     if (cudaMemsetAsync(st.framesum, 0, sizeof(double) * m, s) != cudaSuccess)
@@ -170,7 +183,7 @@ extern "C" int ddm_spectra_noalloc(const void* frames, int32_t dtype, int32_t n,
     rp.rows = st.rows;
     rp.framec = st.rowc;
     rp.framesum = st.framesum;
-    rp.err = nullptr;  // bounded waits still end; there is no engine to report to
+    rp.err = st.err;
     if (launch_rows(N, dtype, rp, s) != cudaSuccess)
       return nf_fail(DDM_ERR_CUDA, "ddm_spectra_noalloc: row kernel launch failed");
     ColParams cp{};
@@ -189,9 +202,30 @@ extern "C" int ddm_spectra_noalloc(const void* frames, int32_t dtype, int32_t n,
     cp.T = T;
     cp.NH = NH;
     cp.NHB = NHB;
-    cp.err = nullptr;
+    cp.err = st.err;
     if (launch_cols(N, cp, s) != cudaSuccess)
       return nf_fail(DDM_ERR_CUDA, "ddm_spectra_noalloc: column kernel launch failed");
+  }
+  return DDM_OK;
+}
+
+extern "C" int ddm_spectra_noalloc_status(void* stream) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return nf_fail(DDM_ERR_NODEV, "ddm_spectra_noalloc_status: no device");
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if ((int)g_state.size() <= dev || !g_state[dev].ready) return DDM_OK;  // no call on this device yet
+  }
+  if (cudaStreamSynchronize((cudaStream_t)stream) != cudaSuccess)
+    return nf_fail(DDM_ERR_CUDA, "ddm_spectra_noalloc_status: stream synchronisation failed");
+  int e = 0;
+  if (cudaMemcpyFromSymbol(&e, g_err, sizeof(int)) != cudaSuccess)
+    return nf_fail(DDM_ERR_CUDA, "ddm_spectra_noalloc_status: reading the error word failed");
+  if (e) {
+    const int zero = 0;
+    cudaMemcpyToSymbol(g_err, &zero, sizeof(int));
+    return nf_fail(DDM_ERR_CUDA, e == 2 ? "ddm_spectra_noalloc: a staged row copy did not complete in time (code 2)"
+                                        : "ddm_spectra_noalloc: a staged column copy did not complete in time (code 3)");
   }
   return DDM_OK;
 }

@@ -402,10 +402,19 @@ int ddm_mlp_sync(ddm_mlp *h, void *stream);
  * first call before any stream capture. All calls share the scratch: calls
  * whose work overlaps on the GPU race, so serialise them. Errors: DDM_ERR_ARG,
  * DDM_ERR_TOO_LARGE, DDM_ERR_CUDA, DDM_ERR_NODEV; message from
- * ddm_create_error(). */
+ * ddm_create_error(). The call returns once its work is queued; a bounded
+ * wait for a staged copy that gave up on the device is reported by
+ * ddm_spectra_noalloc_status. */
 int ddm_spectra_noalloc(const void *frames, int32_t dtype, int32_t n, int32_t N,
                         int32_t T, const int32_t *slots, float scale, void *hist,
                         void *stream);
+/* Completion status of the last ddm_spectra_noalloc call queued on `stream`
+ * on the current device: waits for the stream, then returns DDM_OK, or
+ * DDM_ERR_CUDA when one of its kernels recorded a staged copy that did not
+ * complete in time (the ring is then partly written; the device word is
+ * cleared). Allocates nothing. No counterpart in the reference (its WebGPU
+ * queue reports validation errors through onError, ddm-engine.ts:28). */
+int ddm_spectra_noalloc_status(void *stream);
 
 /* ------------------------------------------------------------------ movies
  * The reference's seeded movie generator (test/sim.mjs:90-186: mulberry32

@@ -164,16 +164,17 @@ void or_make_bins(int N, int NB, double kmin, double kmax, int K,
   free(hk);
 }
 
-/* Transform luma frames into ring slots (ddm_ref.js:196-206). */
-void or_history_ingest(double *hist, int N, int T, const double *luma,
-                       const int *slots, int nframes) {
+/* Transform luma frames into ring slots (ddm_ref.js:196-206); smask: the
+ * spatial-mask extension of or_spectrum2d_half_masked (NULL = none). */
+void or_history_ingest_masked(double *hist, int N, int T, const double *luma,
+                              const uint8_t *smask, const int *slots, int nframes) {
   const int NH = (N >> 1) + 1, M = N * NH;
   double *win = (double *)malloc(sizeof(double) * N);
   or_blackman_harris(win, N);
 #pragma omp parallel for schedule(dynamic)
   for (int f = 0; f < nframes; f++) {
     double *spec = (double *)malloc(sizeof(double) * 2 * M);
-    or_spectrum2d_half(luma + (size_t)f * N * N, N, win, spec);
+    or_spectrum2d_half_masked(luma + (size_t)f * N * N, N, win, smask, spec);
     const int slot = slots[f];
     for (int m = 0; m < M; m++) {
       const size_t o = ((size_t)m * T + slot) * 2;
@@ -183,6 +184,11 @@ void or_history_ingest(double *hist, int N, int T, const double *luma,
     free(spec);
   }
   free(win);
+}
+
+void or_history_ingest(double *hist, int N, int T, const double *luma,
+                       const int *slots, int nframes) {
+  or_history_ingest_masked(hist, N, T, luma, NULL, slots, nframes);
 }
 
 /* Masked Wiener-Khinchin structure function of one mode (ddm_ref.js:229-288).

@@ -91,18 +91,28 @@ void or_blackman_harris(double *w, int n) {
 
 /* Mean-subtracted, separably windowed half-plane 2D spectrum scaled by 1/N
  * (fft.js:149-183). out[2*(ky*NH + kx) + {re,im}], kx in [0, N/2]. */
-void or_spectrum2d_half(const double *img, int N, const double *win,
-                        double *out) {
+/* Extension (the reference has no spatial mask): with smask != NULL the mean
+ * is taken over the pixels where smask != 0, and those pixels alone enter the
+ * transform, ((I - mean) * w(x) * w(y) * S(x, y)). smask == NULL is the
+ * reference's spectrum2dHalf exactly. */
+void or_spectrum2d_half_masked(const double *img, int N, const double *win,
+                               const uint8_t *smask, double *out) {
   const int NH = (N >> 1) + 1;
-  double mean = 0;
-  for (int i = 0; i < N * N; i++) mean += img[i];
-  mean /= (double)N * N;
+  double mean = 0, cnt = 0;
+  if (smask) {
+    for (int i = 0; i < N * N; i++)
+      if (smask[i]) mean += img[i], cnt += 1;
+    mean = cnt > 0 ? mean / cnt : 0;
+  } else {
+    for (int i = 0; i < N * N; i++) mean += img[i];
+    mean /= (double)N * N;
+  }
   double *row = (double *)malloc(sizeof(double) * 2 * N);
   double *rows = (double *)malloc(sizeof(double) * 2 * N * NH);
   for (int y = 0; y < N; y++) {
     const double wy = win[y];
     for (int x = 0; x < N; x++) {
-      row[2 * x] = (img[y * N + x] - mean) * win[x] * wy;
+      row[2 * x] = (smask && !smask[y * N + x]) ? 0 : (img[y * N + x] - mean) * win[x] * wy;
       row[2 * x + 1] = 0;
     }
     or_fft(row, N, 0);
@@ -126,4 +136,9 @@ void or_spectrum2d_half(const double *img, int N, const double *win,
   }
   free(row);
   free(rows);
+}
+
+void or_spectrum2d_half(const double *img, int N, const double *win,
+                        double *out) {
+  or_spectrum2d_half_masked(img, N, win, NULL, out);
 }

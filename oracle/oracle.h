@@ -40,6 +40,9 @@ void or_dft(const double *in, double *out, int n, int inverse); /* fft.js:101-11
 void or_blackman_harris(double *w, int n);                      /* fft.js:126-133 */
 void or_spectrum2d_half(const double *img, int N, const double *win,
                         double *out);                           /* fft.js:149-183 */
+/* Extension: spatial pixel mask (mean over smask != 0, masked pixels zero). */
+void or_spectrum2d_half_masked(const double *img, int N, const double *win,
+                               const uint8_t *smask, double *out);
 
 /* ------------------------------------------------------------ ddm_ref.js */
 int or_window_leakage(int N, double step, double *d, double *p); /* ddm_ref.js:40-55 */
@@ -56,6 +59,9 @@ void or_make_bins(int N, int NB, double kmin, double kmax, int knodes,
  * spec_out, if not NULL, receives the last frame's spectrum. */
 void or_history_ingest(double *hist, int N, int T, const double *luma,
                        const int *slots, int nframes);
+/* Same with the spatial-mask extension (smask N*N bytes, NULL = none). */
+void or_history_ingest_masked(double *hist, int N, int T, const double *luma,
+                              const uint8_t *smask, const int *slots, int nframes);
 
 /* ddm_ref.js:229-288, with n = TPAD (the reference uses 2T). */
 double or_temporal_mode(const double *hist, int mode, int T, int TPAD,

@@ -91,6 +91,7 @@ def lib():
         "or_make_bins": (None, [C.c_int, C.c_int, C.c_double, C.c_double, C.c_int,
                                 _u32p, _i32p, _dp, _u32p, _dp]),
         "or_history_ingest": (None, [_dp, C.c_int, C.c_int, _dp, _i32p, C.c_int]),
+        "or_history_ingest_masked": (None, [_dp, C.c_int, C.c_int, _dp, C.c_void_p, _i32p, C.c_int]),
         "or_temporal_mode": (C.c_double, [_dp, C.c_int, C.c_int, C.c_int, _u32p, _dp,
                                           C.c_int, _dp, _dp]),
         "or_temporal_mode_direct": (C.c_double, [_dp, C.c_int, C.c_int, _u32p, _dp,
@@ -209,17 +210,25 @@ def make_bins(N, NB, kmin, kmax, knodes=4):
                 nModes=nm, kNodes=kn)
 
 
-def history_ingest(luma, slots, T, hist=None):
+def history_ingest(luma, slots, T, hist=None, smask=None):
     """History.ingest (ddm_ref.js:196-206) for a stack of frames [F, N, N].
-    Returns the history as complex128 [modes, T] (the reference layout)."""
+    Returns the history as complex128 [modes, T] (the reference layout).
+    smask: the spatial-mask extension (N x N, nonzero = used; the reference
+    has none): mean over the used pixels, the others left out."""
     luma = np.ascontiguousarray(luma, dtype=np.float64)
     F, N, _ = luma.shape
     M = N * (N // 2 + 1)
     if hist is None:
         hist = np.zeros((M, T), np.complex128)
     h = hist.view(np.float64).reshape(-1)
-    lib().or_history_ingest(h, N, T, luma.reshape(-1),
-                            np.ascontiguousarray(slots, dtype=np.int32), F)
+    if smask is None:
+        lib().or_history_ingest(h, N, T, luma.reshape(-1),
+                                np.ascontiguousarray(slots, dtype=np.int32), F)
+    else:
+        sm = np.ascontiguousarray(smask, dtype=np.uint8).reshape(-1)
+        assert sm.size == N * N
+        lib().or_history_ingest_masked(h, N, T, luma.reshape(-1), sm.ctypes.data,
+                                       np.ascontiguousarray(slots, dtype=np.int32), F)
     return hist
 
 

@@ -10,14 +10,16 @@ README and stored here as JSON:
   validation_matrix.json  the per-scenario outputs the reference publishes
                           for its 11-scenario matrix (README.md section 6)
 
-Usage (needs the reference checkout):  python tests/golden/make_golden.py
+Usage (needs a checkout of the reference's motility-ddm app):
+    python tests/golden/make_golden.py <path to motility-ddm>
+or set MOTILITY_DDM_REF to that path. Without either, it exits with a message.
 """
 import json
 import os
 import re
 import sys
 
-REF = "/root/reference/motility-ddm"
+REF = None  # the motility-ddm checkout, from the command line or MOTILITY_DDM_REF
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 
@@ -106,5 +108,16 @@ def main():
         print("wrote", name)
 
 
+def _ref_path(argv):
+    path = argv[1] if len(argv) > 1 else os.environ.get("MOTILITY_DDM_REF")
+    if not path:
+        sys.exit("make_golden.py: give the motility-ddm checkout as the first argument "
+                 "or in MOTILITY_DDM_REF")
+    if not os.path.isfile(os.path.join(path, "test", "t_kernels.mjs")):
+        sys.exit(f"make_golden.py: {path} does not look like motility-ddm (no test/t_kernels.mjs)")
+    return path
+
+
 if __name__ == "__main__":
+    REF = _ref_path(sys.argv)
     main()

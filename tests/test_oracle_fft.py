@@ -128,3 +128,23 @@ def test_temporal_meta_counts():
     z = np.zeros(TPAD)
     z[:T] = mask
     assert np.max(np.abs(ms - np.fft.fft(z))) < 1e-10
+
+
+def test_spatial_mask_extension_vs_numpy():
+    """The oracle's spatial-mask extension (the reference has none): mean over
+    the used pixels, masked pixels left out, against numpy's FP64 FFT; with no
+    mask it is the reference's spectrum2dHalf unchanged."""
+    N, T = 64, 3
+    rng = np.random.default_rng(5)
+    luma = rng.random((T, N, N))
+    yy, xx = np.mgrid[:N, :N]
+    S = ((xx - N / 2) ** 2 + (yy - N / 2) ** 2 <= (0.4 * N) ** 2).astype(np.uint8)
+    h = O.history_ingest(luma, np.arange(T, dtype=np.int32), T, smask=S)
+    h0 = O.history_ingest(luma, np.arange(T, dtype=np.int32), T)
+    w = O.blackman_harris(N)
+    NH = N // 2 + 1
+    for t in range(T):
+        mu = (luma[t] * S).sum() / S.sum()
+        F = np.fft.fft2((luma[t] - mu) * w[None, :] * w[:, None] * S)[:, :NH] / N
+        assert np.abs(h[:, t] - F.reshape(-1)).max() < 1e-12 * np.abs(F).max()
+        assert np.array_equal(h0[:, t], O.spectrum2d_half(luma[t]).reshape(-1))

@@ -214,6 +214,18 @@ def cpu_baseline(frames_u16, valid, roi, threads=None, gpu_radial=None, one_core
                      f"video's own FP64 history, scaled to all binned modes; TPAD={TPAD}, L={L}, FP64",
            "sample_mode_frac": frac, "spatial_s": t_sp, "temporal_s_sampled": t_tm, "reps": reps}
     if gpu_radial is not None:
+        # the same record's motility analysis by the oracle (one thread, like
+        # the reference's worker), beside the GPU's
+        rec = O.Radial(gpu_radial.N, gpu_radial.NB, gpu_radial.L, np.asarray(gpu_radial.kCenter, np.float64),
+                       np.asarray(gpu_radial.kNodes, np.float64), np.asarray(gpu_radial.nModes, np.uint32),
+                       np.asarray(gpu_radial.D, np.float64), np.asarray(gpu_radial.P, np.float64),
+                       np.asarray(gpu_radial.drift, np.float64))
+        t0 = time.perf_counter()
+        ores = O.analyze_motility(rec, **MOTILITY_OPTS)
+        ta = time.perf_counter() - t0
+        out["analysis"] = {"what": "analyzeMotility of the GPU's radial record, FP64 oracle, one thread",
+                           "s_per_record": ta, "records_per_s": 1.0 / ta,
+                           "result": {k: ores[k] for k in ("verdict", "alpha", "vbar", "Z", "Ddiff", "dBIC")}}
         Dg = gpu_radial.D2()[sel]
         sc = np.where(ro["D"].max(axis=1) > 0, ro["D"].max(axis=1), 1)
         out["agreement"] = {"what": "GPU radial record vs this run's FP64 radial, sampled bins",
@@ -237,6 +249,43 @@ def cpu_baseline(frames_u16, valid, roi, threads=None, gpu_radial=None, one_core
         os.environ["OMP_NUM_THREADS"] = str(threads)
     del hist
     return out
+
+
+# the motility analysis of the 512^2 x 1024 record: pixel/frame units; the
+# reference's 2 um/s swimmer floor (GATES.SWIM_MIN_UM_S) is lowered to 0.1
+# px/frame because this workload's mean swim speed, 1.5 px/frame, lies below it
+MOTILITY_OPTS = dict(dxUm=1.0, fps=1.0, geometry="3d", swimMin=0.1)
+
+
+def motility_benchmark(radial, truth, n_batch=48, reps=5):
+    """analyzeMotility (motility_fit.js:870-990) on the video's radial
+    record: every model fit on the GPU (csrc/gfit.cu), the statistics on the
+    host. Wall-clock per call through the C ABI (host record in, result out):
+    one record at a time, and n_batch records in one batched call (one launch
+    per stage for all records)."""
+    from hackathon_b200.motility import analyze_motility, analyze_motility_batch
+    analyze_motility(radial, **MOTILITY_OPTS)  # context and 2D table set-up, outside the timing
+    t = []
+    res = None
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        res = analyze_motility(radial, **MOTILITY_OPTS)
+        t.append(time.perf_counter() - t0)
+    analyze_motility_batch([radial] * 2, **MOTILITY_OPTS)
+    t0 = time.perf_counter()
+    batch = analyze_motility_batch([radial] * n_batch, **MOTILITY_OPTS)
+    tb = time.perf_counter() - t0
+    same = all(b["alpha"] == res["alpha"] and b["vbar"] == res["vbar"] for b in batch)
+    return {"what": "analyzeMotility of the video's radial record (Brownian, swimmer and drift fits of one "
+                    "parameter set over all q-bins on the GPU; drift LSQ, BIC and gates on the host), "
+                    "wall clock through the C ABI",
+            "records_per_s": 1.0 / statistics.median(t), "ms_per_record": 1e3 * statistics.median(t),
+            "batch": {"records": n_batch, "records_per_s": n_batch / tb, "equal_to_single": bool(same)},
+            "options": MOTILITY_OPTS, "nbins": res["nbins"], "nlags": res["nlags"],
+            "result": {k: res[k] for k in ("verdict", "alpha", "vbar", "Z", "Ddiff", "DdiffBrownian", "dBIC",
+                                           "driftMag", "mu", "TSI")},
+            "generator_truth": {"swimmer_share": 1 - truth["frac_brownian"], "vbar": truth["vbar"],
+                                "Z": truth["Z"], "D": truth["D"]}}
 
 
 # the surrogate's training videos: 512^2 x 1024, 1024 q-bins over the network's
@@ -890,6 +939,8 @@ def main():
               "kernel": eng.last_temporal_kernel}
     del fullr
 
+    motility = motility_benchmark(fused, truth) if rank == 0 else None
+
     fit = None
     if rank == 0 and not args.no_fit:
         fit = fit_benchmark()
@@ -919,6 +970,7 @@ def main():
                 "clocks": clk,
                 "cpu_baseline": cpu,
                 "checks": checks,
+                "motility": motility,
                 "binned_modes": nbinned,
                 "fit": fit}
         print(json.dumps(line), flush=True)

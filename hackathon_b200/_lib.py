@@ -21,7 +21,8 @@ class RadialView(C.Structure):
 
 class MotilityOptions(C.Structure):
     _fields_ = [("dxUm", C.c_double), ("fps", C.c_double), ("geometry2d", C.c_int32),
-                ("exposureLocked", C.c_int32), ("swimMin", C.c_double)]
+                ("exposureLocked", C.c_int32), ("swimMin", C.c_double), ("optimizer", C.c_int32),
+                ("reserved", C.c_int32)]
 
 
 class MotilityFit(C.Structure):
@@ -91,6 +92,8 @@ _SIGS = {
     "ddm_kernel_launches": (C.c_int64, [_vp]),
     "ddm_fit_lm": (C.c_int, [_i32, _i32, _i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i32, _i32,
                              C.c_double, _i32, _vp, _vp, _vp, _vp, _vp, _i32, _vp]),
+    "ddm_fit_lm_model": (C.c_int, [_i32, _i32, _i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i32, _i32,
+                                   C.c_double, _i32, _i32, _vp, _vp, _vp, _vp, _vp, _vp, _i32, _vp]),
     "ddm_model_curves": (C.c_int, [_i32, _i32, _vp, _vp, _i32, _vp, C.c_float, C.c_uint64, _vp, _vp, _vp]),
     "ddm_autotune": (C.c_int, [_vp, C.c_char_p, _i32]),
     "ddm_get_tuning": (C.c_int, [_vp, C.POINTER(_i32), C.POINTER(_i32), C.POINTER(_i32)]),
@@ -99,6 +102,15 @@ _SIGS = {
     "ddm_simulate_error": (C.c_char_p, []),
     "ddm_analyze_motility": (C.c_int, [C.POINTER(RadialView), C.POINTER(MotilityOptions),
                                        C.POINTER(MotilityResult)]),
+    "ddm_analyze_motility_batch": (C.c_int, [_i32, C.POINTER(RadialView), C.POINTER(MotilityOptions),
+                                             C.POINTER(MotilityResult)]),
+    "ddm_isf_eval": (C.c_int, [_i32, _i32, _vp, _vp, _vp, _vp, _vp]),
+    "ddm_prepared_bins": (C.c_int, [C.POINTER(RadialView), C.POINTER(MotilityOptions), _vp, C.POINTER(_i32),
+                                    C.POINTER(_i32)]),
+    "ddm_temporal_structure_index": (C.c_double, [C.POINTER(RadialView)]),
+    "ddm_estimate_drift": (C.c_int, [C.POINTER(RadialView), C.POINTER(MotilityOptions), _vp, _vp]),
+    "ddm_scaling_exponent": (C.c_int, [C.POINTER(RadialView), C.POINTER(MotilityOptions), _vp,
+                                       C.POINTER(C.c_double)]),
     "ddm_batch_create": (C.c_int, [_vp, _i32, C.POINTER(_vp)]),
     "ddm_batch_destroy": (None, [_vp]),
     "ddm_batch_last_error": (C.c_char_p, [_vp]),

@@ -4,6 +4,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "isf.cuh"
+
 namespace ddm {
 
 constexpr int KB = 2;       // kx columns per block of the row-spectrum scratch
@@ -122,6 +124,9 @@ struct LmParams {
   int* counter;            // work counter, 0 at launch (warps fetch fits)
   int mode, max_iter, nrefine;
   double tol;
+  int geometry2d;          // swimmer kernel: 0 3D closed form, 1 2D table
+  const float* vmag;       // [nfit] drift speed |V| of the J0 factor, or nullptr (none)
+  Isf2dTable tab;          // the 2D table (geometry2d = 1)
 };
 
 // launchers (return cudaGetLastError())

@@ -2,9 +2,12 @@
 //
 // Model (the reference's model column, motility_fit.js:417-432, per bin):
 //   y(tau) = A c(tau) + B,
-//   c(tau) = 1 - <exp(-D q^2 tau) (1 - alpha + alpha g(q vbar tau; Z))>_nodes
-// with g the Schulz-averaged 3D swimmer ISF (isf3d, motility_fit.js:140-144)
-// averaged over the bin's effective-|k| nodes. Parameters
+//   c(tau) = 1 - <exp(-D q^2 tau) J0(q |V| tau) (1 - alpha + alpha g(q vbar tau; Z))>_nodes
+// with g the Schulz-averaged swimmer ISF -- 3D (isf3d, motility_fit.js:140-144)
+// or 2D (isf2d, :152-159, read from the device table of isf2d.cu; the
+// reference's swimmerKernel, :227-229) -- averaged over the bin's
+// effective-|k| nodes, and J0(q |V| tau) the radial average of a known
+// uniform drift |V| per fit (0: no factor). Parameters
 //   theta = (A, B, alpha, ln vbar, ln Z, ln D),  A, B >= 0, alpha in [0, 1],
 // ln vbar, ln Z, ln D clamped to the reference's bounds (bounds(),
 // motility_fit.js:480-491). The reference fits (alpha, vbar, Z, D) globally by
@@ -24,6 +27,7 @@
 #include <cstdint>
 
 #include "../../include/ddm_b200.h"
+#include "isf.cuh"
 #include "kernels.cuh"
 
 namespace ddm {
@@ -35,46 +39,36 @@ constexpr int LM_WARPS = 8;        // fits per 256-thread CTA
 
 // Precision-generic math for the model: FP32 for the bulk of the
 // iterations, FP64 for the final refinement.
-__device__ __forceinline__ float m_atan(float x) { return atanf(x); }
-__device__ __forceinline__ double m_atan(double x) { return atan(x); }
-__device__ __forceinline__ float m_log1p(float x) { return log1pf(x); }
-__device__ __forceinline__ double m_log1p(double x) { return log1p(x); }
 __device__ __forceinline__ float m_exp(float x) { return expf(x); }
 __device__ __forceinline__ double m_exp(double x) { return exp(x); }
-__device__ __forceinline__ void m_sincos(float x, float* s, float* c) { sincosf(x, s, c); }
-__device__ __forceinline__ void m_sincos(double x, double* s, double* c) { sincos(x, s, c); }
-
-// g(x; Z) (isf3d, motility_fit.js:140-144) and its log-derivatives
-// x dg/dx, Z dg/dZ.
-template <typename R>
-__device__ __forceinline__ void isf3d_d(R x, R Z, R& g, R& gx, R& gz) {
-  const R Z1 = Z + R(1);
-  const R L = x / Z1;
-  if (L < R(1e-4)) {
-    const R x2 = x * x;
-    g = R(1) - x2 * (Z + R(2)) / (R(6) * Z1);
-    gx = R(-2) * x2 * (Z + R(2)) / (R(6) * Z1);
-    gz = x2 * Z / (R(6) * Z1 * Z1);
-    return;
-  }
-  const R a = m_atan(L), u = R(1) + L * L, lu = m_log1p(L * L);
-  const R U = m_exp(R(0.5) * Z * lu);
-  R s, c;
-  m_sincos(Z * a, &s, &c);
-  const R G = s / (Z * L * U);
-  const R LgL = c / (u * U) - G * (R(1) + Z * L * L / u);
-  g = G;
-  gx = LgL;
-  gz = a * c / (L * U) - G - R(0.5) * Z * G * lu - (Z / Z1) * LgL;
-}
 
 struct LmProblem {
   int nt, K;
+  int g2d;             // swimmer kernel: 0 3D, 1 2D (table)
+  float V;             // drift speed |V| of the J0 factor (0: none)
+  Isf2dTable tab;
   float w;
   float qn[LM_MAX_NODES];
   float d[4], tau[4];  // this lane's lags j = lane + 32 r
   double lo[LM_NP], hi[LM_NP];
 };
+
+__device__ __forceinline__ float m_j0(float y) { return j0f(y); }
+__device__ __forceinline__ double m_j0(double y) { return j0(y); }
+
+// The swimmer kernel of the fit's geometry: g, x dg/dx, Z dg/dZ.
+template <typename R>
+__device__ __forceinline__ void swim_isf(const LmProblem& P, R x, R Z, R& g, R& gx, R& gz) {
+  if (P.g2d) {
+    double a, b, c;
+    isf2d_d(P.tab, (double)x, (double)Z, a, b, c);
+    g = (R)a;
+    gx = (R)b;
+    gz = (R)c;
+  } else {
+    isf3d_d<R>(x, Z, g, gx, gz);
+  }
+}
 
 template <typename T>
 __device__ __forceinline__ T warp_sum(T v) {
@@ -96,10 +90,11 @@ __device__ __forceinline__ void model_c(const LmProblem& P, int lane, float al, 
     float sE = 0.f;
     for (int n = 0; n < P.K; n++) {
       const float q = P.qn[n];
-      const float E = expf(-D * q * q * t);
+      float E = expf(-D * q * q * t);
+      if (P.V > 0.f) E *= m_j0(q * P.V * t);
       if (al > 0.f) {
         float g, gx, gz;
-        isf3d_d(q * v * t, Z, g, gx, gz);
+        swim_isf<float>(P, q * v * t, Z, g, gx, gz);
         sE += E * (1.f - al + al * g);
       } else {
         sE += E;
@@ -175,7 +170,7 @@ __device__ __forceinline__ double varpro_brownian64(const LmProblem& P, int lane
     double sE = 0.0;
     for (int n = 0; n < P.K; n++) {
       const double q = P.qn[n];
-      sE += exp(-D * q * q * t);
+      sE += P.V > 0.f ? exp(-D * q * q * t) * j0(q * (double)P.V * t) : exp(-D * q * q * t);
     }
     c[r] = 1.0 - sE * iK;
   }
@@ -202,9 +197,10 @@ __device__ __forceinline__ void lm_normal(const LmProblem& P, const double (&th)
     R sE = 0, sEg = 0, sdD = 0, sgx = 0, sgz = 0;
     for (int n = 0; n < P.K; n++) {
       const R q = (R)P.qn[n];
-      const R E = m_exp(-D * q * q * t);
+      R E = m_exp(-D * q * q * t);
+      if (P.V > 0.f) E *= m_j0(q * (R)P.V * t);
       R g, gx, gz;
-      isf3d_d<R>(q * v * t, Z, g, gx, gz);
+      swim_isf<R>(P, q * v * t, Z, g, gx, gz);
       const R mix = R(1) - al + al * g;
       sE += E * mix;
       sEg += E * (g - R(1));
@@ -466,6 +462,9 @@ __device__ __noinline__ void lm_one(const LmParams& p, int fit, int lane) {
   LmProblem P;
   P.nt = min(p.nt[fit], min(p.nt_max, LM_MAX_LAGS));
   P.K = min(p.K, LM_MAX_NODES);
+  P.g2d = p.geometry2d;
+  P.V = p.vmag ? p.vmag[fit] : 0.f;
+  P.tab = p.tab;
   P.w = p.w[fit];
 #pragma unroll
   for (int n = 0; n < LM_MAX_NODES; n++) P.qn[n] = n < P.K ? p.qn[(size_t)fit * p.K + n] : 0.f;
@@ -610,11 +609,11 @@ cudaError_t stage_in(T** dst, const T* src, size_t n, cudaStream_t s) {
 
 }  // namespace
 
-extern "C" int ddm_fit_lm(int32_t nfit, int32_t nt_max, int32_t K, const int32_t* nt, const float* d,
-                          const float* tau, const float* qn, const float* w, const float* bounds,
-                          const float* start, int32_t mode, int32_t max_iter, double tol,
-                          int32_t nrefine, double* theta, double* cost, int32_t* iters, int32_t* evals,
-                          int32_t* status, int32_t on_device, void* stream) {
+extern "C" int ddm_fit_lm_model(int32_t nfit, int32_t nt_max, int32_t K, const int32_t* nt, const float* d,
+                                const float* tau, const float* qn, const float* w, const float* bounds,
+                                const float* start, int32_t mode, int32_t max_iter, double tol, int32_t nrefine,
+                                int32_t geometry2d, const float* vmag, double* theta, double* cost, int32_t* iters,
+                                int32_t* evals, int32_t* status, int32_t on_device, void* stream) {
   ddm_detached_error().clear();
   if (nfit < 0 || nt_max < 1 || nt_max > ddm::LM_MAX_LAGS || K < 1 || K > ddm::LM_MAX_NODES)
     return lm_fail(DDM_ERR_ARG, "ddm_fit_lm: need nfit >= 0, 1 <= nt_max <= %d, 1 <= K <= %d",
@@ -624,6 +623,7 @@ extern "C" int ddm_fit_lm(int32_t nfit, int32_t nt_max, int32_t K, const int32_t
                    "ddm_fit_lm: mode must be 0 (reference starts), 1 (seeded), 2 (seeded, fallback) or 3 (Brownian)");
   if (max_iter < 1 || nrefine < 1 || nrefine > 64 || !(tol >= 0))
     return lm_fail(DDM_ERR_ARG, "ddm_fit_lm: need max_iter >= 1, 1 <= nrefine <= 64, tol >= 0");
+  if (geometry2d != 0 && geometry2d != 1) return lm_fail(DDM_ERR_ARG, "ddm_fit_lm: geometry2d must be 0 or 1");
   if (nfit == 0) return DDM_OK;
   const bool seeded = mode == ddm::LM_SEEDED || mode == ddm::LM_SEEDED_FALLBACK;
   if (!nt || !d || !tau || !qn || !w || !bounds || !theta || !cost || (seeded && !start))
@@ -637,7 +637,13 @@ extern "C" int ddm_fit_lm(int32_t nfit, int32_t nt_max, int32_t K, const int32_t
   p.max_iter = max_iter;
   p.nrefine = nrefine;
   p.tol = tol;
+  p.geometry2d = geometry2d;
+  if (geometry2d) {
+    const cudaError_t te = ddm::isf2d_table(&p.tab);
+    if (te != cudaSuccess) return lm_fail(DDM_ERR_CUDA, "ddm_fit_lm: 2D table: %s", cudaGetErrorString(te));
+  }
   if (on_device) {
+    p.vmag = vmag;
     p.nt = nt; p.d = d; p.tau = tau; p.qn = qn; p.w = w; p.bounds = bounds; p.start = start;
     p.theta = theta; p.cost = cost; p.iters = iters; p.evals = evals; p.status = status;
     int* ctr = nullptr;
@@ -651,7 +657,7 @@ extern "C" int ddm_fit_lm(int32_t nfit, int32_t nt_max, int32_t K, const int32_t
   }
   const size_t nf = (size_t)nfit, nd = nf * nt_max;
   int *dnt = nullptr, *dit = nullptr, *dev = nullptr, *dst = nullptr;
-  float *dd = nullptr, *dtau = nullptr, *dqn = nullptr, *dw = nullptr, *db = nullptr, *ds = nullptr;
+  float *dd = nullptr, *dtau = nullptr, *dqn = nullptr, *dw = nullptr, *db = nullptr, *ds = nullptr, *dv = nullptr;
   double *dth = nullptr, *dc = nullptr;
   cudaError_t e = cudaSuccess;
   auto step = [&](cudaError_t x) { if (e == cudaSuccess) e = x; };
@@ -662,6 +668,7 @@ extern "C" int ddm_fit_lm(int32_t nfit, int32_t nt_max, int32_t K, const int32_t
   step(stage_in(&dw, w, nf, s));
   step(stage_in(&db, bounds, nf * 6, s));
   if (seeded) step(stage_in(&ds, start, nf * 4, s));
+  if (vmag) step(stage_in(&dv, vmag, nf, s));
   step(stage_in<double>(&dth, nullptr, nf * 6, s));
   step(stage_in<double>(&dc, nullptr, nf, s));
   step(stage_in<int>(&dit, nullptr, nf, s));
@@ -671,7 +678,7 @@ extern "C" int ddm_fit_lm(int32_t nfit, int32_t nt_max, int32_t K, const int32_t
   step(stage_in<int>(&ctr, nullptr, 1, s));
   step(cudaMemsetAsync(ctr, 0, sizeof(int), s));
   if (e == cudaSuccess) {
-    p.nt = dnt; p.d = dd; p.tau = dtau; p.qn = dqn; p.w = dw; p.bounds = db; p.start = ds;
+    p.nt = dnt; p.d = dd; p.tau = dtau; p.qn = dqn; p.w = dw; p.bounds = db; p.start = ds; p.vmag = dv;
     p.theta = dth; p.cost = dc; p.iters = dit; p.evals = dev; p.status = dst; p.counter = ctr;
     step(ddm::launch_lm(p, s));
     step(cudaMemcpyAsync(theta, dth, sizeof(double) * nf * 6, cudaMemcpyDeviceToHost, s));
@@ -680,12 +687,21 @@ extern "C" int ddm_fit_lm(int32_t nfit, int32_t nt_max, int32_t K, const int32_t
     if (evals) step(cudaMemcpyAsync(evals, dev, sizeof(int) * nf, cudaMemcpyDeviceToHost, s));
     if (status) step(cudaMemcpyAsync(status, dst, sizeof(int) * nf, cudaMemcpyDeviceToHost, s));
   }
-  for (void* ptr : {(void*)dnt, (void*)dd, (void*)dtau, (void*)dqn, (void*)dw, (void*)db, (void*)ds,
+  for (void* ptr : {(void*)dnt, (void*)dd, (void*)dtau, (void*)dqn, (void*)dw, (void*)db, (void*)ds, (void*)dv,
                     (void*)dth, (void*)dc, (void*)dit, (void*)dev, (void*)dst, (void*)ctr})
     if (ptr) cudaFreeAsync(ptr, s);
   step(cudaStreamSynchronize(s));
   if (e != cudaSuccess) return lm_fail(DDM_ERR_CUDA, "ddm_fit_lm: %s", cudaGetErrorString(e));
   return DDM_OK;
+}
+
+extern "C" int ddm_fit_lm(int32_t nfit, int32_t nt_max, int32_t K, const int32_t* nt, const float* d,
+                          const float* tau, const float* qn, const float* w, const float* bounds,
+                          const float* start, int32_t mode, int32_t max_iter, double tol,
+                          int32_t nrefine, double* theta, double* cost, int32_t* iters, int32_t* evals,
+                          int32_t* status, int32_t on_device, void* stream) {
+  return ddm_fit_lm_model(nfit, nt_max, K, nt, d, tau, qn, w, bounds, start, mode, max_iter, tol, nrefine, 0,
+                          nullptr, theta, cost, iters, evals, status, on_device, stream);
 }
 
 // ------------------------------------------------------------------ model curves

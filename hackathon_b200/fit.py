@@ -124,14 +124,17 @@ def _check(rc):
 
 
 def fit_lm(d, tau, qn, w, bnds, mode="plain", start=None, nt=None, max_iter=200, tol=1e-10,
-           nrefine=3):
+           nrefine=3, geometry="3d", vmag=None):
     """Batched LM over independent bins (host arrays in, host arrays out).
 
     d, tau [nfit, nt_max]; qn [nfit, K]; w [nfit]; bnds [6] or [nfit, 6];
     start [nfit, 4] = (alpha, vbar, Z, D) for mode "seeded"; nt [nfit] lags
     used per fit (default nt_max). mode "brownian" fits the Brownian model
     alone, A (1 - <exp(-D q^2 tau)>) + B per bin (fitBrownian's search,
-    motility_fit.js:500-536, one D per bin)."""
+    motility_fit.js:500-536, one D per bin). geometry "2d" uses the in-plane
+    swimmer kernel (swimmerKernel, motility_fit.js:227-229); vmag [nfit] (or
+    a scalar) multiplies the model by J0(q |V| tau) for a known drift speed
+    (modelColumn :426)."""
     lib = _lib.load()
     d = np.ascontiguousarray(d, np.float32)
     nfit, nt_max = d.shape
@@ -151,9 +154,13 @@ def fit_lm(d, tau, qn, w, bnds, mode="plain", start=None, nt=None, max_iter=200,
     iters = np.zeros(nfit, np.int32)
     evals = np.zeros(nfit, np.int32)
     status = np.zeros(nfit, np.int32)
+    vm = None if vmag is None else np.ascontiguousarray(np.broadcast_to(vmag, (nfit,)), np.float32)
+    if geometry not in ("3d", "2d"):
+        raise ValueError(f"geometry must be '3d' or '2d', not {geometry!r}")
     p = lambda a: C.c_void_p(a.ctypes.data) if a is not None else None  # noqa: E731
-    _check(lib.ddm_fit_lm(nfit, nt_max, K, p(ntv), p(d), p(tau), p(qn), p(w), p(bnds), p(st), m,
-                          max_iter, tol, nrefine, p(theta), p(cost), p(iters), p(evals), p(status), 0, None))
+    _check(lib.ddm_fit_lm_model(nfit, nt_max, K, p(ntv), p(d), p(tau), p(qn), p(w), p(bnds), p(st), m,
+                                max_iter, tol, nrefine, 1 if geometry == "2d" else 0, p(vm), p(theta), p(cost),
+                                p(iters), p(evals), p(status), 0, None))
     return FitResult(theta, cost, iters, evals, status)
 
 

@@ -7,11 +7,13 @@ caller src/main.ts:325-353 (runFit: one waiter per id; if the worker fails,
 every pending fit and every later one runs on the calling thread).
 
 Here the worker is a thread that runs the library's decision layer
-(ddm_analyze_motility, host FP64, the reference's analyzeMotility): the ctypes
-call releases the GIL, so a fit overlaps the caller's ingest and temporal
-launches the way the reference's Worker keeps fits off the frame-delivery
-thread. Replies keep the reference's shape; results are the dicts
-hackathon_b200.motility.analyze_motility returns.
+(ddm_analyze_motility: the reference's analyzeMotility with its model fits on
+the GPU): the ctypes call releases the GIL, so a fit overlaps the caller's
+ingest and temporal launches the way the reference's Worker keeps fits off
+the frame-delivery thread. Replies keep the reference's shape; results are
+the dicts hackathon_b200.motility.analyze_motility returns. The analysis
+function can be replaced (FitWorker(analyze=...)), e.g. to serve the
+protocol where no GPU is present.
 
 Extension: opt["binFits"] = "plain" | "seeded" adds per-q-bin fits from the
 batched GPU LM (ddm_fit_lm, one warp per bin) to the reply's result as
@@ -41,11 +43,11 @@ class WorkerFailed(RuntimeError):
     """The worker thread stopped; fits run on the calling thread."""
 
 
-def handle(radial, opt, surrogate=None):
+def handle(radial, opt, surrogate=None, analyze=None):
     """One request: analyzeMotility(radial, opt) (+ binFits when asked)."""
     opt = dict(opt or {})
     kw = {k: opt[k] for k in _OPT_KEYS if k in opt}
-    result = analyze_motility(radial, **kw)
+    result = (analyze or analyze_motility)(radial, **kw)
     mode = opt.get("binFits")
     if mode:
         result["binFits"] = bin_fits(radial, opt, mode, surrogate)
@@ -103,10 +105,11 @@ class FitWorker:
     is main.ts runFit: it returns a Future of the result dict; an {error}
     reply becomes the Future's exception."""
 
-    def __init__(self, on_message=None, surrogate=None):
+    def __init__(self, on_message=None, surrogate=None, analyze=None):
         self._q = queue.Queue()
         self._on_message = on_message
         self._surrogate = surrogate
+        self._analyze = analyze
         self._waiters = {}
         self._lock = threading.Lock()
         self._ids = itertools.count(1)
@@ -135,7 +138,7 @@ class FitWorker:
     def _serve(self, msg):
         rid = msg.get("id") if isinstance(msg, dict) else None
         try:
-            result = handle(msg["radial"], msg.get("opt"), self._surrogate)
+            result = handle(msg["radial"], msg.get("opt"), self._surrogate, self._analyze)
         except Exception as e:  # the reference posts String(e.stack || e)
             self._reply({"id": rid, "error": "".join(traceback.format_exception(e)).rstrip()})
             return
@@ -164,7 +167,7 @@ class FitWorker:
         the worker has failed, computed here (main.ts:346-353)."""
         fut = Future()
         if self.failed:
-            fut.set_result(handle(radial, opt, self._surrogate))
+            fut.set_result(handle(radial, opt, self._surrogate, self._analyze))
             return fut
         rid = next(self._ids)
         with self._lock:
@@ -178,7 +181,7 @@ class FitWorker:
         try:
             return self.run_fit(radial, opt).result(timeout)
         except WorkerFailed:
-            return handle(radial, opt, self._surrogate)
+            return handle(radial, opt, self._surrogate, self._analyze)
 
     def close(self):
         self._q.put(None)

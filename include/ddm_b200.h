@@ -207,12 +207,18 @@ int ddm_set_tuning(ddm_engine *h, int32_t chunk, int32_t unit_size, int32_t vari
 int64_t ddm_kernel_launches(const ddm_engine *h);
 
 /* ---------------------------------------------------------------------------
- * Decision layer: analyzeMotility (motility-ddm/src/motility_fit.js:853-990)
- * on a Radial record -- Brownian, Brownian+drift and swimmer fits (VarPro +
- * bounded Nelder-Mead, the reference's start sets), phase drift, temporal
+ * Decision layer: analyzeMotility (motility-ddm/src/motility_fit.js:870-990)
+ * on a Radial record -- Brownian, Brownian+drift and swimmer fits of ONE
+ * parameter set shared by all q-bins (the reference's VarPro objective,
+ * evalModel :450-474, with its start sets: fitBrownian :500-536,
+ * fitBrownianDrift :545-568, fitSwimmer :577-611), phase drift, temporal
  * structure index, BIC with the residual autocorrelation, q-scaling, and the
- * five gates -> verdict. Host FP64 like the reference's fit worker; the
- * Radial record is the one ddm_read_radial returns with the engine's bins. */
+ * five gates -> verdict. The fits run on the current CUDA device in FP64:
+ * scans and start sets as parallel jobs, each search a bounded
+ * Levenberg-Marquardt iteration by one thread-block cluster (the reference
+ * uses Nelder-Mead on one CPU thread). The Radial record is the one
+ * ddm_read_radial returns with the engine's bins. The first call on a device
+ * builds the 2D swimmer-ISF table (a kernel launch and a synchronisation). */
 typedef struct ddm_radial_view {
   int32_t N, NB, L, knodes;
   const double *kCenter;   /* [NB] */
@@ -228,6 +234,9 @@ typedef struct ddm_motility_options {
   int32_t geometry2d;      /* 0: 3D swimmers ('3d'), 1: in-plane ('2d') */
   int32_t exposureLocked;  /* 0 gives UNLOCKED_EXPOSURE (gate G5) */
   double swimMin;          /* GATES.SWIM_MIN_UM_S, 2 in the reference */
+  int32_t optimizer;       /* 0: the reference's searches (golden section, Nelder-Mead);
+                              1: bounded Levenberg-Marquardt from the same starts (extension) */
+  int32_t reserved;
 } ddm_motility_options;
 
 typedef struct ddm_motility_fit {
@@ -254,6 +263,37 @@ typedef struct ddm_motility_result {
 
 int ddm_analyze_motility(const ddm_radial_view *radial, const ddm_motility_options *opt,
                          ddm_motility_result *out);
+/* analyzeMotility of n records at once (no counterpart in the reference,
+ * which analyses one record per worker message, motility_fit.js:996-1004):
+ * each stage of the analysis runs the device jobs of every record in one
+ * launch. out[i] equals ddm_analyze_motility(&radials[i], &opts[i]). */
+int ddm_analyze_motility_batch(int32_t n, const ddm_radial_view *radials,
+                               const ddm_motility_options *opts, ddm_motility_result *out);
+/* The swimmer self-ISF kernels as the fits evaluate them, for n points of
+ * host arrays x = q vbar tau and Z: g, x dg/dx and Z dg/dZ (the last two may
+ * be NULL). geometry2d 0: isf3d (motility_fit.js:140-144); 1: the 2D kernel
+ * isf2d (:152-159) read from the device table that replaces the reference's
+ * isf2dFast (:168-220). */
+int ddm_isf_eval(int32_t n, int32_t geometry2d, const double *x, const double *Z,
+                 double *g, double *xdgdx, double *Zdgdz);
+/* The host half of the analysis on its own (no device needed). The q-bins
+ * are those prepare() keeps (motility_fit.js:383-401): ddm_prepared_bins
+ * returns their Radial indices (bins may be NULL to query the count; up to
+ * NB values) and the number of fit lags (lagGrid, :358-369). */
+int ddm_prepared_bins(const ddm_radial_view *radial, const ddm_motility_options *opt,
+                      int32_t *bins, int32_t *nbins, int32_t *nlags);
+/* temporalStructureIndex (:735-749); NaN for an invalid record. */
+double ddm_temporal_structure_index(const ddm_radial_view *radial);
+/* estimateDrift (:672-725). lag_mask [nbins][L] (prepared bins; 1 = use the
+ * lag) restricts the drift sums to lags where the swimmer ISF has decayed,
+ * NULL = every lag. out[8] = Vx, Vy, |V|, sigma, angle (deg), significant,
+ * pairs, samples. */
+int ddm_estimate_drift(const ddm_radial_view *radial, const ddm_motility_options *opt,
+                       const uint8_t *lag_mask, double *out);
+/* scalingExponent's mu (:771-804) from per-prepared-bin amplitudes
+ * amps[2*i] = A, amps[2*i+1] = B; NaN when fewer than 3 bins cross half. */
+int ddm_scaling_exponent(const ddm_radial_view *radial, const ddm_motility_options *opt,
+                         const double *amps, double *mu);
 
 /* ---------------------------------------------------------------------------
  * Batches: many videos of uneven size and frame count analysed together (no
@@ -306,7 +346,8 @@ int ddm_batch_launch_graph(ddm_batch *b);
  * bin,
  *   min sum_j (w (A c(tau_j) + B - d_j))^2,
  *   c = 1 - <exp(-D q^2 tau) (1 - alpha + alpha g(q vbar tau; Z))>_nodes
- * (modelColumn, motility_fit.js:417-432, 3D Schulz swimmer ISF g) over
+ * (modelColumn, motility_fit.js:417-432, 3D Schulz swimmer ISF g; see
+ * ddm_fit_lm_model for the 2D kernel and the drift factor) over
  * theta = (A, B, alpha, ln vbar, ln Z, ln D), A, B >= 0, alpha in [0, 1], the
  * rest clamped to bounds[6*i..] = (vmin, vmax, Zmin, Zmax, Dmin, Dmax)
  * (bounds(), :480-491). Model in FP32, normal equations (J^T J + lambda I,
@@ -337,6 +378,19 @@ int ddm_fit_lm(int32_t nfit, int32_t nt_max, int32_t K, const int32_t *nt, const
                const float *start, int32_t mode, int32_t max_iter, double tol, int32_t nrefine,
                double *theta, double *cost, int32_t *iters, int32_t *evals, int32_t *status,
                int32_t on_device, void *stream);
+/* ddm_fit_lm with the rest of modelColumn (motility_fit.js:417-432): the
+ * swimmer kernel of the geometry (geometry2d 0: isf3d :140-144; 1: the 2D
+ * kernel isf2d :152-159 from the device table, swimmerKernel :227-229) and
+ * the drift factor J0(q |V| tau) with vmag[nfit] the known drift speed of
+ * each fit (NULL: no factor; host or device array like the others). The
+ * first 2D call on a device builds the table (a kernel launch and a
+ * synchronisation: make it before any stream capture). ddm_fit_lm is this
+ * call with geometry2d = 0 and vmag = NULL. */
+int ddm_fit_lm_model(int32_t nfit, int32_t nt_max, int32_t K, const int32_t *nt, const float *d,
+                     const float *tau, const float *qn, const float *w, const float *bounds,
+                     const float *start, int32_t mode, int32_t max_iter, double tol, int32_t nrefine,
+                     int32_t geometry2d, const float *vmag, double *theta, double *cost,
+                     int32_t *iters, int32_t *evals, int32_t *status, int32_t on_device, void *stream);
 
 /* Model curves for training and evaluation data (no reference counterpart):
  * y[i][j] = (A c(tau_j) + B) (1 + noise * n_ij), c the model column above

@@ -14,7 +14,8 @@ the bins so that it finishes in seconds:
     D within 1e-4 of each bin's scale, P within 1e-5 relative;
   - temporal stage alone: the oracle's per-mode D, C, P from the engine's own
     history on every 5th mode of those bins: |dD|/2P, |dC|/P, |dP|/P at
-    p99 <= 1e-4 (the reference harness's metrics, harness.ts:115-151);
+    p99 <= 1e-4 (the reference harness's metrics, harness.ts:115-151), for
+    the two kernels that write full per-mode outputs;
   - D(q, 0) = 0 and the fused record equals the record of the full outputs.
 """
 import numpy as np
@@ -101,8 +102,10 @@ def test_headline_radial_vs_oracle(headline, variant, kernel):
     assert np.allclose(rg.P[sel], ro["P"], rtol=1e-5, atol=0)
 
 
-@pytest.mark.parametrize("variant,kernel", VARIANTS, ids=[v for v, _ in VARIANTS])
+@pytest.mark.parametrize("variant,kernel", VARIANTS[:2], ids=[v for v, _ in VARIANTS[:2]])
 def test_headline_modes_vs_oracle(headline, variant, kernel):
+    """Per-mode outputs (readTemporalFull). The radix-16 kernel writes only
+    the fused radial record, so full outputs come from the other two."""
     eng = headline["eng"]
     order, mask = headline["order"], headline["mask"]
     _use(eng, variant)

@@ -36,15 +36,22 @@ constexpr int LM_NP = 6;
 constexpr int LM_MAX_LAGS = 128;   // 4 per lane
 constexpr int LM_MAX_NODES = 8;
 constexpr int LM_WARPS = 8;        // fits per 256-thread CTA
+// CTAs per SM the register budget is sized for: 3 (80 registers). Measured on
+// B200 over 1e5 analytic curves (q-fits/s, plain / seeded from the truth):
+// 1 CTA (210 registers) 113K / 759K, 2 CTAs 107K / 984K, 3 CTAs 104K / 1.07M.
+#ifndef LM_MIN_BLOCKS
+#define LM_MIN_BLOCKS 3
+#endif
 
 // Precision-generic math for the model: FP32 for the bulk of the
 // iterations, FP64 for the final refinement.
 __device__ __forceinline__ float m_exp(float x) { return expf(x); }
 __device__ __forceinline__ double m_exp(double x) { return exp(x); }
 
-struct LmProblem {
+template <bool G2D>
+struct LmProblemT {
+  static constexpr bool g2d_kernel = G2D;
   int nt, K;
-  int g2d;             // swimmer kernel: 0 3D, 1 2D (table)
   float V;             // drift speed |V| of the J0 factor (0: none)
   Isf2dTable tab;
   float w;
@@ -57,9 +64,9 @@ __device__ __forceinline__ float m_j0(float y) { return j0f(y); }
 __device__ __forceinline__ double m_j0(double y) { return j0(y); }
 
 // The swimmer kernel of the fit's geometry: g, x dg/dx, Z dg/dZ.
-template <typename R>
-__device__ __forceinline__ void swim_isf(const LmProblem& P, R x, R Z, R& g, R& gx, R& gz) {
-  if (P.g2d) {
+template <typename R, class PR>
+__device__ __forceinline__ void swim_isf(const PR& P, R x, R Z, R& g, R& gx, R& gz) {
+  if constexpr (PR::g2d_kernel) {
     double a, b, c;
     isf2d_d(P.tab, (double)x, (double)Z, a, b, c);
     g = (R)a;
@@ -78,7 +85,8 @@ __device__ __forceinline__ T warp_sum(T v) {
 }
 
 // Model column c(tau) at this lane's lags (FP32), 0 beyond nt.
-__device__ __forceinline__ void model_c(const LmProblem& P, int lane, float al, float v, float Z, float D,
+template <class PR>
+__device__ __forceinline__ void model_c(const PR& P, int lane, float al, float v, float Z, float D,
                                         float (&c)[4]) {
   const float iK = 1.f / P.K;
 #pragma unroll
@@ -107,8 +115,8 @@ __device__ __forceinline__ void model_c(const LmProblem& P, int lane, float al, 
 // VarPro amplitudes at fixed nonlinear parameters: the 2-column NNLS of the
 // reference's evalModel (motility_fit.js:450-474) by nnls3's support
 // enumeration (:243-263) over {A}, {B}, {A, B}. Returns the weighted cost.
-template <typename CT>
-__device__ __forceinline__ double varpro_c(const LmProblem& P, int lane, const CT (&c)[4], double& A, double& B) {
+template <typename CT, class PR>
+__device__ __forceinline__ double varpro_c(const PR& P, int lane, const CT (&c)[4], double& A, double& B) {
   double g11 = 0, g12 = 0, h1 = 0, h2 = 0, dd = 0;
 #pragma unroll
   for (int r = 0; r < 4; r++) {
@@ -148,7 +156,8 @@ __device__ __forceinline__ double varpro_c(const LmProblem& P, int lane, const C
   return fmax(best, 0.0) * (double)P.w * (double)P.w;
 }
 
-__device__ __forceinline__ double varpro(const LmProblem& P, int lane, double al, double lv, double lZ,
+template <class PR>
+__device__ __forceinline__ double varpro(const PR& P, int lane, double al, double lv, double lZ,
                                          double lD, double& A, double& B) {
   float c[4];
   model_c(P, lane, (float)al, (float)exp(lv), (float)exp(lZ), (float)exp(lD), c);
@@ -158,7 +167,8 @@ __device__ __forceinline__ double varpro(const LmProblem& P, int lane, double al
 // The Brownian column c(tau) = 1 - <exp(-D q_n^2 tau)> in FP64, for the
 // Brownian-only fit: its golden section walks a valley that can be flat to
 // FP32 rounding (noise-dominated or barely decaying bins).
-__device__ __forceinline__ double varpro_brownian64(const LmProblem& P, int lane, double lD, double& A,
+template <class PR>
+__device__ __forceinline__ double varpro_brownian64(const PR& P, int lane, double lD, double& A,
                                                     double& B) {
   const double D = exp(lD), iK = 1.0 / P.K;
   double c[4];
@@ -177,16 +187,52 @@ __device__ __forceinline__ double varpro_brownian64(const LmProblem& P, int lane
   return varpro_c(P, lane, c, A, B);
 }
 
-// Normal equations at theta: H (upper triangle, 21), g (6), cost; warp-reduced.
-// The model and Jacobian are evaluated in R; the sums are FP64.
-template <typename R>
-__device__ __forceinline__ void lm_normal(const LmProblem& P, const double (&th)[LM_NP], int lane,
-                                          double (&H)[21], double (&gr)[LM_NP], double& cost) {
+// Normal equations, spread over the warp. The 28 sums (J^T J lower triangle,
+// J^T r, cost) are laid out in 32 slots -- slot tri(i, j) = i (i + 1) / 2 + j
+// for J^T J (i >= j), 21 + i for J^T r, 27 for the cost -- and reduced with a
+// reduce-scatter (recursive halving over the xor partners 16, 8, 4, 2, 1:
+// 31 shuffles): lane l ends holding the total of slot l. Nothing else of the
+// normal equations lives in every lane, which keeps the kernel's registers
+// low enough for several CTAs per SM; the Cholesky factorisation below works
+// on these lane-held entries through shuffles.
+constexpr int LM_SLOT_G = 21, LM_SLOT_COST = 27;
+__device__ __forceinline__ constexpr int tri(int i, int j) { return i * (i + 1) / 2 + j; }
+
+__device__ __forceinline__ double reduce_scatter32(double (&v)[32], int lane) {
+  double h16[16], h8[8], h4[4], h2[2];
+#pragma unroll
+  for (int i = 0; i < 16; i++) {
+    const bool up = lane & 16;
+    h16[i] = (up ? v[i + 16] : v[i]) + __shfl_xor_sync(0xffffffffu, up ? v[i] : v[i + 16], 16);
+  }
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    const bool up = lane & 8;
+    h8[i] = (up ? h16[i + 8] : h16[i]) + __shfl_xor_sync(0xffffffffu, up ? h16[i] : h16[i + 8], 8);
+  }
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    const bool up = lane & 4;
+    h4[i] = (up ? h8[i + 4] : h8[i]) + __shfl_xor_sync(0xffffffffu, up ? h8[i] : h8[i + 4], 4);
+  }
+#pragma unroll
+  for (int i = 0; i < 2; i++) {
+    const bool up = lane & 2;
+    h2[i] = (up ? h4[i + 2] : h4[i]) + __shfl_xor_sync(0xffffffffu, up ? h4[i] : h4[i + 2], 2);
+  }
+  const bool up = lane & 1;
+  return (up ? h2[1] : h2[0]) + __shfl_xor_sync(0xffffffffu, up ? h2[0] : h2[1], 1);
+}
+
+// The normal equations at theta; returns this lane's slot total. The model
+// and Jacobian are evaluated in R; the sums are FP64.
+template <typename R, class PR>
+__device__ __forceinline__ double lm_normal(const PR& P, const double (&th)[LM_NP], int lane) {
   const R A = (R)th[0], B = (R)th[1], al = (R)th[2];
   const R v = (R)exp(th[3]), Z = (R)exp(th[4]), D = (R)exp(th[5]);
-  for (int i = 0; i < 21; i++) H[i] = 0.0;
-  for (int i = 0; i < LM_NP; i++) gr[i] = 0.0;
-  cost = 0.0;
+  double acc[32];
+#pragma unroll
+  for (int i = 0; i < 32; i++) acc[i] = 0.0;
   const R iK = R(1) / R(P.K);
   const R w = (R)P.w;
 #pragma unroll
@@ -217,63 +263,53 @@ __device__ __forceinline__ void lm_normal(const LmProblem& P, const double (&th)
     J[3] = (double)(-w * A * sgx * iK);
     J[4] = (double)(-w * A * sgz * iK);
     J[5] = (double)(w * A * sdD * iK);
-    cost += rr * rr;
-    int k = 0;
+    acc[LM_SLOT_COST] += rr * rr;
 #pragma unroll
     for (int a = 0; a < LM_NP; a++) {
-      gr[a] += J[a] * rr;
+      acc[LM_SLOT_G + a] += J[a] * rr;
 #pragma unroll
-      for (int b = a; b < LM_NP; b++) H[k++] += J[a] * J[b];
+      for (int b = 0; b <= a; b++) acc[tri(a, b)] += J[a] * J[b];
     }
   }
-#pragma unroll
-  for (int i = 0; i < 21; i++) H[i] = warp_sum(H[i]);
-#pragma unroll
-  for (int i = 0; i < LM_NP; i++) gr[i] = warp_sum(gr[i]);
-  cost = warp_sum(cost);
+  return reduce_scatter32(acc, lane);
 }
 
-// (H + lambda diag H) delta = -g by Cholesky; false if not positive definite.
-__device__ __forceinline__ bool lm_solve(const double (&H)[21], const double (&gr)[LM_NP], double lambda,
+__device__ __forceinline__ double lm_cost(double hv) { return __shfl_sync(0xffffffffu, hv, LM_SLOT_COST); }
+
+// (H + lambda diag H) delta = -g by Cholesky on the lane-held entries: lane
+// tri(i, j) (< 21) owns entry (i, j) of the lower triangle, (li, lj) its
+// position; pivots, column entries and the triangular solves travel by
+// shuffles, and every lane ends with the same delta. False if not positive
+// definite (the same on every lane).
+__device__ __forceinline__ bool lm_solve(double hv, double lambda, int lane, int li, int lj,
                                          double (&delta)[LM_NP]) {
-  double M[LM_NP][LM_NP];
-  int k = 0;
+  const bool in = lane < LM_SLOT_G;
+  double a = hv;
+  if (in && li == lj) a += lambda * (a > 0 ? a : 1e-30);
 #pragma unroll
-  for (int a = 0; a < LM_NP; a++)
-#pragma unroll
-    for (int b = a; b < LM_NP; b++) M[a][b] = M[b][a] = H[k++];
-#pragma unroll
-  for (int a = 0; a < LM_NP; a++) M[a][a] += lambda * (M[a][a] > 0 ? M[a][a] : 1e-30);
-  double Lm[LM_NP][LM_NP];
-#pragma unroll
-  for (int i = 0; i < LM_NP; i++) {
-#pragma unroll
-    for (int j = 0; j <= i; j++) {
-      double s = M[i][j];
-#pragma unroll
-      for (int q = 0; q < j; q++) s -= Lm[i][q] * Lm[j][q];
-      if (i == j) {
-        if (!(s > 0)) return false;
-        Lm[i][i] = sqrt(s);
-      } else {
-        Lm[i][j] = s / Lm[j][j];
-      }
-    }
+  for (int k = 0; k < LM_NP; k++) {
+    const double dkk = __shfl_sync(0xffffffffu, a, tri(k, k));
+    if (!(dkk > 0)) return false;
+    const double lkk = sqrt(dkk);
+    if (in && lj == k) a = li == k ? lkk : a / lkk;
+    const double lik = __shfl_sync(0xffffffffu, a, in && li > k ? tri(li, k) : lane);
+    const double ljk = __shfl_sync(0xffffffffu, a, in && lj > k ? tri(lj, k) : lane);
+    if (in && lj > k) a -= lik * ljk;
   }
   double y[LM_NP];
 #pragma unroll
   for (int i = 0; i < LM_NP; i++) {
-    double s = -gr[i];
+    double s = -__shfl_sync(0xffffffffu, hv, LM_SLOT_G + i);
 #pragma unroll
-    for (int q = 0; q < i; q++) s -= Lm[i][q] * y[q];
-    y[i] = s / Lm[i][i];
+    for (int q = 0; q < i; q++) s -= __shfl_sync(0xffffffffu, a, tri(i, q)) * y[q];
+    y[i] = s / __shfl_sync(0xffffffffu, a, tri(i, i));
   }
 #pragma unroll
   for (int i = LM_NP - 1; i >= 0; i--) {
     double s = y[i];
 #pragma unroll
-    for (int q = i + 1; q < LM_NP; q++) s -= Lm[q][i] * delta[q];
-    delta[i] = s / Lm[i][i];
+    for (int q = i + 1; q < LM_NP; q++) s -= __shfl_sync(0xffffffffu, a, tri(q, i)) * delta[q];
+    delta[i] = s / __shfl_sync(0xffffffffu, a, tri(i, i));
   }
   return true;
 }
@@ -282,16 +318,19 @@ __device__ __forceinline__ bool lm_solve(const double (&H)[21], const double (&g
 // set), continuing from lambda; returns the iterations taken.
 // max_reject > 0 ends the phase after that many consecutive rejected steps
 // (used by the FP32 phase, whose cost cannot resolve the last decreases).
-template <typename R>
-__device__ int lm_phase(const LmProblem& P, int lane, double (&th)[LM_NP], double& cost, double& lambda,
+template <typename R, class PR>
+__device__ int lm_phase(const PR& P, int lane, double (&th)[LM_NP], double& cost, double& lambda,
                         int max_iter, double tol, bool& converged, int max_reject = 0) {
-  double H[21], gr[LM_NP];
-  lm_normal<R>(P, th, lane, H, gr, cost);
+  int li = 0;
+  while (tri(li + 1, 0) <= lane) li++;
+  const int lj = lane - tri(li, 0);
+  double hv = lm_normal<R>(P, th, lane);
+  cost = lm_cost(hv);
   int small = 0, it = 0, rejected = 0;
   converged = false;
   for (it = 0; it < max_iter; it++) {
     double delta[LM_NP];
-    if (!lm_solve(H, gr, lambda, delta)) {
+    if (!lm_solve(hv, lambda, lane, li, lj, delta)) {
       lambda *= 4;
       if (lambda > 1e12 || (max_reject && ++rejected >= max_reject)) {
         converged = lambda > 1e12;  // no step lowers the cost: a numerical minimum
@@ -302,17 +341,13 @@ __device__ int lm_phase(const LmProblem& P, int lane, double (&th)[LM_NP], doubl
     double th2[LM_NP];
 #pragma unroll
     for (int a = 0; a < LM_NP; a++) th2[a] = fmin(P.hi[a], fmax(P.lo[a], th[a] + delta[a]));
-    double H2[21], g2[LM_NP], c2;
-    lm_normal<R>(P, th2, lane, H2, g2, c2);
+    const double hv2 = lm_normal<R>(P, th2, lane);
+    const double c2 = lm_cost(hv2);
     if (c2 < cost) {
       const double rel = (cost - c2) / (cost > 0 ? cost : 1e-300);
 #pragma unroll
-      for (int a = 0; a < LM_NP; a++) {
-        th[a] = th2[a];
-        gr[a] = g2[a];
-      }
-#pragma unroll
-      for (int i = 0; i < 21; i++) H[i] = H2[i];
+      for (int a = 0; a < LM_NP; a++) th[a] = th2[a];
+      hv = hv2;
       cost = c2;
       lambda = fmax(lambda / 3, 1e-12);
       rejected = 0;
@@ -339,7 +374,8 @@ __device__ int lm_phase(const LmProblem& P, int lane, double (&th)[LM_NP], doubl
 // the walk early along flat valleys). Returns the iterations taken;
 // `converged` = the FP64 phase stopped at a minimum (the relative-decrease
 // test, or no step lowering the cost any more) rather than at the cap.
-__device__ int lm_run(const LmProblem& P, int lane, double (&th)[LM_NP], double& cost, int max_iter,
+template <class PR>
+__device__ int lm_run(const PR& P, int lane, double (&th)[LM_NP], double& cost, int max_iter,
                       double tol, bool& converged) {
   double lambda = 1e-3;
   bool c32;
@@ -358,8 +394,8 @@ __device__ int lm_run(const LmProblem& P, int lane, double (&th)[LM_NP], double&
 // q-nodes, VarPro amplitudes; a 49-point scan of ln D over its bounds, then
 // golden section (at most 60 steps, to 1e-6 in ln D). Returns ln D;
 // `settled` when the bracket closed.
-template <bool F64>
-__device__ double brownian_search(const LmProblem& P, int lane, int& evals, bool& settled) {
+template <bool F64, class PR>
+__device__ double brownian_search(const PR& P, int lane, int& evals, bool& settled) {
   double A, B;
   auto cost_at = [&](double x) {
     return F64 ? varpro_brownian64(P, lane, x, A, B) : varpro(P, lane, 0.0, P.lo[3], 0.0, x, A, B);
@@ -403,7 +439,8 @@ __device__ double brownian_search(const LmProblem& P, int lane, int& evals, bool
 // The reference's start strategy (fitBrownian, motility_fit.js:500-536;
 // fitSwimmer :577-611) per bin, LM from the best `nrefine` of 64 starts
 // (oracle/lm.c or_lm_fit_plain). Accumulates iterations and evaluations.
-__device__ void plain_fit(const LmProblem& P, int lane, int nrefine, int max_iter, double tol,
+template <class PR>
+__device__ void plain_fit(const PR& P, int lane, int nrefine, int max_iter, double tol,
                           double (&th)[LM_NP], double& cost, int& iters, int& evals, bool& converged) {
   double A, B;
   bool settled;
@@ -458,11 +495,11 @@ __device__ void plain_fit(const LmProblem& P, int lane, int nrefine, int max_ite
   converged = bconv;
 }
 
+template <bool G2D>
 __device__ __noinline__ void lm_one(const LmParams& p, int fit, int lane) {
-  LmProblem P;
+  LmProblemT<G2D> P;
   P.nt = min(p.nt[fit], min(p.nt_max, LM_MAX_LAGS));
   P.K = min(p.K, LM_MAX_NODES);
-  P.g2d = p.geometry2d;
   P.V = p.vmag ? p.vmag[fit] : 0.f;
   P.tab = p.tab;
   P.w = p.w[fit];
@@ -555,14 +592,15 @@ __device__ __noinline__ void lm_one(const LmParams& p, int fit, int lane) {
 // Persistent: each warp takes the next fit from an atomic counter until all
 // are done, so fits of very different cost (a fallback, a slow valley) do
 // not hold a CTA's other warps.
-__global__ void __launch_bounds__(32 * LM_WARPS) lm_kernel(LmParams p) {
+template <bool G2D>
+__global__ void __launch_bounds__(32 * LM_WARPS, LM_MIN_BLOCKS) lm_kernel(LmParams p) {
   const int lane = threadIdx.x & 31;
   for (;;) {
     int fit = 0;
     if (lane == 0) fit = atomicAdd(p.counter, 1);
     fit = __shfl_sync(0xffffffffu, fit, 0);
     if (fit >= p.nfit) return;  // whole warp
-    lm_one(p, fit, lane);
+    lm_one<G2D>(p, fit, lane);
   }
 }
 
@@ -572,10 +610,11 @@ cudaError_t launch_lm(const LmParams& p, cudaStream_t s) {
   int dev = 0, sms = 0, per = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, lm_kernel, 32 * LM_WARPS, 0);
+  auto k = p.geometry2d ? lm_kernel<true> : lm_kernel<false>;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, 32 * LM_WARPS, 0);
   const int need = (p.nfit + LM_WARPS - 1) / LM_WARPS;
   const int wave = sms * (per > 0 ? per : 1);
-  lm_kernel<<<need < wave ? need : wave, 32 * LM_WARPS, 0, s>>>(p);
+  k<<<need < wave ? need : wave, 32 * LM_WARPS, 0, s>>>(p);
   return cudaGetLastError();
 }
 

@@ -1567,7 +1567,32 @@ __global__ void reduce_kernel(ReduceParams p) {
 }
 
 // Radial reduction of full per-mode outputs, one CTA per bin, one thread per
-// lag, modes of the bin in table order (ddm.wgsl:265-322 with FP64 sums).
+// lag, modes of the bin in table order (ddm.wgsl:265-322 with FP64 sums). The
+// mode loop loads RF_AHEAD modes' values before it adds any of them, so that
+// many loads are in flight per thread (the sums still add in table order).
+constexpr int RF_AHEAD = 8;
+
+__device__ __forceinline__ void radial_full_add(double (&s)[PFIELDS], float D, float2 a, float2 c1, bool next,
+                                                int4 e) {
+  s[0] += (double)D;
+  if (next) {
+    const float zr = fmaf(c1.x, a.x, c1.y * a.y);
+    const float zi = fmaf(c1.y, a.x, -c1.x * a.y);
+    const float w = sqrtf(fmaf(zr, zr, zi * zi));
+    if (w > 0.f) {
+      const double wd = w, ph = atan2f(zi, zr), kx = e.y, ky = e.z;
+      s[1] += wd;
+      s[2] += wd * kx * kx;
+      s[3] += wd * kx * ky;
+      s[4] += wd * ky * ky;
+      s[5] += wd * kx * ph;
+      s[6] += wd * ky * ph;
+      s[7] += wd * ph * ph;
+      s[8] += 1.0;
+    }
+  }
+}
+
 __global__ void radial_full_kernel(RadialFullParams p) {
   const int b = blockIdx.x;
   const int L = p.L;
@@ -1578,27 +1603,29 @@ __global__ void radial_full_kernel(RadialFullParams p) {
     double s[PFIELDS];
 #pragma unroll
     for (int c = 0; c < PFIELDS; c++) s[c] = 0.0;
-    for (uint32_t i = i0; i < i1; i++) {
-      const int4 e = p.items[i];
-      const size_t m = (size_t)e.x;
-      s[0] += (double)p.D[m * L + tau];
-      if (tau + 1 < L) {
-        const float2 a = p.C[m * L + tau], c1 = p.C[m * L + tau + 1];
-        const float zr = fmaf(c1.x, a.x, c1.y * a.y);
-        const float zi = fmaf(c1.y, a.x, -c1.x * a.y);
-        const float w = sqrtf(fmaf(zr, zr, zi * zi));
-        if (w > 0.f) {
-          const double wd = w, ph = atan2f(zi, zr), kx = e.y, ky = e.z;
-          s[1] += wd;
-          s[2] += wd * kx * kx;
-          s[3] += wd * kx * ky;
-          s[4] += wd * ky * ky;
-          s[5] += wd * kx * ph;
-          s[6] += wd * ky * ph;
-          s[7] += wd * ph * ph;
-          s[8] += 1.0;
-        }
+    const bool next = tau + 1 < L;
+    uint32_t i = i0;
+    for (; i + RF_AHEAD <= i1; i += RF_AHEAD) {
+      int4 e[RF_AHEAD];
+      float D[RF_AHEAD];
+      float2 a[RF_AHEAD], c1[RF_AHEAD];
+#pragma unroll
+      for (int k = 0; k < RF_AHEAD; k++) e[k] = __ldg(&p.items[i + k]);
+#pragma unroll
+      for (int k = 0; k < RF_AHEAD; k++) {
+        const size_t m = (size_t)e[k].x;
+        D[k] = __ldg(&p.D[m * L + tau]);
+        a[k] = __ldg(&p.C[m * L + tau]);
+        c1[k] = next ? __ldg(&p.C[m * L + tau + 1]) : make_float2(0.f, 0.f);
       }
+#pragma unroll
+      for (int k = 0; k < RF_AHEAD; k++) radial_full_add(s, D[k], a[k], c1[k], next, e[k]);
+    }
+    for (; i < i1; i++) {
+      const int4 e = __ldg(&p.items[i]);
+      const size_t m = (size_t)e.x;
+      radial_full_add(s, __ldg(&p.D[m * L + tau]), __ldg(&p.C[m * L + tau]),
+                      next ? __ldg(&p.C[m * L + tau + 1]) : make_float2(0.f, 0.f), next, e);
     }
     p.oD[(size_t)b * L + tau] = s[0] * inv;
 #pragma unroll

@@ -527,3 +527,48 @@ def test_async_ingest_matches_sync():
     for o in out[1:]:
         for a, b in zip(out[0], o):
             assert np.array_equal(a, b)
+
+
+def test_temporal_sparse_big_256():
+    """The sparse-mask kernel at TPAD 8192 on a 256^2 x 4096 video (82
+    dropped frames, 2 %): radial D on every 4th bin against the oracle's
+    pipeline from the raw frames, and against the transform kernel."""
+    N, T, L, NB = 256, 4096, 128, 16
+    sim = dict(O.BASE, N=N, T=T, seed=31, swimmers=dict(n=40, vbar=20.0, sigma=8.0, geometry="3d"),
+               passive=dict(n=40), dropExact=82)
+    frames, valid, _ = O.simulate(sim)
+    idx = np.nonzero(valid)[0]
+    eng = _engine(N=N, T=T, L=L, NB=NB, kmin=4, kmax=100)
+    try:
+        assert eng.TPAD == 8192
+        eng.ingest_frames(frames[idx], idx)
+        order, mask = O.linear_order(valid)
+        eng.compute_temporal(order, mask)
+        assert eng.last_temporal_kernel == "temporal_sparse_big_kernel"
+        D = eng.read_radial().D2()
+        eng.set_sparse(False)
+        eng.compute_temporal(order, mask)
+        assert eng.last_temporal_kernel == "temporal_big_kernel"
+        D2 = eng.read_radial().D2()
+    finally:
+        eng.destroy()
+    bins = O.make_bins(N, NB, 4, 100)
+    sel = np.arange(0, NB, 4)
+    off = bins["binOffsets"]
+    rows = [bins["binModes"][off[b]:off[b + 1]] for b in sel]
+    sub = dict(bins, NB=len(sel), binModes=np.ascontiguousarray(np.concatenate(rows)),
+               binOffsets=np.concatenate([[0], np.cumsum([len(r) for r in rows])]).astype(np.uint32),
+               nModes=np.ascontiguousarray(bins["nModes"][sel]).astype(np.uint32))
+    hist = np.zeros((N * (N // 2 + 1), T), np.complex128)
+    for c in range(0, idx.size, 256):
+        k = idx[c:c + 256]
+        O.history_ingest(O.luma_of(frames[k]), k.astype(np.int32), T, hist=hist)
+    ro = O.analyze_radial(hist, order, mask, sub, L, TPAD=8192)
+    for i, b in enumerate(sel):
+        sc = ro["D"][i].max()
+        assert sc > 0
+        assert np.abs(D[b] - ro["D"][i]).max() <= 1e-4 * sc, b
+    for b in range(NB):
+        sc = np.abs(D2[b]).max()
+        if sc > 0:
+            assert np.abs(D[b] - D2[b]).max() <= 1e-5 * sc, b

@@ -380,7 +380,7 @@ LARGE_WORKLOAD = ("2048x2048x4096 u16 video: 40,000 blobs sigma 2 px with the 51
                   "dropped frames; TPAD=8192, L=128 lags, 1024 q-bins (kmin 4, kmax 800)")
 
 
-def run_large(args, rank, world, dist):
+def run_large(args, rank, world, dist, quiet=False):
     """The large streamed configuration: one 2048^2 x 4096 video per GPU
     (68.8 GB history). value: frames already in HBM; e2e: the frames streamed
     from host memory through the engine's pinned staging, radial read back.
@@ -450,6 +450,8 @@ def run_large(args, rank, world, dist):
     ms_step = R.max_over_ranks(ms, dist, device="cuda") / args.steps
     value = R.weak_scaling_throughput(T, ms_step, world)
     fused = eng.read_radial()
+    fused_bins = eng.bins
+    large_tk = eng.last_temporal_kernel
 
     # full-size consistency: the full-output path's radial equals the fused one
     eng.compute_temporal(order, tmask, full=True)
@@ -486,6 +488,44 @@ def run_large(args, rank, world, dist):
         e2e = {"value": R.weak_scaling_throughput(T * args.e2e_steps, ms_e2e, world), "unit": "frames/s",
                "h2d_bytes_per_step": int(need), "d2h_bytes_per_step": rad_bytes,
                "host_memory": "pinned" if pinned else "pageable, staged through the engine's pinned ring"}
+        banded = None
+        if args.band_budget_gb > 0:
+            # the same video with the history held one band of spectrum columns
+            # at a time, sized to the stated budget: per band the frames
+            # stream from host memory through the spatial pass again
+            eng.destroy()
+            eng = None
+            torch.cuda.empty_cache()
+            budget = int(args.band_budget_gb * 2**30)
+            beng = H.DdmEngine.create_banded(budget, N=N, T=T, TPAD=g["TPAD"], L=L, NB=NB, kmin=g["KMIN"],
+                                             kmax=g["KMAX"])
+            beng.set_spatial_mask(synth.hot_mask(spec))
+            beng.set_tuning(tune["best_chunk"], tune["best_unit"], tune["best_variant"])
+            beng.set_stream(stream.cuda_stream)
+            nbands, bcols = beng.bands
+            beng.analyze_banded(host, slots, order, tmask, scale)  # warm
+            torch.cuda.synchronize()
+            b0, b1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            b0.record(stream)
+            beng.analyze_banded(host, slots, order, tmask, scale)
+            b1.record(stream)
+            torch.cuda.synchronize()
+            ms_b = R.max_over_ranks(b0.elapsed_time(b1), dist, device="cuda")
+            rb = beng.read_radial()
+            Db = rb.D2()
+            banded = {"what": "the history held one band of spectrum columns at a time (ddm_create_banded), "
+                              "the frames streamed from host memory through the spatial pass once per band",
+                      "history_budget_bytes": budget, "bands": nbands, "band_columns": bcols,
+                      "history_bytes_on_device": int(bcols) * N * T * 8,
+                      "value": R.weak_scaling_throughput(T, ms_b, world), "unit": "frames/s",
+                      "ms_per_video": ms_b, "h2d_bytes_per_step": int(need) * nbands,
+                      "host_memory": "pinned" if pinned else "pageable",
+                      "checks": {"banded_vs_resident_D_max_rel": float(
+                          (np.abs(Db - D1) / np.where(sc > 0, sc, 1)).max()),
+                                 "banded_vs_resident_P_max_rel": float(
+                          np.abs(rb.P / np.where(fused.P > 0, fused.P, 1) - 1)[fused.P > 0].max())}}
+            beng.destroy()
+        e2e["banded"] = banded
         del host
     else:
         e2e = {"value": None, "unit": "frames/s",
@@ -493,11 +533,11 @@ def run_large(args, rank, world, dist):
                f"host memory {avail / 2**30:.0f} GiB < 1.5 x video"}
 
     peak, peak_kind = _peaks()
-    nbinned = int(eng.bins["binOffsets"][-1])
-    sp_bytes = T * (N * N * 2 + eng.modes * BYTES_PER_MODE_SLOT)
+    nbinned = int(fused_bins["binOffsets"][-1])
+    sp_bytes = T * (N * N * 2 + N * (N // 2 + 1) * BYTES_PER_MODE_SLOT)
     tm_bytes = nbinned * T * BYTES_PER_MODE_SLOT
     TP = g["TPAD"]
-    tk = eng.last_temporal_kernel  # 1.5 transforms per mode for the sparse-mask kernels, else 2.5
+    tk = large_tk  # 1.5 transforms per mode for the sparse-mask kernels, else 2.5
     per_mode = 1.5 if tk in ("temporal_sparse_kernel", "temporal_sparse_big_kernel") else 2.5
     stages = {"spatial": {"ms": t_sp, "bytes": sp_bytes, "GBps": sp_bytes / (t_sp * 1e6),
                           "gflop": T * (N + 1) * 5 * N * np.log2(N) / 1e9},
@@ -510,6 +550,7 @@ def run_large(args, rank, world, dist):
     roof = {"bound": "hbm", "kernel": tk, "achieved": tm["GBps"], "peak": peak, "unit": "GB/s",
             "frac": tm["frac"], "peak_source": peak_kind, "traffic": None, "algorithmic_bytes": tm_bytes,
             "stages": stages}
+    line = None
     if rank == 0:
         metric = LARGE_METRIC if (N, T) == (LARGE["N"], LARGE["T"]) else \
             f"DDM frames/s at {N}²×{T} (large streamed run, reduced)"
@@ -518,13 +559,16 @@ def run_large(args, rank, world, dist):
                 "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic (seeded GPU generator, hackathon_b200/synth.py large())",
                 "config": {"workload": LARGE_WORKLOAD, **{k.lower(): v for k, v in g.items()},
-                           "binned_modes": nbinned, "history_bytes": eng.modes * T * 8,
+                           "binned_modes": nbinned, "history_bytes": N * (N // 2 + 1) * T * 8,
                            "l2": "inputs larger than L2", "generation_s": t_gen,
                            "autotuned": {"chunk": tune["best_chunk"], "unit": tune["best_unit"],
                                          "temporal_variant": tune["best_variant"]}},
                 "e2e": e2e, "gpu_launches": int(launches), "roofline": roof, "clocks": clk, "checks": checks}
-        print(json.dumps(line), flush=True)
-    eng.destroy()
+        if not quiet:
+            print(json.dumps(line), flush=True)
+    if eng is not None:
+        eng.destroy()
+    return line
 
 
 BATCH_METRIC = "DDM frames/s, 48 uneven videos in one persistent launch"
@@ -685,6 +729,10 @@ def main():
     ap.add_argument("--workload", default="config2", choices=["config2", "large", "batch", "surrogate"],
                     help="large: one 2048^2 x 4096 video per GPU (68.8 GB history), its own JSON line")
     ap.add_argument("--frames", type=int, default=0, help="large workload: frames per video (default 4096)")
+    ap.add_argument("--band-budget-gb", type=float, default=24.0,
+                    help="large workload: device history budget of the banded streamed run (0: skip it)")
+    ap.add_argument("--no-large", action="store_true",
+                    help="skip the large streamed run nested in the 512^2 x 1024 line")
     ap.add_argument("--roi", type=int, default=0, help="large workload: ROI size (default 2048)")
     ap.add_argument("--videos", type=int, default=0,
                     help="batch workload: number of videos (48); surrogate: cap on pipeline videos (2000)")
@@ -950,6 +998,27 @@ def main():
         fr = frames.view(torch.int16).cpu().numpy().view(np.uint16)
         cpu = cpu_baseline(fr, valid, mask_roi, gpu_radial=radial, one_core=True, reps=3)
 
+    # the large streamed configuration (2048^2 x 4096, resident and banded),
+    # summarised in this line so that one run records both workloads
+    large = None
+    eng.destroy()
+    eng = None
+    if rank == 0 and world == 1 and not args.no_large:
+        del frames
+        torch.cuda.empty_cache()
+        la = argparse.Namespace(**vars(args))
+        la.steps, la.warmup, la.e2e_steps = 2, 3, 1
+        try:
+            ll = run_large(la, 0, 1, None, quiet=True)
+            large = {k: ll[k] for k in ("metric", "value", "unit", "ms_per_step", "e2e", "checks", "clocks",
+                                        "gpu_launches")}
+            large["roofline"] = {k: ll["roofline"][k] for k in ("kernel", "achieved", "peak", "frac", "unit")}
+            large["stages"] = {k: {"ms": v["ms"], "frac": v["frac"]} for k, v in ll["roofline"]["stages"].items()}
+            large["config"] = {k: ll["config"][k] for k in ("workload", "history_bytes", "binned_modes",
+                                                            "generation_s")}
+        except Exception as e:  # e.g. too little host memory for the pinned video
+            large = {"unavailable": f"{type(e).__name__}: {str(e)[:200]}"}
+
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
@@ -971,10 +1040,12 @@ def main():
                 "cpu_baseline": cpu,
                 "checks": checks,
                 "motility": motility,
+                "large": large,
                 "binned_modes": nbinned,
                 "fit": fit}
         print(json.dumps(line), flush=True)
-    eng.destroy()
+    if eng is not None:
+        eng.destroy()
     if dist:
         dist.barrier()
         dist.destroy_process_group()

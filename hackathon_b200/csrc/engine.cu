@@ -87,6 +87,18 @@ struct ddm_engine {
   float *d_fullD = nullptr, *d_fullP = nullptr;
   float2 *d_fullC = nullptr;
   bool full_valid = false, radial_valid = false;
+
+  // banded analysis (ddm_create_banded): the history holds band_w spectrum
+  // columns of every row at a time; each band has its own work units
+  struct Band {
+    int kb0 = 0, nkb = 0, nunits = 0;
+    int4 *d_items = nullptr, *d_units = nullptr;
+    int *d_bin_units = nullptr;
+  };
+  int band_w = 0;            // columns per history row; 0 = the whole half-plane (NH)
+  std::vector<Band> bands;
+  int cur_kb0 = 0, cur_nkb = 0;  // the band the spatial pass writes (0, 0: all)
+  bool in_banded = false;        // inside ddm_analyze_banded
 };
 
 static int fail(ddm_engine *h, int code, const char *fmt, ...) {
@@ -144,6 +156,9 @@ static void release(ddm_engine *h) {
     if (p) cudaFree(p);
   for (void *p : h->d_stage)
     if (p) cudaFree(p);
+  for (auto &b : h->bands)
+    for (void *p : {(void *)b.d_items, (void *)b.d_units, (void *)b.d_bin_units})
+      if (p) cudaFree(p);
   if (h->h_meta) cudaFreeHost(h->h_meta);
   for (int i = 0; i < NSTAGE; i++) {
     if (h->ready_ev[i]) cudaEventDestroy(h->ready_ev[i]);
@@ -220,6 +235,45 @@ static int build_units(ddm_engine *h, int U = 0) {
   return DDM_OK;
 }
 
+// Work units of each band of a banded engine: the binned modes whose column
+// kx lies in the band, renumbered to the band's history rows (mode (ky, kx)
+// -> ky * band_w + kx - kb0 * KB), in runs of up to unit_size modes inside
+// one bin, bins in order -- the fused path's units restricted to the band.
+static int build_band_units(ddm_engine *h) {
+  const int NB = h->g.NB, NH = h->NH, W = h->band_w, U = h->unit_size;
+  for (auto &b : h->bands) {
+    for (void *p : {(void *)b.d_items, (void *)b.d_units, (void *)b.d_bin_units})
+      if (p) cudaFree(p);
+    b.d_items = b.d_units = nullptr;
+    b.d_bin_units = nullptr;
+    const int kx0 = b.kb0 * KB, kx1 = std::min(NH, (b.kb0 + b.nkb) * KB);
+    std::vector<int4> items, units;
+    std::vector<int> bin_units(NB + 1, 0);
+    for (int bin = 0; bin < NB; bin++) {
+      const int i0 = (int)items.size();
+      for (uint32_t i = h->bins.offsets[bin]; i < h->bins.offsets[bin + 1]; i++) {
+        const int32_t *m = &h->bins.modes[4 * (size_t)i];
+        const int kx = m[0] % NH, row = m[0] / NH;
+        if (kx < kx0 || kx >= kx1) continue;
+        items.push_back(make_int4(row * W + kx - kx0, m[1], m[2], bin));
+      }
+      const int i1 = (int)items.size();
+      bin_units[bin] = (int)units.size();
+      for (int i = i0; i < i1; i += U) units.push_back(make_int4(i, std::min(U, i1 - i), bin, 0));
+    }
+    bin_units[NB] = (int)units.size();
+    b.nunits = (int)units.size();
+    int rc;
+    if ((rc = dalloc(h, &b.d_items, std::max<size_t>(items.size(), 1))) ||
+        (rc = dalloc(h, &b.d_units, std::max<size_t>(units.size(), 1))) || (rc = dalloc(h, &b.d_bin_units, NB + 1)))
+      return rc;
+    if (!items.empty()) CK(cudaMemcpy(b.d_items, items.data(), sizeof(int4) * items.size(), cudaMemcpyHostToDevice));
+    if (!units.empty()) CK(cudaMemcpy(b.d_units, units.data(), sizeof(int4) * units.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(b.d_bin_units, bin_units.data(), sizeof(int) * (NB + 1), cudaMemcpyHostToDevice));
+  }
+  return DDM_OK;
+}
+
 // Uploads the spatial weighting: window, w(y)*scale is per call (scale), row
 // normalisers and the window-spectrum correction for the current mask.
 static int upload_mask_tables(ddm_engine *h, const uint8_t *mask) {
@@ -280,7 +334,7 @@ std::string &ddm_detached_error() { return g_create_error; }
 
 extern "C" const char *ddm_create_error(void) { return g_create_error.c_str(); }
 
-extern "C" int ddm_create(const ddm_geometry *geometry, ddm_engine **out) {
+static int create_impl(const ddm_geometry *geometry, uint64_t band_budget, ddm_engine **out) {
   g_create_error.clear();
   if (!geometry || !out) {
     g_create_error = "ddm_create: null argument";
@@ -349,6 +403,27 @@ extern "C" int ddm_create(const ddm_geometry *geometry, ddm_engine **out) {
     h->chunk_cap = std::max(h->chunk, std::min<int>(MAX_CHUNK, (int)std::max<size_t>(fg, cap_bytes / per)) / fg * fg);
   }
   h->bins = make_bins(g.N, g.NB, g.kmin, g.kmax, g.knodes);
+  if (band_budget) {
+    // columns of history that fit the budget, in whole column blocks
+    const uint64_t per_col = (uint64_t)g.N * g.T * sizeof(float2);
+    const uint64_t cols = band_budget / per_col;
+    if (cols < (uint64_t)KB) {
+      snprintf(msg, sizeof msg, "history budget %llu B holds fewer than %d spectrum columns (%llu B each)",
+               (unsigned long long)band_budget, KB, (unsigned long long)per_col);
+      g_create_error = msg;
+      delete h;
+      return DDM_ERR_ARG;
+    }
+    const int bkb = (int)std::min<uint64_t>((uint64_t)h->NHB, cols / KB);
+    h->band_w = bkb * KB;
+    for (int kb0 = 0; kb0 < h->NHB; kb0 += bkb) {
+      ddm_engine::Band b;
+      b.kb0 = kb0;
+      b.nkb = std::min(bkb, h->NHB - kb0);
+      h->bands.push_back(b);
+    }
+  }
+  const size_t hist_modes = (size_t)g.N * (h->band_w ? h->band_w : h->NH);
   int rc = DDM_OK;
   auto bail = [&](int code) {
     g_create_error = h->err;
@@ -372,7 +447,7 @@ extern "C" int ddm_create(const ddm_geometry *geometry, ddm_engine **out) {
   const int N = g.N;
   h->stage_bytes = (size_t)h->chunk_cap * N * N * sizeof(float);
   h->rowc_cap = std::max<size_t>((size_t)h->chunk_cap * N, (size_t)g.T);
-  if ((rc = dalloc(h, &h->d_hist, (size_t)h->modes * g.T)) ||
+  if ((rc = dalloc(h, &h->d_hist, hist_modes * g.T)) ||
       (rc = dalloc(h, &h->d_rows, (size_t)h->chunk_cap * h->NHB * N * KB)) ||
       (rc = dalloc(h, &h->d_rowc, h->rowc_cap)) ||
       (rc = dalloc(h, &h->d_framesum, (size_t)h->chunk_cap)) ||
@@ -414,12 +489,32 @@ extern "C" int ddm_create(const ddm_geometry *geometry, ddm_engine **out) {
       cudaMemcpy(h->d_tw_t, twt.data(), sizeof(float) * twt.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(h->d_tw_t16, twt16.data(), sizeof(float) * twt16.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(h->d_wcorr4, wc4, sizeof wc4, cudaMemcpyHostToDevice) != cudaSuccess ||
-      cudaMemset(h->d_hist, 0, sizeof(float2) * (size_t)h->modes * g.T) != cudaSuccess) {
+      cudaMemset(h->d_hist, 0, sizeof(float2) * hist_modes * g.T) != cudaSuccess) {
     h->err = "table upload failed";
     return bail(DDM_ERR_CUDA);
   }
   if ((rc = upload_mask_tables(h, nullptr)) || (rc = build_units(h))) return bail(rc);
+  if (h->band_w && (rc = build_band_units(h))) return bail(rc);
   *out = h;
+  return DDM_OK;
+}
+
+extern "C" int ddm_create(const ddm_geometry *geometry, ddm_engine **out) {
+  return create_impl(geometry, 0, out);
+}
+
+extern "C" int ddm_create_banded(const ddm_geometry *geometry, uint64_t history_budget_bytes, ddm_engine **out) {
+  if (history_budget_bytes == 0) {
+    g_create_error = "ddm_create_banded: the history budget must be > 0";
+    return DDM_ERR_ARG;
+  }
+  return create_impl(geometry, history_budget_bytes, out);
+}
+
+extern "C" int ddm_get_bands(const ddm_engine *h, int32_t *nbands, int32_t *band_cols) {
+  if (!h) return DDM_ERR_ARG;
+  if (nbands) *nbands = h->band_w ? (int32_t)h->bands.size() : 1;
+  if (band_cols) *band_cols = h->band_w ? h->band_w : h->NH;
   return DDM_OK;
 }
 
@@ -499,6 +594,9 @@ static int launch_chunk(ddm_engine *h, const void *dframes, int dtype, int n, co
   cp.NH = h->NH;
   cp.NHB = h->NHB;
   cp.err = h->d_err;
+  cp.kb0 = h->cur_kb0;
+  cp.nkb = h->cur_nkb;
+  cp.hist_w = h->band_w;
   CKL(launch_cols(N, cp, h->stream));
   h->last_mean_index = n - 1;
   h->have_frames = true;
@@ -543,6 +641,8 @@ static int dtype_size(int dtype) { return dtype == 0 ? 1 : dtype == 1 ? 2 : 4; }
 static int ingest_impl(ddm_engine *h, const void *frames, int dtype, int n, const int32_t *slots,
                        float scale, bool device, bool wait_copies = true) {
   cudaSetDevice(h->device);
+  if (h->band_w && !h->in_banded)
+    return fail(h, DDM_ERR_STATE, "a banded engine analyses a video with ddm_analyze_banded");
   int rc = check_frames_args(h, frames, dtype, n, slots);
   if (rc) return rc;
   if (device && ((uintptr_t)frames & 15))
@@ -654,8 +754,11 @@ extern "C" int ddm_set_spatial_mask(ddm_engine *h, const uint8_t *mask) {
   return upload_mask_tables(h, mask);
 }
 
-static int temporal_impl(ddm_engine *h, const uint32_t *order, const float *mask, int full, cudaStream_t st) {
+static int temporal_impl(ddm_engine *h, const uint32_t *order, const float *mask, int full, cudaStream_t st,
+                         const ddm_engine::Band *band = nullptr) {
   cudaSetDevice(h->device);
+  if (h->band_w && !band)
+    return fail(h, DDM_ERR_STATE, "a banded engine analyses a video with ddm_analyze_banded");
   const int T = h->g.T, L = h->g.L, TPAD = h->g.TPAD;
   if (!order || !mask) return fail(h, DDM_ERR_ARG, "computeTemporal: order/mask must have length %d", T);
   for (int j = 0; j < T; j++)
@@ -737,18 +840,21 @@ static int temporal_impl(ddm_engine *h, const uint32_t *order, const float *mask
     CKL(launch_radial_full(rp, st));
     h->full_valid = true;
   } else {
-    tp.items = h->d_items;
-    tp.units = h->d_units;
-    tp.nunits = h->nunits;
+    // the engine's work units, or those of one band of a banded analysis
+    const int nunits = band ? band->nunits : h->nunits;
+    tp.items = band ? band->d_items : h->d_items;
+    tp.units = band ? band->d_units : h->d_units;
+    tp.nunits = nunits;
     tp.partials = h->d_partials;
-    const int grid = std::min(temporal_max_grid(TPAD, T, L, false, h->variant, tp.sparse != 0), h->nunits);
+    const int grid = std::min(temporal_max_grid(TPAD, T, L, false, h->variant, tp.sparse != 0), nunits);
     CK(cudaMemsetAsync(h->d_counter, 0, sizeof(int), st));
-    if (h->nunits > 0) CKL(launch_temporal(TPAD, L, false, tp, std::max(grid, 1), st));
+    if (nunits > 0) CKL(launch_temporal(TPAD, L, false, tp, std::max(grid, 1), st));
     ReduceParams rp{};
+    rp.accumulate = band && band != &h->bands[0];
     rp.partials = h->d_partials;
-    rp.bin_units = h->d_bin_units;
+    rp.bin_units = band ? band->d_bin_units : h->d_bin_units;
     rp.nmodes = h->d_nmodes;
-    rp.nunits = h->nunits;
+    rp.nunits = nunits;
     rp.NB = h->g.NB;
     rp.L = L;
     rp.D = h->d_radD;
@@ -877,6 +983,7 @@ extern "C" int ddm_read_radial(ddm_engine *h, double *D, double *P, double *drif
 
 extern "C" int ddm_read_history(ddm_engine *h, float *out) {
   if (!h || !out) return DDM_ERR_ARG;
+  if (h->band_w) return fail(h, DDM_ERR_STATE, "readHistory: a banded engine holds one band of the history at a time");
   cudaSetDevice(h->device);
   CK(cudaMemcpyAsync(out, h->d_hist, sizeof(float2) * (size_t)h->modes * h->g.T, cudaMemcpyDeviceToHost,
                      h->stream));
@@ -990,8 +1097,10 @@ extern "C" int ddm_batch_create(ddm_engine *const *engines, int32_t n, ddm_batch
   g_create_error.clear();
   if (!out || !engines || n < 1) return bfail(nullptr, DDM_ERR_ARG, "ddm_batch_create: need n >= 1 engines");
   *out = nullptr;
-  for (int i = 0; i < n; i++)
+  for (int i = 0; i < n; i++) {
     if (!engines[i]) return bfail(nullptr, DDM_ERR_ARG, "ddm_batch_create: engine %d is NULL", i);
+    if (engines[i]->band_w) return bfail(nullptr, DDM_ERR_ARG, "ddm_batch_create: engine %d is banded", i);
+  }
   ddm_batch *b = new ddm_batch();
   b->e.assign(engines, engines + n);
   b->device = engines[0]->device;
@@ -1296,6 +1405,7 @@ extern "C" int ddm_batch_launch_graph(ddm_batch *b) {
 // ingesting, and before building batches over the engine.
 extern "C" int ddm_autotune(ddm_engine *h, char *report, int32_t report_len) {
   if (!h) return DDM_ERR_ARG;
+  if (h->band_w) return fail(h, DDM_ERR_STATE, "autotune: not available on a banded engine (use ddm_set_tuning)");
   cudaSetDevice(h->device);
   if (int rc0 = join_analysis(h)) return rc0;
   h->radial_from_live = false;
@@ -1459,8 +1569,40 @@ extern "C" int ddm_set_tuning(ddm_engine *h, int32_t chunk, int32_t unit_size, i
   }
   if (unit_size && unit_size != h->unit_size) {
     int rc = build_units(h, unit_size);
+    if (!rc && h->band_w) rc = build_band_units(h);
     if (rc) return rc;
     h->radial_valid = h->full_valid = false;
   }
+  return DDM_OK;
+}
+
+// The analysis of a video on a banded engine: for each band of spectrum
+// columns, the spatial pass of every frame (host frames stream through the
+// pinned staging again: the frame stack is not held on the device) writing
+// only that band's history, then the band's temporal pass, whose radial sums
+// are added to the record band after band.
+extern "C" int ddm_analyze_banded(ddm_engine *h, const void *frames, int32_t dtype, int32_t n, const int32_t *slots,
+                                  float scale, const uint32_t *order, const float *mask, int32_t on_device) {
+  if (!h) return DDM_ERR_ARG;
+  if (!h->band_w) return fail(h, DDM_ERR_STATE, "ddm_analyze_banded: the engine was not created banded");
+  cudaSetDevice(h->device);
+  int rc = check_frames_args(h, frames, dtype, n, slots);
+  if (rc) return rc;
+  if (!order || !mask) return fail(h, DDM_ERR_ARG, "ddm_analyze_banded: order/mask must have length %d", h->g.T);
+  h->radial_valid = false;
+  h->in_banded = true;
+  for (const auto &b : h->bands) {
+    h->cur_kb0 = b.kb0;
+    h->cur_nkb = b.nkb;
+    if ((rc = ingest_impl(h, frames, dtype, n, slots, scale, on_device != 0)) ||
+        (rc = temporal_impl(h, order, mask, 0, h->stream, &b)))
+      break;
+  }
+  h->in_banded = false;
+  h->cur_kb0 = h->cur_nkb = 0;
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(h->stream));
+  if ((rc = check_device_error(h))) return rc;
+  h->radial_valid = true;
   return DDM_OK;
 }

@@ -42,6 +42,10 @@ struct ColParams {
   float scale;
   int nframes, T, NH, NHB;
   int* err;                // error word (bounded waits that timed out), or nullptr
+  // history band (0 = the whole half-plane): column blocks kb0 .. kb0 + nkb - 1
+  // (KB columns each) and hist_w columns per history row, so mode (ky, kx)
+  // of the band is stored at ((ky * hist_w) + kx - kb0 * KB) * T + slot
+  int kb0, nkb, hist_w;
 };
 
 // One video of a batched temporal launch (units carry the video index in .w).
@@ -84,6 +88,7 @@ constexpr int SPARSE_ZMAX = 64;  // masked time indices the sparse temporal kern
 constexpr int SPARSE_ZMAX_BIG = 256;  // ... and its TPAD 8192 variant (zero-list capacity)
 
 struct ReduceParams {
+  int accumulate;          // 1: add into D, P, drift (a band of a banded analysis after the first)
   const double* partials;
   const int* bin_units;    // [NB+1] unit range of each bin
   const uint32_t* nmodes;  // [NB]

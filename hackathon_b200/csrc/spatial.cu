@@ -285,12 +285,14 @@ __global__ void __launch_bounds__(256) cols_kernel(ColParams p) {
   for (int i = threadIdx.x; i < tw_count<N>(); i += blockDim.x) s_tw[i] = p.tw[i];
   if (threadIdx.x < 4) s_wc4[threadIdx.x] = p.wc4[threadIdx.x];
   const int nfg = (p.nframes + G - 1) / G;
-  const int ntiles = p.NHB * nfg;
+  const int NKB = p.nkb > 0 ? p.nkb : p.NHB, kb0 = p.kb0;  // the column blocks of the history band
+  const int W = p.hist_w > 0 ? p.hist_w : p.NH;            // columns per history row
+  const int ntiles = NKB * nfg;
   const float invN = 1.f / N;
   const int sf = threadIdx.x % G;  // frame of the tile this thread stores
   const double inv_total = p.inv_total[0];
   auto issue = [&](int tile) {
-    const int kb = tile % p.NHB, f0 = (tile / p.NHB) * G;
+    const int kb = kb0 + tile % NKB, f0 = (tile / NKB) * G;
     const int nf = min(G, p.nframes - f0);
     mbar_arrive_expect_tx(&bar, nf * FRAME_BYTES);
     for (int i = 0; i < nf; i++)
@@ -305,14 +307,14 @@ __global__ void __launch_bounds__(256) cols_kernel(ColParams p) {
   __syncthreads();
   uint32_t phase = 0;
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const int kb = tile % p.NHB;
-    const int f0 = (tile / p.NHB) * G;
+    const int kb = kb0 + tile % NKB;
+    const int f0 = (tile / NKB) * G;
     const int nf = min(G, p.nframes - f0);
     if (threadIdx.x < nf) {
       const int f = f0 + threadIdx.x;
       const double mu = p.framesum[f] * inv_total;
       s_dc[threadIdx.x] = (float)(((double)p.framec[f] - mu) * (double)p.scale / N);
-      if (kb == 0) p.means[f] = mu * (double)p.scale;
+      if (kb == kb0) p.means[f] = mu * (double)p.scale;
     }
     if (!mbar_wait(&bar, phase, p.err, 3)) return;  // nothing else is in flight
     phase ^= 1u;
@@ -347,8 +349,8 @@ __global__ void __launch_bounds__(256) cols_kernel(ColParams p) {
       if (sf < nf) {
         const int yoff = (int)(Y - (sm + (size_t)g * GSTRIDE<N>()));
         const float2* ys = sm + (size_t)sf * GSTRIDE<N>() + yoff;
-        float2* hs = p.hist + (size_t)kx * p.T + slot;
-        const size_t mstride = (size_t)p.NH * p.T;
+        float2* hs = p.hist + (size_t)(kx - kb0 * KB) * p.T + slot;
+        const size_t mstride = (size_t)W * p.T;
         const float dc = s_dc[sf];
         const float2 wkx = kx < 4 ? s_wc4[kx] : make_float2(0.f, 0.f);
 #pragma unroll
@@ -405,16 +407,18 @@ __global__ void __launch_bounds__(256, 1) cols_wide_kernel(ColParams p) {
   for (int i = threadIdx.x; i < tw_size(N); i += blockDim.x) s_tw[i] = p.tw[i];
   if (threadIdx.x < 4) s_wc4[threadIdx.x] = p.wc4[threadIdx.x];
   const int nfg = (p.nframes + F - 1) / F;
-  const int ntiles = p.NHB * nfg;
+  const int NKB = p.nkb > 0 ? p.nkb : p.NHB, kb0 = p.kb0;  // the column blocks of the history band
+  const int W = p.hist_w > 0 ? p.hist_w : p.NH;            // columns per history row
+  const int ntiles = NKB * nfg;
   const float invN = 1.f / N;
   const double inv_total = p.inv_total[0];
   // item (tile, j): frames f0 + j*G .. f0 + j*G + G - 1 of the tile (those < nframes)
   auto items_of = [&](int tile) {
-    const int f0 = (tile / p.NHB) * F;
+    const int f0 = (tile / NKB) * F;
     return (min(F, p.nframes - f0) + G - 1) / G;
   };
   auto issue = [&](int tile, int j, int s) {
-    const int kb = tile % p.NHB, f0 = (tile / p.NHB) * F + j * G;
+    const int kb = kb0 + tile % NKB, f0 = (tile / NKB) * F + j * G;
     const int nf = min(G, p.nframes - f0);
     mbar_arrive_expect_tx(&bar[s], nf * FRAME_BYTES);
     for (int i = 0; i < nf; i++)
@@ -443,14 +447,14 @@ __global__ void __launch_bounds__(256, 1) cols_wide_kernel(ColParams p) {
   int e = 0;  // items consumed by this CTA
   constexpr int SPT = 256 / F;  // ky stride of the store loop
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const int kb = tile % p.NHB;
-    const int f0 = (tile / p.NHB) * F;
+    const int kb = kb0 + tile % NKB;
+    const int f0 = (tile / NKB) * F;
     const int nf = min(F, p.nframes - f0);
     if (threadIdx.x < nf) {
       const int f = f0 + threadIdx.x;
       const double mu = p.framesum[f] * inv_total;
       s_dc[threadIdx.x] = (float)(((double)p.framec[f] - mu) * (double)p.scale / N);
-      if (kb == 0) p.means[f] = mu * (double)p.scale;
+      if (kb == kb0) p.means[f] = mu * (double)p.scale;
     }
     if (p.w2d && threadIdx.x == 0) {
       // the correction rows of this tile's columns, read by the store loop
@@ -495,13 +499,13 @@ __global__ void __launch_bounds__(256, 1) cols_wide_kernel(ColParams p) {
     if (sf < nf) {
       const int slot = p.slots[f0 + sf];
       const float dc = s_dc[sf];
-      const size_t mstride = (size_t)p.NH * p.T;
+      const size_t mstride = (size_t)W * p.T;
 #pragma unroll 1
       for (int c = 0; c < KB; c++) {
         const int kx = kb * KB + c;
         if (kx >= p.NH) break;
         const float2* ys = R + (size_t)(c * F + sf) * N;
-        float2* hs = p.hist + (size_t)kx * p.T + slot;
+        float2* hs = p.hist + (size_t)(kx - kb0 * KB) * p.T + slot;
         const float2 wkx = kx < 4 ? s_wc4[kx] : make_float2(0.f, 0.f);
         if (p.w2d) {
           // correction table loads run one batch of WB ahead of the stores
@@ -665,13 +669,13 @@ static cudaError_t cols_n(const ColParams& p, cudaStream_t s) {
   if constexpr (use_wide_cols(N)) {
     auto k = cols_wide_kernel<N>;
     const size_t sm = cols_wide_smem<N>();
-    const int grid = persistent_grid(k, G * (N / 8), sm, (long long)p.NHB * ((p.nframes + WIDE_F - 1) / WIDE_F));
+    const int grid = persistent_grid(k, G * (N / 8), sm, (long long)(p.nkb > 0 ? p.nkb : p.NHB) * ((p.nframes + WIDE_F - 1) / WIDE_F));
     k<<<grid, G * (N / pts(N)), sm, s>>>(p);
     return cudaGetLastError();
   }
   auto k = cols_kernel<N>;
   const size_t sm = fft_smem<N>() + (size_t)G * N * KB * sizeof(float2);
-  const int grid = persistent_grid(k, G * (N / pts(N)), sm, (long long)p.NHB * ((p.nframes + G - 1) / G));
+  const int grid = persistent_grid(k, G * (N / pts(N)), sm, (long long)(p.nkb > 0 ? p.nkb : p.NHB) * ((p.nframes + G - 1) / G));
   k<<<grid, G * (N / pts(N)), sm, s>>>(p);
   return cudaGetLastError();
 }

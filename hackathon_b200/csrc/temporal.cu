@@ -1535,7 +1535,8 @@ __global__ void __launch_bounds__(NP / 16, 1) temporal_sparse_big_kernel(Tempora
 
 // Sums the unit partials of each bin in unit order (deterministic), divides
 // D and P by the bin's mode count (ddm_ref.js:404-412) and writes the
-// reference's Radial layout: D[b*L+tau], P[b], drift[(b*L+tau)*8+c].
+// reference's Radial layout: D[b*L+tau], P[b], drift[(b*L+tau)*8+c] (or adds
+// to it: the bands of a banded analysis after the first, in band order).
 // Grid (lag blocks, bins), one thread per (bin, lag): the unit loop is
 // unrolled so several units' loads are in flight (the sums still add in
 // unit order).
@@ -1555,14 +1556,18 @@ __global__ void reduce_kernel(ReduceParams p) {
     for (int u = u0; u < u1; u++)
 #pragma unroll
       for (int c = 0; c < PFIELDS; c++) s[c] += __ldg(&src[((size_t)u * PFIELDS + c) * L]);
-    p.D[(size_t)b * L + tau] = s[0] * inv;
+    double* dD = &p.D[(size_t)b * L + tau];
+    *dD = p.accumulate ? *dD + s[0] * inv : s[0] * inv;
 #pragma unroll
-    for (int c = 0; c < DRIFT; c++) p.drift[((size_t)b * L + tau) * DRIFT + c] = s[c + 1];
+    for (int c = 0; c < DRIFT; c++) {
+      double* d = &p.drift[((size_t)b * L + tau) * DRIFT + c];
+      *d = p.accumulate ? *d + s[c + 1] : s[c + 1];
+    }
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     double s = 0.0;
     for (int u = u0; u < u1; u++) s += p.partials[(size_t)p.nunits * PFIELDS * L + u];
-    p.P[b] = s * inv;
+    p.P[b] = p.accumulate ? p.P[b] + s * inv : s * inv;
   }
 }
 

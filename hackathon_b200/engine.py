@@ -77,6 +77,51 @@ class DdmEngine:
         lib.ddm_get_geometry(h, C.byref(out))
         return cls(h, out)
 
+    @classmethod
+    def create_banded(cls, history_budget_bytes, N=256, T=256, TPAD=0, L=128, NB=32, kmin=4.0, kmax=100.0,
+                      knodes=4):
+        """An engine for videos whose history does not fit the device at once
+        (ddm_create_banded): it holds a band of spectrum columns sized to
+        history_budget_bytes and analyses a whole video with analyze_banded."""
+        lib = _lib.load()
+        g = _lib.Geometry(N, T, TPAD, L, NB, float(kmin), float(kmax), knodes, 0)
+        h = C.c_void_p()
+        rc = lib.ddm_create_banded(C.byref(g), int(history_budget_bytes), C.byref(h))
+        if rc != _lib.DDM_OK:
+            msg = lib.ddm_create_error().decode()
+            raise (DdmArgError if rc == _lib.DDM_ERR_ARG else DdmError)(rc, msg)
+        out = _lib.Geometry()
+        lib.ddm_get_geometry(h, C.byref(out))
+        return cls(h, out)
+
+    @property
+    def bands(self):
+        """(number of bands, spectrum columns per band) -- (1, N/2+1) for an
+        ordinary engine."""
+        self._alive()
+        nb, bc = C.c_int32(), C.c_int32()
+        self._check(self._lib.ddm_get_bands(self._h, C.byref(nb), C.byref(bc)))
+        return nb.value, bc.value
+
+    def analyze_banded(self, frames, slots, order, mask, scale=None):
+        """The whole analysis of one video on a banded engine
+        (ddm_analyze_banded): per band the spatial pass of every frame (host
+        frames stream through pinned staging once per band), then the band's
+        temporal pass; read the record with read_radial()."""
+        self._alive()
+        dt, n, dev_ptr, host_ptr, keep, slots = self._frames_arg(frames, slots)
+        if scale is None:
+            scale = {"u8": 1 / 255, "u16": 1 / 65535, "f32": 1.0}[dt]
+        o = np.ascontiguousarray(order, dtype=np.uint32).reshape(-1)
+        m = np.ascontiguousarray(mask, dtype=np.float32).reshape(-1)
+        if o.size != self.T or m.size != self.T:
+            raise DdmArgError(_lib.DDM_ERR_ARG, f"temporalMeta: order/mask must have length {self.T}")
+        ptr = dev_ptr if dev_ptr is not None else host_ptr
+        rc = self._lib.ddm_analyze_banded(self._h, C.c_void_p(ptr), _lib.DTYPES[dt], n, _ptr(slots), float(scale),
+                                          _ptr(o), _ptr(m), 1 if dev_ptr is not None else 0)
+        del keep
+        self._check(rc)
+
     def destroy(self):
         """DdmEngine.destroy (ddm-engine.ts:421-425)."""
         if not self._destroyed:
@@ -144,16 +189,12 @@ class DdmEngine:
         self._check(self._lib.ddm_ingest_luma(self._h, _ptr(a), int(slot), C.byref(ok)))
         return bool(ok.value)
 
-    def ingest_frames(self, frames, slots, scale=None, wait=True):
-        """Raw frames [n, N, N] (numpy, or torch CPU/CUDA tensor) into ring slots
-        `slots[i] % T`. luma = value * scale; scale defaults to 1/255 for u8
-        (lumaOf, test/sim.mjs:189-193), 1/65535 for u16 and 1 for f32.
-        wait=False (host frames): return once the copies are queued
-        (ddm_ingest_frames_async); the engine keeps a reference to the host
-        buffer until ingest_wait() -- do not change it before then."""
-        self._alive()
+    def _frames_arg(self, frames, slots):
+        """(dtype name, n, device pointer or None, host pointer or None, the
+        object keeping the data alive, slots) of a frames argument: numpy, or
+        a torch CPU/CUDA tensor, [n, N, N] u8 / u16 / f32."""
         slots = np.ascontiguousarray(slots, dtype=np.int32).reshape(-1)
-        dev_ptr = None
+        dev_ptr = host_ptr = keep = None
         try:
             import torch
             if isinstance(frames, torch.Tensor):
@@ -173,7 +214,7 @@ class DdmEngine:
                 keep = frames
         except ImportError:
             pass
-        if dev_ptr is None and "keep" not in locals():
+        if keep is None:
             arr = np.ascontiguousarray(frames)
             dt = {np.dtype(np.uint8): "u8", np.dtype(np.uint16): "u16",
                   np.dtype(np.float32): "f32"}.get(arr.dtype)
@@ -186,6 +227,17 @@ class DdmEngine:
             keep = arr
         if slots.size != n:
             raise DdmArgError(_lib.DDM_ERR_ARG, f"{n} frames but {slots.size} slots")
+        return dt, n, dev_ptr, host_ptr, keep, slots
+
+    def ingest_frames(self, frames, slots, scale=None, wait=True):
+        """Raw frames [n, N, N] (numpy, or torch CPU/CUDA tensor) into ring slots
+        `slots[i] % T`. luma = value * scale; scale defaults to 1/255 for u8
+        (lumaOf, test/sim.mjs:189-193), 1/65535 for u16 and 1 for f32.
+        wait=False (host frames): return once the copies are queued
+        (ddm_ingest_frames_async); the engine keeps a reference to the host
+        buffer until ingest_wait() -- do not change it before then."""
+        self._alive()
+        dt, n, dev_ptr, host_ptr, keep, slots = self._frames_arg(frames, slots)
         if scale is None:
             scale = {"u8": 1 / 255, "u16": 1 / 65535, "f32": 1.0}[dt]
         code = _lib.DTYPES[dt]

@@ -73,6 +73,28 @@ const char *ddm_last_error(const ddm_engine *h);
  * ddm_create or ddm_spectra_noalloc. */
 const char *ddm_create_error(void);
 
+/* Large videos (no counterpart in the reference, whose ring is fixed at
+ * 256^2 x 256): an engine whose history holds only a band of spectrum
+ * columns at a time, sized to history_budget_bytes (whole pairs of columns of
+ * N * T complex values each; the whole half-plane if it fits). Such an engine
+ * analyses a video only through ddm_analyze_banded, reads its record with
+ * ddm_read_radial; the per-frame ingest, computeTemporal, readHistory and the
+ * full outputs answer DDM_ERR_STATE. */
+int ddm_create_banded(const ddm_geometry *geometry, uint64_t history_budget_bytes,
+                      ddm_engine **out);
+/* Bands of a banded engine and the spectrum columns each holds (1 and N/2+1
+ * for an ordinary engine). */
+int ddm_get_bands(const ddm_engine *h, int32_t *nbands, int32_t *band_cols);
+/* The analysis of one video on a banded engine: for each band, the spatial
+ * pass of all n frames writing that band's history (host frames stream
+ * through the engine's pinned staging once per band; on_device = 1: the
+ * frames are in device memory), then the band's masked Wiener-Khinchin pass
+ * (order, mask as ddm_compute_temporal), its radial sums added to the record
+ * band after band. Blocks until the record is ready. */
+int ddm_analyze_banded(ddm_engine *h, const void *frames, int32_t dtype, int32_t n,
+                       const int32_t *slots, float scale, const uint32_t *order,
+                       const float *mask, int32_t on_device);
+
 /* Resolved geometry (TPAD filled in). */
 int ddm_get_geometry(const ddm_engine *h, ddm_geometry *out);
 /* DdmEngine.bins (ddm-engine.ts:69): number of binned modes, then the table. */

@@ -268,6 +268,7 @@ struct Device {
   uint8_t* mbuf = nullptr;
   int max_jobs = 0;
   std::vector<GfitProblem> hprobs;
+  int max_bins = 1;
   cudaError_t err = cudaSuccess;
 
   ~Device() {
@@ -319,6 +320,7 @@ struct Device {
       P.dmask = mbuf + om;
       om += (size_t)R->nb * R->r->L;
       R->prob = (int)hprobs.size();
+      max_bins = std::max(max_bins, R->nb);
       hprobs.push_back(P);
       P.amps = dbuf + o;  // the Brownian entry: its own amplitudes, no mask
       o += 2 * (size_t)R->nb;
@@ -349,6 +351,7 @@ struct Device {
     a.max_iter = MAX_ITER;
     a.tol = LM_TOL;
     a.tab = tab;
+    a.max_bins = max_bins;
     if (!ok(launch_gfit_model(model, a, s))) return false;
     if (!ok(cudaMemcpyAsync(out.data(), res, sizeof(GfitResult) * J.size(), cudaMemcpyDeviceToHost, s))) return false;
     return ok(cudaStreamSynchronize(s));

@@ -43,7 +43,7 @@ namespace {
 
 constexpr int GF_THREADS = 256;
 constexpr int GF_WARPS = GF_THREADS / 32;
-constexpr int GF_CLUSTER = 4;
+constexpr int GF_MAX_CLUSTER = 16;  // CTAs per job at most (a non-portable cluster size)
 constexpr int GF_NV = 1 + 4 + 10;  // cost, gradient, upper triangle of the 4x4 curvature
 
 template <int M>
@@ -694,16 +694,54 @@ __global__ void __launch_bounds__(GF_THREADS) gfit_kernel(GfitLaunch a) {
   cl.sync();  // no CTA leaves while another may still read its shared memory
 }
 
+// CTAs per job: about two bins per warp (each warp walks its bins in turn,
+// so fewer bins per warp shortens every objective evaluation, the search's
+// serial step), a power of two from 2 to 16, but no more than leaves every
+// job of the launch a cluster at once (a batch of records runs many jobs:
+// smaller clusters, more of them in flight), and no more than the device can
+// co-schedule as one cluster.
+template <int M>
+int cluster_size(const GfitLaunch& a) {
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (sms <= 0) sms = 148;
+  }
+  int want = 2;
+  while (want < GF_MAX_CLUSTER && want * GF_WARPS * 2 < a.max_bins && 2 * want * a.njobs <= sms) want *= 2;
+  auto k = gfit_kernel<M>;
+  if (want > 8) cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  for (; want > 2; want /= 2) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3((unsigned)want);
+    cfg.blockDim = dim3(GF_THREADS);
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = want;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, k, &cfg) == cudaSuccess && n >= 1) break;
+    cudaGetLastError();
+  }
+  return want;
+}
+
 template <int M>
 cudaError_t launch_model(const GfitLaunch& a, cudaStream_t s) {
+  const int cl = cluster_size<M>(a);
   cudaLaunchConfig_t cfg{};
-  cfg.gridDim = dim3((unsigned)(a.njobs * GF_CLUSTER));
+  cfg.gridDim = dim3((unsigned)(a.njobs * cl));
   cfg.blockDim = dim3(GF_THREADS);
   cfg.dynamicSmemBytes = 0;
   cfg.stream = s;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeClusterDimension;
-  attr[0].val.clusterDim.x = GF_CLUSTER;
+  attr[0].val.clusterDim.x = cl;
   attr[0].val.clusterDim.y = 1;
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;

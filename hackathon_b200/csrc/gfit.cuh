@@ -64,6 +64,7 @@ struct GfitLaunch {
   int njobs, max_iter;
   double tol;             // relative cost decrease that counts as no progress
   Isf2dTable tab;
+  int max_bins;           // the most bins of any problem of the launch (sizes the clusters)
 };
 
 // One thread-block cluster per job (bins split across the cluster, sums

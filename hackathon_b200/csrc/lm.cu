@@ -36,11 +36,15 @@ constexpr int LM_NP = 6;
 constexpr int LM_MAX_LAGS = 128;   // 4 per lane
 constexpr int LM_MAX_NODES = 8;
 constexpr int LM_WARPS = 8;        // fits per 256-thread CTA
-// CTAs per SM the register budget is sized for: 3 (80 registers). Measured on
+// CTAs per SM the register budget is sized for: 1 (no cap). The model and
+// normal-equation routines (varpro, varpro_brownian64, lm_normal, lm_solve)
+// are not inlined: inlined at every call site they overflowed the
+// instruction cache (ncu: "no instruction" was the top stall). Measured on
 // B200 over 1e5 analytic curves (q-fits/s, plain / seeded from the truth):
-// 1 CTA (210 registers) 113K / 759K, 2 CTAs 107K / 984K, 3 CTAs 104K / 1.07M.
+// inlined, 3 CTAs (80 registers) 132K / 1.13M; not inlined, 1 CTA 144K /
+// 1.31M, 2 CTAs 104K / 1.04M, 3 CTAs 99K / 1.35M.
 #ifndef LM_MIN_BLOCKS
-#define LM_MIN_BLOCKS 3
+#define LM_MIN_BLOCKS 1
 #endif
 
 // Precision-generic math for the model: FP32 for the bulk of the
@@ -157,7 +161,7 @@ __device__ __forceinline__ double varpro_c(const PR& P, int lane, const CT (&c)[
 }
 
 template <class PR>
-__device__ __forceinline__ double varpro(const PR& P, int lane, double al, double lv, double lZ,
+__device__ __noinline__ double varpro(const PR& P, int lane, double al, double lv, double lZ,
                                          double lD, double& A, double& B) {
   float c[4];
   model_c(P, lane, (float)al, (float)exp(lv), (float)exp(lZ), (float)exp(lD), c);
@@ -168,7 +172,7 @@ __device__ __forceinline__ double varpro(const PR& P, int lane, double al, doubl
 // Brownian-only fit: its golden section walks a valley that can be flat to
 // FP32 rounding (noise-dominated or barely decaying bins).
 template <class PR>
-__device__ __forceinline__ double varpro_brownian64(const PR& P, int lane, double lD, double& A,
+__device__ __noinline__ double varpro_brownian64(const PR& P, int lane, double lD, double& A,
                                                     double& B) {
   const double D = exp(lD), iK = 1.0 / P.K;
   double c[4];
@@ -227,7 +231,7 @@ __device__ __forceinline__ double reduce_scatter32(double (&v)[32], int lane) {
 // The normal equations at theta; returns this lane's slot total. The model
 // and Jacobian are evaluated in R; the sums are FP64.
 template <typename R, class PR>
-__device__ __forceinline__ double lm_normal(const PR& P, const double (&th)[LM_NP], int lane) {
+__device__ __noinline__ double lm_normal(const PR& P, const double (&th)[LM_NP], int lane) {
   const R A = (R)th[0], B = (R)th[1], al = (R)th[2];
   const R v = (R)exp(th[3]), Z = (R)exp(th[4]), D = (R)exp(th[5]);
   double acc[32];
@@ -281,7 +285,7 @@ __device__ __forceinline__ double lm_cost(double hv) { return __shfl_sync(0xffff
 // position; pivots, column entries and the triangular solves travel by
 // shuffles, and every lane ends with the same delta. False if not positive
 // definite (the same on every lane).
-__device__ __forceinline__ bool lm_solve(double hv, double lambda, int lane, int li, int lj,
+__device__ __noinline__ bool lm_solve(double hv, double lambda, int lane, int li, int lj,
                                          double (&delta)[LM_NP]) {
   const bool in = lane < LM_SLOT_G;
   double a = hv;

@@ -197,7 +197,7 @@ struct Dft<16, INV> {
 // (j - j%Ns)*R + j%Ns + m*Ns.
 // TW_SMEM: the twiddle table is in shared memory (plain loads) rather than
 // global memory (read-only cache loads).
-template <int n, int R, int Ns, bool INV, bool TW_SMEM>
+template <int n, int R, int Ns, bool INV, bool TW_SMEM, bool TW_REC = false>
 __device__ __forceinline__ void stage(float2 (&v)[8], int t, float2* __restrict__ out,
                                       const float2* __restrict__ tw) {
   constexpr int NT = n / 8;
@@ -210,14 +210,26 @@ __device__ __forceinline__ void stage(float2 (&v)[8], int t, float2* __restrict_
 #pragma unroll
     for (int m = 0; m < R; m++) a[m] = v[i + B * m];
     if (Ns > 1) {
-      // every W^m from the FP64-derived table (products of table entries
-      // would save loads but add roundings the accuracy budget cannot take)
       const float2* tws = tw + tw_offset(n, Ns) + k;
+      if constexpr (TW_REC) {
+        // W^1 from the FP64-derived table, the higher powers as products
+        // (one table load instead of R - 1; each product adds a rounding)
+        float2 w1 = TW_SMEM ? tws[0] : __ldg(&tws[0]);
+        if (INV) w1.y = -w1.y;
+        float2 wm[R];
+        wm[1] = w1;
 #pragma unroll
-      for (int m = 1; m < R; m++) {
-        float2 w = TW_SMEM ? tws[(m - 1) * Ns] : __ldg(&tws[(m - 1) * Ns]);
-        if (INV) w.y = -w.y;
-        a[m] = cmul(a[m], w);
+        for (int m = 2; m < R; m++) wm[m] = cmul(wm[m / 2], wm[m - m / 2]);
+#pragma unroll
+        for (int m = 1; m < R; m++) a[m] = cmul(a[m], wm[m]);
+      } else {
+        // every W^m from the FP64-derived table
+#pragma unroll
+        for (int m = 1; m < R; m++) {
+          float2 w = TW_SMEM ? tws[(m - 1) * Ns] : __ldg(&tws[(m - 1) * Ns]);
+          if (INV) w.y = -w.y;
+          a[m] = cmul(a[m], w);
+        }
       }
     }
     Dft<R, INV>::run(a);
@@ -255,18 +267,18 @@ __host__ __device__ constexpr int sync_kind(int n, int groups) {
   return groups == 1 ? SYNC_CTA : (n / 8 <= 32 ? SYNC_WARP : SYNC_GROUP);
 }
 
-template <int n, int Ns, bool INV, bool TW_SMEM, int SYNC>
+template <int n, int Ns, bool INV, bool TW_SMEM, int SYNC, bool TW_REC = false>
 struct Stages {
   // Runs the stages from stride Ns on; the stage writes `a`, the next one
   // writes `b`. Ends with a barrier after the last store.
   static __device__ __forceinline__ void run(float2 (&v)[8], int t, float2* a, float2* b,
                                              const float2* __restrict__ tw, int bar_id) {
     constexpr int R = (n / Ns) >= 8 ? 8 : (n / Ns);
-    stage<n, R, Ns, INV, TW_SMEM>(v, t, a, tw);
+    stage<n, R, Ns, INV, TW_SMEM, TW_REC>(v, t, a, tw);
     stage_sync<n, SYNC>(bar_id);
     if constexpr (Ns * R < n) {
       load8<n>(v, t, a);
-      Stages<n, Ns * R, INV, TW_SMEM, SYNC>::run(v, t, b, a, tw, bar_id);
+      Stages<n, Ns * R, INV, TW_SMEM, SYNC, TW_REC>::run(v, t, b, a, tw, bar_id);
     }
   }
 };
@@ -274,10 +286,10 @@ struct Stages {
 // Full n-point FFT of the 8 register points per thread (layout contract
 // above). Returns the buffer holding the natural-order result (read it at
 // pad(k)); the result lands in buf0 when the stage count is odd, else buf1.
-template <int n, bool INV, bool TW_SMEM = false, int SYNC = SYNC_CTA>
+template <int n, bool INV, bool TW_SMEM = false, int SYNC = SYNC_CTA, bool TW_REC = false>
 __device__ __forceinline__ float2* fft(float2 (&v)[8], int t, float2* buf0, float2* buf1,
                                        const float2* __restrict__ tw, int bar_id = 0) {
-  Stages<n, 1, INV, TW_SMEM, SYNC>::run(v, t, buf0, buf1, tw, bar_id);
+  Stages<n, 1, INV, TW_SMEM, SYNC, TW_REC>::run(v, t, buf0, buf1, tw, bar_id);
   return (fft_stages(n) & 1) ? buf0 : buf1;
 }
 

@@ -110,7 +110,7 @@ struct RadialFullParams {
   double* odrift;
 };
 
-enum { LM_PLAIN = 0, LM_SEEDED = 1, LM_SEEDED_FALLBACK = 2, LM_BROWNIAN = 3 };
+enum { LM_PLAIN = 0, LM_SEEDED = 1, LM_SEEDED_FALLBACK = 2, LM_BROWNIAN = 3, LM_SEEDED_COST = 4 };
 
 struct LmParams {
   int nfit, nt_max, K;

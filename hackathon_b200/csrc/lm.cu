@@ -531,7 +531,7 @@ __device__ __noinline__ void lm_one(const LmParams& p, int fit, int lane) {
   double th[LM_NP], cost = 0;
   int iters = 0, evals = 0, status = 0;
   bool conv = false;
-  if (p.mode == LM_SEEDED || p.mode == LM_SEEDED_FALLBACK) {
+  if (p.mode == LM_SEEDED || p.mode == LM_SEEDED_FALLBACK || p.mode == LM_SEEDED_COST) {
     const float* s = p.start + (size_t)fit * 4;
     th[2] = (double)s[0];
     th[3] = log((double)s[1]);
@@ -556,7 +556,21 @@ __device__ __noinline__ void lm_one(const LmParams& p, int fit, int lane) {
       evals += 17;
       bad = cost > bmin;
     }
-    if (p.mode == LM_SEEDED_FALLBACK && bad) {
+    if (p.mode == LM_SEEDED_COST) {
+      // cost alone decides: the bin's Brownian optimum (fitBrownian's scan
+      // and golden section, FP64 model) bounds the optimum from above; a
+      // seeded fit above it sits in a wrong basin, whether or not its LM
+      // converged. A fit at or below it is kept even when the LM stopped at
+      // max_iter (a long valley it was still walking down).
+      bool settled;
+      int be = 0;
+      const double lD = brownian_search<true>(P, lane, be, settled);
+      double A, B;
+      const double bopt = varpro_brownian64(P, lane, lD, A, B);
+      evals += be + 1;
+      bad = cost > bopt * (1.0 + 1e-9);
+    }
+    if ((p.mode == LM_SEEDED_FALLBACK || p.mode == LM_SEEDED_COST) && bad) {
       // the seed did not lead to a converged fit: the reference's start
       // strategy decides, and the lower cost wins
       double t2[LM_NP], c2;
@@ -661,14 +675,15 @@ extern "C" int ddm_fit_lm_model(int32_t nfit, int32_t nt_max, int32_t K, const i
   if (nfit < 0 || nt_max < 1 || nt_max > ddm::LM_MAX_LAGS || K < 1 || K > ddm::LM_MAX_NODES)
     return lm_fail(DDM_ERR_ARG, "ddm_fit_lm: need nfit >= 0, 1 <= nt_max <= %d, 1 <= K <= %d",
                    ddm::LM_MAX_LAGS, ddm::LM_MAX_NODES);
-  if (mode != ddm::LM_PLAIN && mode != ddm::LM_SEEDED && mode != ddm::LM_SEEDED_FALLBACK && mode != ddm::LM_BROWNIAN)
+  if (mode < ddm::LM_PLAIN || mode > ddm::LM_SEEDED_COST)
     return lm_fail(DDM_ERR_ARG,
-                   "ddm_fit_lm: mode must be 0 (reference starts), 1 (seeded), 2 (seeded, fallback) or 3 (Brownian)");
+                   "ddm_fit_lm: mode must be 0 (reference starts), 1 (seeded), 2 (seeded, fallback), 3 (Brownian) "
+                   "or 4 (seeded, fallback by cost)");
   if (max_iter < 1 || nrefine < 1 || nrefine > 64 || !(tol >= 0))
     return lm_fail(DDM_ERR_ARG, "ddm_fit_lm: need max_iter >= 1, 1 <= nrefine <= 64, tol >= 0");
   if (geometry2d != 0 && geometry2d != 1) return lm_fail(DDM_ERR_ARG, "ddm_fit_lm: geometry2d must be 0 or 1");
   if (nfit == 0) return DDM_OK;
-  const bool seeded = mode == ddm::LM_SEEDED || mode == ddm::LM_SEEDED_FALLBACK;
+  const bool seeded = mode == ddm::LM_SEEDED || mode == ddm::LM_SEEDED_FALLBACK || mode == ddm::LM_SEEDED_COST;
   if (!nt || !d || !tau || !qn || !w || !bounds || !theta || !cost || (seeded && !start))
     return lm_fail(DDM_ERR_ARG, "ddm_fit_lm: null array");
   cudaStream_t s = (cudaStream_t)stream;

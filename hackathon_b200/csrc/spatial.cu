@@ -279,8 +279,19 @@ __global__ void __launch_bounds__(256) rows_kernel(RowParams p) {
 #ifndef COLS_PAIRED
 #define COLS_PAIRED 1
 #endif
+// CTAs per SM the power-of-two column kernels' registers are bounded for
+// (the mixed-radix 384 and 768 would spill under a bound of 3). Measured at
+// 512^2 x 1024: unbounded (126 registers, 2 CTAs per SM) 1.383 ms per video,
+// bounded to 3 CTAs (80 registers, no spills) 1.393 ms.
+#ifndef COLS_MIN_BLOCKS
+#define COLS_MIN_BLOCKS 1
+#endif
 template <int N>
-__global__ void __launch_bounds__(256) cols_kernel(ColParams p) {
+__host__ __device__ constexpr int cols_min_blocks() {
+  return pts(N) == 8 ? COLS_MIN_BLOCKS : 1;
+}
+template <int N>
+__global__ void __launch_bounds__(256, cols_min_blocks<N>()) cols_kernel(ColParams p) {
   constexpr int P = pts(N);
   constexpr int NT = N / P;
   constexpr int G = row_groups<N>();  // frames per tile, one per group

@@ -21,7 +21,7 @@ import numpy as np
 from . import _lib
 
 SWIM_MIN_UM_S = 2.0  # GATES.SWIM_MIN_UM_S, motility_fit.js:28-38
-MODES = {"plain": 0, "seeded": 1, "seeded_fallback": 2, "brownian": 3}
+MODES = {"plain": 0, "seeded": 1, "seeded_fallback": 2, "brownian": 3, "seeded_cost": 4}
 MAX_LAGS = 128
 MAX_NODES = 8
 
@@ -147,7 +147,7 @@ def fit_lm(d, tau, qn, w, bnds, mode="plain", start=None, nt=None, max_iter=200,
     ntv = np.ascontiguousarray(np.full(nfit, nt_max) if nt is None else nt, np.int32)
     m = MODES[mode]
     st = None
-    if mode in ("seeded", "seeded_fallback"):
+    if mode in ("seeded", "seeded_fallback", "seeded_cost"):
         st = np.ascontiguousarray(start, np.float32).reshape(nfit, 4)
     theta = np.zeros((nfit, 6))
     cost = np.zeros(nfit)

@@ -203,7 +203,9 @@ def predict_starts(net, x, bnds):
 
 def compare_fits(net, data, bnds, max_iter=200, tol=1e-10, nrefine=3):
     """Plain LM (reference starts), surrogate-seeded LM, and surrogate-seeded
-    LM with the plain strategy as fallback, on the same curves; each
+    LM with the plain strategy as fallback -- on non-convergence or a cost
+    above a coarse Brownian scan ("fallback", mode 2), or on a cost above the
+    bin's Brownian optimum alone ("costfb", mode 4) -- on the same curves; each
     device-timed with CUDA events on one stream (the seeded timings include
     the surrogate's inference)."""
     import torch
@@ -216,7 +218,8 @@ def compare_fits(net, data, bnds, max_iter=200, tol=1e-10, nrefine=3):
     ntv = torch.full((n,), nt, dtype=torch.int32, device="cuda")
     predict_starts(net, data["x"][:8], bnds)  # first-call set-up outside the timed region
     res = {}
-    for name, mode in (("plain", "plain"), ("seeded", "seeded"), ("fallback", "seeded_fallback")):
+    for name, mode in (("plain", "plain"), ("seeded", "seeded"), ("fallback", "seeded_fallback"),
+                       ("costfb", "seeded_cost")):
         theta = torch.empty((n, 6), dtype=torch.float64, device="cuda")
         cost = torch.empty(n, dtype=torch.float64, device="cuda")
         iters = torch.empty(n, dtype=torch.int32, device="cuda")
@@ -237,7 +240,7 @@ def compare_fits(net, data, bnds, max_iter=200, tol=1e-10, nrefine=3):
     p = res["plain"]
     summary = dict(n=n, plain_qfits_per_s=p["qfits_per_s"], plain_mean_iters=float(p["iters"].mean()),
                    plain_mean_evals=float(p["evals"].mean()))
-    for name in ("seeded", "fallback"):
+    for name in ("seeded", "fallback", "costfb"):
         r = res[name]
         equal = r["cost"] <= p["cost"] * (1 + 1e-3) + 1e-30
         ratio = r["cost"] / np.maximum(p["cost"], 1e-300)
@@ -253,7 +256,7 @@ def compare_fits(net, data, bnds, max_iter=200, tol=1e-10, nrefine=3):
     # vbar (curves whose label has a motile fraction >= 0.2)
     lab = np.asarray(data["theta"], np.float64)
     motile = lab[:, 2] >= 0.2
-    for name in ("plain", "seeded", "fallback"):
+    for name in ("plain", "seeded", "fallback", "costfb"):
         th = res[name]["theta"]
         eD = np.abs(np.exp(th[:, 5]) / lab[:, 5] - 1)
         ev = np.abs(np.exp(th[:, 3]) / lab[:, 3] - 1)[motile]

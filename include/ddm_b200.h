@@ -385,6 +385,10 @@ int ddm_batch_launch_graph(ddm_batch *b);
  *           (alpha = 0) scan -- impossible at a global optimum, since the
  *           Brownian model is nested -- also runs mode 0 and keeps the lower
  *           cost (the reference's starts as the fallback).
+ *   mode 4: as mode 1; the fallback to mode 0 is decided by the cost alone:
+ *           it runs when the seeded cost exceeds the bin's Brownian optimum
+ *           (mode 3's search, FP64 model). A seeded LM stopped at max_iter
+ *           below that bound is kept.
  *   mode 3: the Brownian model alone, A (1 - <exp(-D q_n^2 tau)>) + B, one D
  *           per bin by fitBrownian's search (the 49-point scan + golden
  *           section of mode 0); theta = (A, B, 0, ln vmin, ln Zmin, ln D),

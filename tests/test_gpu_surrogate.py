@@ -53,6 +53,28 @@ def test_seeded_fallback_recovers_from_bad_seeds():
     assert (fb.cost <= plain.cost * (1 + 1e-3) + 1e-30).mean() >= 0.95
 
 
+def test_seeded_cost_fallback_rule():
+    """Mode 4: a seeded fit above the bin's Brownian optimum (mode 3 on the
+    same curve) falls back to the plain strategy and keeps the lower cost, so
+    it ends at or below the plain fit's cost; every kept seeded fit is at or
+    below the Brownian optimum."""
+    data = ST.analytic_set(256, seed=3)
+    bnds = ST.swim_bounds(data["qn"])
+    d = data["d"].cpu().numpy()
+    tau = ST.lm_tau()
+    w = 1 / d.max(1)
+    plain = F.fit_lm(d, tau, data["qn"], w, bnds, mode="plain")
+    brown = F.fit_lm(d, tau, data["qn"], w, bnds, mode="brownian")
+    bad = np.tile([0.5, bnds[1] * 0.99, 90.0, bnds[4] * 1.01], (256, 1))  # far from every truth
+    good = np.stack([data["theta"][:, 2], data["theta"][:, 3], data["theta"][:, 4], data["theta"][:, 5]], 1)
+    for start in (bad, good):
+        r = F.fit_lm(d, tau, data["qn"], w, bnds, mode="seeded_cost", start=start.astype(np.float32))
+        fell = ((r.status >> 1) & 1).astype(bool)
+        assert np.all(r.cost[fell] <= plain.cost[fell] * (1 + 1e-12) + 1e-30)
+        assert np.all(r.cost[~fell] <= brown.cost[~fell] * (1 + 1e-9) + 1e-30)
+    assert fell.mean() < 0.2  # from the generator's own parameters few fits fall back
+
+
 def test_trained_surrogate_gains_over_plain_lm():
     """Equal fit error = final cost within 1e-3 of the plain LM's (or lower)."""
     net = ST.build_and_train(n_analytic=1 << 18, epochs=16, seed=0, batch_max=4096)

@@ -9,9 +9,9 @@ analyzeRadial, motility-ddm/src/ddm_ref.js:196-206, 425-437).
   value  frames/s with the frames already in HBM (device-timed, CUDA events on
          the engine's stream, max over ranks, summed over ranks)
   e2e    the same through the C ABI from pinned HOST frames: every step copies
-         its frames host->device and reads the radial record back; two engines
-         take the videos in turn, so one video's copies overlap the previous
-         video's temporal analysis
+         its frames host->device and reads the radial record back; three
+         engines take the videos in turn, so one video's copies overlap the
+         previous videos' temporal analyses
 Under torchrun each rank analyses its own video (weak scaling, no collective
 on the data path).
 
@@ -156,6 +156,7 @@ def _profile_traffic():
 # q-bin from bin 3 on (25.2 % of the binned modes at 256 bins), on the
 # video's real history
 CPU_BIN_STRIDE = 4
+E2E_ENGINES = 3  # engines taking videos in turn in the e2e measurement
 
 
 def _sampled_bins(bins, stride):
@@ -830,22 +831,28 @@ def main():
     ms_step = ms / args.steps
     value = R.weak_scaling_throughput(T, ms_step, world)
 
-    # ---------------- e2e: pinned host frames through the C ABI. Two engines
-    # take videos in turn (a user with a stream of videos): while one
+    # ---------------- e2e: pinned host frames through the C ABI. Three
+    # engines take videos in turn (a user with a stream of videos): while one
     # video's temporal analysis runs, the next video's frames already cross
-    # PCIe into the other engine; every video's radial record is read back.
-    # (Measured alternatives, no faster: two host threads, one per engine;
-    # ddm_ingest_frames_async with the host's set-up overlapping the copies;
-    # four staging buffers instead of two.)
+    # PCIe into the next engine; every video's radial record is read back,
+    # two videos behind the ingest, so the host's reads and queueing never
+    # wait on an analysis that is still running. (Measured on one B200 at
+    # 512^2 x 1024: two engines 94.7-96.3K frames/s, three 101.2K; no faster:
+    # two host threads, one per engine; ddm_ingest_frames_async with the
+    # host's set-up overlapping the copies; four staging buffers instead of
+    # two.)
     host = frames.view(torch.int16).cpu().pin_memory()
     rad_bytes = 8 * (NB * L + NB + NB * L * 8)
     eng.set_stream(stream.cuda_stream)
-    eng2 = H.DdmEngine.create(N=N, T=T, TPAD=TPAD, L=L, NB=NB, kmin=KMIN, kmax=KMAX)
-    eng2.set_spatial_mask(mask_roi)
-    eng2.set_tuning(tune["best_chunk"], tune["best_unit"], tune["best_variant"])
-    stream2 = torch.cuda.Stream()
-    eng2.set_stream(stream2.cuda_stream)
-    engs = (eng, eng2)
+    engs, e2e_streams = [eng], [stream]
+    for _ in range(E2E_ENGINES - 1):
+        ex = H.DdmEngine.create(N=N, T=T, TPAD=TPAD, L=L, NB=NB, kmin=KMIN, kmax=KMAX)
+        ex.set_spatial_mask(mask_roi)
+        ex.set_tuning(tune["best_chunk"], tune["best_unit"], tune["best_variant"])
+        sx = torch.cuda.Stream()
+        ex.set_stream(sx.cuda_stream)
+        engs.append(ex)
+        e2e_streams.append(sx)
 
     # the radial records come back into pinned host buffers reused across
     # videos (read_radial(out=...)): 9.4 MB at the link's rate, 0.2 ms
@@ -853,30 +860,35 @@ def main():
     rad_out = [torch.empty(n, dtype=torch.float64).pin_memory().numpy() for n in (NB * L, NB, NB * L * 8)]
 
     def e2e_run(n):
-        prev = None
+        pending, radial = [], None
         for i in range(n):
-            x = engs[i % 2]
+            x = engs[i % len(engs)]
             x.ingest_frames(host, slots, scale)
             x.compute_temporal(order, tmask, full=False, wait=False)
-            if prev is not None:
-                prev.read_radial(out=rad_out)
-            prev = x
-        return prev.read_radial(out=rad_out)
+            pending.append(x)
+            if len(pending) == len(engs):  # the engine the next video goes to
+                radial = pending.pop(0).read_radial(out=rad_out)
+        while pending:
+            radial = pending.pop(0).read_radial(out=rad_out)
+        return radial
 
-    e2e_run(2)
+    e2e_run(E2E_ENGINES)
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    stream2.wait_stream(stream)
+    for sx in e2e_streams[1:]:
+        sx.wait_stream(stream)
     radial = e2e_run(args.e2e_steps)
-    stream.wait_stream(stream2)
+    for sx in e2e_streams[1:]:
+        stream.wait_stream(sx)
     e1.record(stream)
     torch.cuda.synchronize()
     ms_e2e = e0.elapsed_time(e1)
-    eng2.destroy()
+    for ex in engs[1:]:
+        ex.destroy()
     ms_e2e = R.max_over_ranks(ms_e2e, dist, device="cuda")
     e2e = R.weak_scaling_throughput(T * args.e2e_steps, ms_e2e, world)
     # the link's ceiling for context: one plain pinned host->device copy of a video
@@ -1029,7 +1041,7 @@ def main():
                            "l2": "inputs larger than L2 (537 MB frames, 1.08 GB history per video)",
                            "autotuned": {"chunk": tune["best_chunk"], "unit": tune["best_unit"],
                                          "temporal_variant": tune["best_variant"]}},
-                "e2e": {"value": e2e, "unit": "frames/s", "pipeline": "two engines take videos in turn",
+                "e2e": {"value": e2e, "unit": "frames/s", "pipeline": f"{E2E_ENGINES} engines take videos in turn",
                         "h2d_GBps": host.numel() * 2 * args.e2e_steps / (ms_e2e * 1e6),
                         "h2d_GBps_plain_copy": h2d_gbps,
                         "h2d_bytes_per_step": int(host.numel() * 2),

@@ -4,7 +4,7 @@
 // No counterpart in the reference (a learned seed for the fit, required by
 // the batched-LM design); its prediction only ever seeds the batched LM
 // (ddm_fit_lm mode 1), and the LM from the reference's start strategy stays
-// the fallback and the judge of its error.
+// the fallback and the reference its error is measured against.
 //
 // Every matrix product is one tcgen05 kernel (gemm_kernel): 128 x N output
 // tiles, BF16 operands staged K-major in shared memory (64-wide K chunks,

@@ -8,7 +8,7 @@ dynamic contrast = 1 - non-motile fraction), ln vbar, ln Z (Schulz width),
 ln D, and ln tau_e (the lag where the model column first reaches 1 - 1/e;
 an extension with no reference counterpart). The prediction seeds the
 batched LM (ddm_fit_lm mode 1); the LM from the reference's start strategy
-(mode 0) remains the fallback and the judge of the error.
+(mode 0) remains the fallback and the reference its error is measured against.
 """
 import ctypes as C
 

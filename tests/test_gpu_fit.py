@@ -45,7 +45,7 @@ def _same_basin(a, b):
 MAX_ITER = 200
 
 
-def _judge(pairs, cap=MAX_ITER):
+def _compare_fits(pairs, cap=MAX_ITER):
     """pairs of (theta_gpu, cost_gpu, theta_oracle, cost_oracle, oracle
     iterations); `cap` = the oracle's iteration budget for one fit."""
     other_basin, bad = 0, []
@@ -84,7 +84,7 @@ def test_lm_seeded_matches_oracle(noise):
     pairs = [(res.theta[i], res.cost[i]) + O.lm_fit_start(c["d"], tau, c["qn"], c["w"], b6, start[i],
                                                           max_iter=MAX_ITER)
              for i, c in enumerate(cases)]
-    _judge(pairs)
+    _compare_fits(pairs)
 
 
 @pytest.mark.parametrize("noise", [0.0, 1e-3])
@@ -95,7 +95,7 @@ def test_lm_plain_matches_oracle(noise):
     res = fit.fit_lm(d, tau, qn, w, b6, mode="plain")
     pairs = [(res.theta[i], res.cost[i]) + O.lm_fit_plain(c["d"], tau, c["qn"], c["w"], b6, max_iter=MAX_ITER)[:3]
              for i, c in enumerate(cases)]
-    _judge(pairs, cap=3 * MAX_ITER)  # three refined starts
+    _compare_fits(pairs, cap=3 * MAX_ITER)  # three refined starts
     assert (res.iters > 0).all() and (res.evals > 100).all()
 
 

@@ -949,6 +949,40 @@ def main():
         lib = {"temporal": {"what": f"torch.fft (cuFFT): {nbinned} forward + {n_inv} inverse {TPAD}-point C2C "
                                     "transforms, device-resident, no other work",
                             "ms": statistics.median(times)}}
+        if T == 1024 and TPAD == 2048:
+            # the forward transforms alone on the tensor cores (ddm_dft2048_tc,
+            # BF16 three-term split) against cuFFT's forward transforms alone
+            import ctypes
+            from hackathon_b200 import _lib as LIB
+            lib_so = LIB.load()
+            X = torch.empty((nbinned, TPAD), dtype=torch.complex64, device="cuda")
+            tf, tt = [], []
+            for r in range(4):
+                torch.cuda.synchronize()
+                f0.record()
+                y = torch.fft.fft(x, n=TPAD, dim=1)
+                f1.record()
+                torch.cuda.synchronize()
+                if r:
+                    tf.append(f0.elapsed_time(f1))
+                f0.record()
+                rc = lib_so.ddm_dft2048_tc(ctypes.c_void_p(x.data_ptr()), T, nbinned, ctypes.c_void_p(X.data_ptr()),
+                                           ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+                f1.record()
+                torch.cuda.synchronize()
+                if rc:
+                    raise RuntimeError(lib_so.ddm_create_error().decode())
+                if r:
+                    tt.append(f0.elapsed_time(f1))
+            s64 = slice(0, 64)
+            rms = torch.sqrt(torch.mean(torch.abs(y[s64]) ** 2, dim=1))
+            err = float((torch.abs(X[s64] - y[s64]).max(dim=1).values / rms).max())
+            lib["tensor_core_forward"] = {
+                "what": f"{nbinned} forward {TPAD}-point transforms of {T} samples, FP32 in and out: tcgen05 "
+                        "four-step DFT (BF16 three-term split) against cuFFT",
+                "tcgen05_ms": statistics.median(tt), "cufft_ms": statistics.median(tf),
+                "max_err_vs_cufft_of_rms": err}
+            del X, y
         del x
         # and the spatial stage's: a 2D real-to-half-plane FFT of every frame
         # already in FP32 (no conversion, window, mean or transposed store)

@@ -105,6 +105,7 @@ _SIGS = {
     "ddm_analyze_motility_batch": (C.c_int, [_i32, C.POINTER(RadialView), C.POINTER(MotilityOptions),
                                              C.POINTER(MotilityResult)]),
     "ddm_isf_eval": (C.c_int, [_i32, _i32, _vp, _vp, _vp, _vp, _vp]),
+    "ddm_dft2048_tc": (C.c_int, [_vp, C.c_int64, _i32, _vp, _vp]),
     "ddm_create_banded": (C.c_int, [C.POINTER(Geometry), C.c_uint64, C.POINTER(_vp)]),
     "ddm_get_bands": (C.c_int, [_vp, C.POINTER(_i32), C.POINTER(_i32)]),
     "ddm_analyze_banded": (C.c_int, [_vp, _vp, _i32, _i32, _vp, C.c_float, _vp, _vp, _i32]),

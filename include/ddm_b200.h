@@ -298,6 +298,15 @@ int ddm_analyze_motility_batch(int32_t n, const ddm_radial_view *radials,
  * isf2dFast (:168-220). */
 int ddm_isf_eval(int32_t n, int32_t geometry2d, const double *x, const double *Z,
                  double *g, double *xdgdx, double *Zdgdz);
+/* Batched zero-padded 2048-point DFT on the tensor cores (no reference
+ * counterpart; a measured reference point for the temporal stage's forward
+ * transforms, not on the analysis path): X[i][k] = sum_{t<1024} x[i*ld + t]
+ * exp(-2 pi i t k / 2048), k < 2048, for n series. x: DEVICE complex64, ld
+ * >= 1024 elements between series; X: DEVICE complex64 [n][2048]. tcgen05
+ * BF16 products with a three-term split, FP32 accumulation: within ~2e-5 of
+ * each series' RMS spectrum. Queued on `stream` (cudaStream_t as void*) and
+ * waited for; errors via ddm_create_error(). */
+int ddm_dft2048_tc(const void *x, int64_t ld, int32_t n, void *X, void *stream);
 /* The host half of the analysis on its own (no device needed). The q-bins
  * are those prepare() keeps (motility_fit.js:383-401): ddm_prepared_bins
  * returns their Radial indices (bins may be NULL to query the count; up to

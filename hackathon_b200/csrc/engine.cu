@@ -471,7 +471,7 @@ static int create_impl(const ddm_geometry *geometry, uint64_t band_budget, ddm_e
   const std::vector<double> w = blackman_harris(N);
   std::vector<float> wf(N);
   for (int i = 0; i < N; i++) wf[i] = (float)w[i];
-  std::vector<float> tws = twiddle_table(N), twt = twiddle_table(g.TPAD), twt16 = twiddle_table(g.TPAD, 16);
+  std::vector<float> tws = twiddle_table(N, spatial_twiddle_radix(N)), twt = twiddle_table(g.TPAD), twt16 = twiddle_table(g.TPAD, 16);
   // DFT of the window at kx = 0..3 (zero beyond for the 4-term window)
   float wc4[8];
   for (int kx = 0; kx < 4; kx++) {

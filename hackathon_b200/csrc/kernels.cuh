@@ -144,6 +144,8 @@ cudaError_t launch_cref(int N, int dtype, const void* frames, long long frame_st
 // frames handled by one column-kernel CTA (one per FFT group); ingest chunks
 // are multiples of it
 int frames_per_col_cta(int N);
+// Largest radix of the spatial transforms' plan for N (the twiddle table's layout).
+int spatial_twiddle_radix(int N);
 cudaError_t launch_temporal(int TPAD, int L, bool full, const TemporalParams& p, int grid,
                             cudaStream_t s);
 int temporal_max_grid(int TPAD, int T, int L, bool full, int variant = 0, bool sparse = false);

@@ -44,9 +44,28 @@ __device__ __forceinline__ float ld_pix(const Tin* p) {
   return (float)__ldg(p);
 }
 
+// The 2048-point rows and columns take the radix-16 plan (16 points per
+// thread, 2048 = 16 x 16 x 8: three passes through shared memory instead of
+// the radix-8 plan's four, two FFT groups of 128 threads per CTA, one
+// in-place buffer per group).
+#ifndef SPATIAL_R16
+#define SPATIAL_R16 1
+#endif
+__host__ __device__ constexpr bool r16(int N) { return SPATIAL_R16 && N == 2048; }
+
 // Points per thread of an N-point transform: 8 (radix-8 plan) for powers of
-// two, 24 (mixed radix, fft_p) for the sizes with a factor 3 (384, 768).
-__host__ __device__ constexpr int pts(int N) { return N % 3 == 0 ? 24 : 8; }
+// two, 16 for the radix-16 plan, 24 (mixed radix, fft_p) for the sizes with a
+// factor 3 (384, 768).
+__host__ __device__ constexpr int pts(int N) { return r16(N) ? 16 : N % 3 == 0 ? 24 : 8; }
+
+// Shared-memory index of point k of a transform's natural-order result.
+template <int N>
+__device__ __forceinline__ int padk(int k) {
+  if constexpr (r16(N))
+    return pad16(k);
+  else
+    return pad(k);
+}
 
 template <int N>
 __host__ __device__ constexpr int row_groups() {
@@ -56,7 +75,7 @@ __host__ __device__ constexpr int row_groups() {
 // twiddle table length and barrier scope of the plan of N
 template <int N>
 __host__ __device__ constexpr int tw_count() {
-  return pts(N) == 8 ? tw_size(N) : tw_size_p(N);
+  return r16(N) ? tw_size16(N) : pts(N) == 8 ? tw_size(N) : tw_size_p(N);
 }
 template <int N>
 __host__ __device__ constexpr int sync_of() {
@@ -75,10 +94,14 @@ __host__ __device__ constexpr int sync_of() {
 template <int N, bool INV, int SYNC>
 __device__ __forceinline__ float2* fft_n(float2 (&v)[pts(N)], int t, float2* buf0, float2* buf1,
                                          const float2* __restrict__ tw, int bar_id) {
-  if constexpr (pts(N) == 8)
+  if constexpr (r16(N)) {
+    fft16<N, INV>(v, t, buf0, tw, bar_id);  // in place in the group's one buffer
+    return buf0;
+  } else if constexpr (pts(N) == 8) {
     return fft<N, INV, true, SYNC, SPATIAL_TW_REC>(v, t, buf0, buf1, tw, bar_id);
-  else
+  } else {
     return fft_p<N, pts(N), INV, SYNC>(v, t, buf0, buf1, tw, bar_id);
+  }
 }
 constexpr int ROW_STAGES = 2;  // depth of the row-batch staging ring
 
@@ -91,7 +114,7 @@ constexpr int ROW_STAGES = 2;  // depth of the row-batch staging ring
 // the groups stay 16-byte aligned.
 template <int N>
 __host__ __device__ constexpr int GSTRIDE() {
-  return 2 * padded(N) + (N >= 512 ? 4 : 2);
+  return r16(N) ? N + 4 : 2 * padded(N) + (N >= 512 ? 4 : 2);  // the radix-16 plan: one buffer
 }
 
 // The pixels whose mean is a frame's reference level c_f: a 16 x 16 grid at
@@ -134,8 +157,20 @@ __global__ void __launch_bounds__(CREF) cref_kernel(const Tin* __restrict__ fram
 // cp.async.bulk) issued ROW_STAGES batches ahead into a ring, so raw pixels
 // never sit in registers waiting and the copy engine, not the warps, moves
 // them.
+// CTAs per SM the radix-16 rows kernel's registers are bounded for: two (128
+// registers, 12 B spilled) against one (158 registers). Measured at 2048^2
+// with a pixel mask, spatial stage per frame: radix-8 plan 32.0 us, radix-16
+// with one CTA per SM 30.0 us, with two 28.4 us; the history within 1.4e-6 of
+// its RMS of the radix-8 plan's.
+#ifndef ROWS16_MIN_BLOCKS
+#define ROWS16_MIN_BLOCKS 2
+#endif
+template <int N>
+__host__ __device__ constexpr int rows_min_blocks() {
+  return r16(N) ? ROWS16_MIN_BLOCKS : 1;
+}
 template <int N, typename Tin>
-__global__ void __launch_bounds__(256) rows_kernel(RowParams p) {
+__global__ void __launch_bounds__(256, rows_min_blocks<N>()) rows_kernel(RowParams p) {
   constexpr int P = pts(N);
   constexpr int NT = N / P;
   constexpr int G = row_groups<N>();
@@ -250,8 +285,8 @@ __global__ void __launch_bounds__(256) rows_kernel(RowParams p) {
 #pragma unroll
         for (int c = 0; c < KB; c++) {
           const int kx = kb * KB + c;
-          const float2 zk = Zg[pad(kx < N ? kx : 0)];
-          const float2 zn = Zg[pad((N - kx) % N)];
+          const float2 zk = Zg[padk<N>(kx < N ? kx : 0)];
+          const float2 zn = Zg[padk<N>((N - kx) % N)];
           R[c] = (rr & 1) ? make_float2(0.5f * (zk.y + zn.y), -0.5f * (zk.x - zn.x))
                           : make_float2(0.5f * (zk.x + zn.x), 0.5f * (zk.y - zn.y));
           if (kx > N / 2) R[c] = make_float2(0.f, 0.f);  // past the half plane
@@ -614,6 +649,155 @@ __global__ void __launch_bounds__(256, 1) cols_wide_kernel(ColParams p) {
   }
 }
 
+// Column pass for the radix-16 plan (N = 2048): the same tiles (column pair
+// kb, WIDE_F frames) and stores as cols_wide_kernel, with two FFT groups of
+// N/16 threads. An item is one frame's [KB][N] block, staged by one bulk copy
+// into a two-deep ring; group g transforms column g of the pair in place in
+// its output slab R[g][frame], so the CTA runs both columns of a frame at once
+// (one group idles on a lone last column, kx = N/2).
+template <int N>
+__global__ void __launch_bounds__(256, 1) cols_wide16_kernel(ColParams p) {
+  constexpr int NT = N / 16;
+  constexpr int F = WIDE_F;
+  constexpr uint32_t FRAME_ELEMS = N * KB;
+  constexpr uint32_t FRAME_BYTES = FRAME_ELEMS * sizeof(float2);
+  static_assert(2 * NT == 256 && KB == 2, "one group per column of the pair");
+  extern __shared__ __align__(16) float2 sm[];
+  float2* ring = sm;                  // [2][KB][N] staged blocks, one frame each
+  float2* R = ring + 2 * FRAME_ELEMS;  // [KB][F][N] column transforms of the tile
+  float2* s_tw = R + KB * F * N;
+  __shared__ __align__(8) uint64_t bar[2];
+  __shared__ float s_dc[F];
+  __shared__ float2 s_wc4[4];
+  const int g = threadIdx.x / NT, t = threadIdx.x % NT;
+  for (int i = threadIdx.x; i < tw_size16(N); i += blockDim.x) s_tw[i] = p.tw[i];
+  if (threadIdx.x < 4) s_wc4[threadIdx.x] = p.wc4[threadIdx.x];
+  const int nfg = (p.nframes + F - 1) / F;
+  const int NKB = p.nkb > 0 ? p.nkb : p.NHB, kb0 = p.kb0;  // the column blocks of the history band
+  const int W = p.hist_w > 0 ? p.hist_w : p.NH;            // columns per history row
+  const int ntiles = NKB * nfg;
+  const float invN = 1.f / N;
+  const double inv_total = p.inv_total[0];
+  auto items_of = [&](int tile) { return min(F, p.nframes - (tile / NKB) * F); };
+  auto issue = [&](int tile, int j, int s) {
+    const int kb = kb0 + tile % NKB, f = (tile / NKB) * F + j;
+    mbar_arrive_expect_tx(&bar[s], FRAME_BYTES);
+    bulk_g2s(ring + s * FRAME_ELEMS, p.rows + ((size_t)f * p.NHB + kb) * FRAME_ELEMS, FRAME_BYTES, &bar[s]);
+  };
+  auto advance = [&](int& tile, int& j) {
+    if (++j >= items_of(tile)) {
+      j = 0;
+      tile += gridDim.x;
+    }
+  };
+  // thread 0 keeps the issue cursor two items ahead of the consumer
+  int it_tile = blockIdx.x, it_j = 0;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fence_barrier_init();
+    for (int s = 0; s < 2 && it_tile < ntiles; s++) {
+      issue(it_tile, it_j, s);
+      advance(it_tile, it_j);
+    }
+  }
+  __syncthreads();
+  int e = 0;  // items consumed by this CTA
+  constexpr int SPT = 256 / F;  // ky stride of the store loop
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int kb = kb0 + tile % NKB;
+    const int f0 = (tile / NKB) * F;
+    const int nf = min(F, p.nframes - f0);
+    const bool col_ok = kb * KB + g < p.NH;  // the last block holds one column
+    if (threadIdx.x < nf) {
+      const int f = f0 + threadIdx.x;
+      const double mu = p.framesum[f] * inv_total;
+      s_dc[threadIdx.x] = (float)(((double)p.framec[f] - mu) * (double)p.scale / N);
+      if (kb == kb0) p.means[f] = mu * (double)p.scale;
+    }
+    if (p.w2d && threadIdx.x == 0) {
+      // the correction rows of this tile's columns into L2 ahead of the stores
+      const int ncol = min(KB, p.NH - kb * KB);
+      asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p.w2d + (size_t)kb * KB * N),
+                   "r"((uint32_t)(ncol * N * sizeof(float2)))
+                   : "memory");
+    }
+    for (int fi = 0; fi < nf; fi++, e++) {
+      const int s = e & 1;
+      if (!mbar_wait(&bar[s], (uint32_t)(e >> 1) & 1u, p.err, 3)) {
+        // give up: let the other copy in flight land (bounded), then stop
+        mbar_wait(&bar[s ^ 1], (uint32_t)((e + 1) >> 1) & 1u, nullptr, 0);
+        return;
+      }
+      float2 v[16];
+      const float2* col = ring + s * FRAME_ELEMS + g * N;
+#pragma unroll
+      for (int q = 0; q < 16; q++) v[q] = col_ok ? col[t + q * NT] : make_float2(0.f, 0.f);
+      // every thread has read ring entry s: its next copy may land
+      fence_proxy_async_smem();
+      __syncthreads();
+      if (threadIdx.x == 0 && it_tile < ntiles) {
+        issue(it_tile, it_j, s);
+        advance(it_tile, it_j);
+      }
+      fft16<N, false>(v, t, R + (size_t)(g * F + fi) * N, s_tw, 1 + g);
+    }
+    __syncthreads();  // R and s_dc complete
+    // store: thread -> (frame sf, ky); lanes 4k..4k+3 write one mode's four slots
+    const int sf = threadIdx.x % F;
+    if (sf < nf) {
+      const int slot = p.slots[f0 + sf];
+      const float dc = s_dc[sf];
+      const size_t mstride = (size_t)W * p.T;
+#pragma unroll 1
+      for (int c = 0; c < KB; c++) {
+        const int kx = kb * KB + c;
+        if (kx >= p.NH) break;
+        const float2* ys = R + (size_t)(c * F + sf) * N;
+        float2* hs = p.hist + (size_t)(kx - kb0 * KB) * p.T + slot;
+        const float2 wkx = kx < 4 ? s_wc4[kx] : make_float2(0.f, 0.f);
+        if (p.w2d) {
+          // correction table loads run one batch of WB ahead of the stores
+          constexpr int WB = 8, NI = N / SPT;
+          static_assert(NI % WB == 0, "store batches");
+          const float2* wcol = p.w2d + (size_t)kx * N + threadIdx.x / F;
+          float2 wcur[WB], wnxt[WB];
+#pragma unroll
+          for (int j = 0; j < WB; j++) wcur[j] = __ldg(&wcol[j * SPT]);
+#pragma unroll 1
+          for (int i0 = 0; i0 < NI; i0 += WB) {
+            if (i0 + WB < NI)
+#pragma unroll
+              for (int j = 0; j < WB; j++) wnxt[j] = __ldg(&wcol[(i0 + WB + j) * SPT]);
+#pragma unroll
+            for (int j = 0; j < WB; j++) {
+              const int ky = threadIdx.x / F + (i0 + j) * SPT;
+              const float2 y = ys[pad16(ky)];
+              const float2 w = wcur[j];
+              hs[(size_t)ky * mstride] = make_float2(fmaf(dc, w.x, y.x * invN), fmaf(dc, w.y, y.y * invN));
+            }
+#pragma unroll
+            for (int j = 0; j < WB; j++) wcur[j] = wnxt[j];
+          }
+        } else {
+#pragma unroll 8
+          for (int i = 0; i < N / SPT; i++) {
+            const int ky = threadIdx.x / F + i * SPT;
+            const float2 y = ys[pad16(ky)];
+            float2 w = make_float2(0.f, 0.f);
+            if (kx < 4 && (ky < 4 || ky > N - 4)) {
+              const float2 wk = ky < 4 ? s_wc4[ky] : make_float2(s_wc4[N - ky].x, -s_wc4[N - ky].y);
+              w = cmul(wkx, wk);
+            }
+            hs[(size_t)ky * mstride] = make_float2(fmaf(dc, w.x, y.x * invN), fmaf(dc, w.y, y.y * invN));
+          }
+        }
+      }
+    }
+    __syncthreads();  // R and s_dc are rewritten by the next tile
+  }
+}
+
 // ------------------------------------------------------------------ launchers
 
 template <int N>
@@ -724,26 +908,40 @@ __host__ __device__ constexpr bool use_wide_cols(int N) { return N >= 1024; }
 
 template <int N>
 static size_t cols_wide_smem() {
-  constexpr int G = groups<N>();
-  return ((size_t)2 * G * N * KB + (size_t)KB * WIDE_F * N + (size_t)G * N + tw_size(N)) * sizeof(float2);
+  if constexpr (r16(N)) {  // ring of two one-frame blocks, the tile's slabs, radix-16 twiddles
+    return ((size_t)2 * N * KB + (size_t)KB * WIDE_F * N + tw_size16(N)) * sizeof(float2);
+  } else {
+    constexpr int G = groups<N>();
+    return ((size_t)2 * G * N * KB + (size_t)KB * WIDE_F * N + (size_t)G * N + tw_size(N)) * sizeof(float2);
+  }
 }
 
 template <int N>
 static cudaError_t cols_n(const ColParams& p, cudaStream_t s) {
   constexpr int G = groups<N>();
-  if constexpr (use_wide_cols(N)) {
+  const long long wide_tiles = (long long)(p.nkb > 0 ? p.nkb : p.NHB) * ((p.nframes + WIDE_F - 1) / WIDE_F);
+  if constexpr (r16(N)) {
+    auto k = cols_wide16_kernel<N>;
+    const size_t sm = cols_wide_smem<N>();
+    const int grid = persistent_grid(k, 256, sm, wide_tiles);
+    k<<<grid, 256, sm, s>>>(p);
+    return cudaGetLastError();
+  } else if constexpr (use_wide_cols(N)) {
     auto k = cols_wide_kernel<N>;
     const size_t sm = cols_wide_smem<N>();
-    const int grid = persistent_grid(k, G * (N / 8), sm, (long long)(p.nkb > 0 ? p.nkb : p.NHB) * ((p.nframes + WIDE_F - 1) / WIDE_F));
+    const int grid = persistent_grid(k, G * (N / 8), sm, wide_tiles);
+    k<<<grid, G * (N / pts(N)), sm, s>>>(p);
+    return cudaGetLastError();
+  } else {
+    auto k = cols_kernel<N>;
+    const size_t sm = fft_smem<N>() + (size_t)G * N * KB * sizeof(float2);
+    const int grid = persistent_grid(k, G * (N / pts(N)), sm, (long long)(p.nkb > 0 ? p.nkb : p.NHB) * ((p.nframes + G - 1) / G));
     k<<<grid, G * (N / pts(N)), sm, s>>>(p);
     return cudaGetLastError();
   }
-  auto k = cols_kernel<N>;
-  const size_t sm = fft_smem<N>() + (size_t)G * N * KB * sizeof(float2);
-  const int grid = persistent_grid(k, G * (N / pts(N)), sm, (long long)(p.nkb > 0 ? p.nkb : p.NHB) * ((p.nframes + G - 1) / G));
-  k<<<grid, G * (N / pts(N)), sm, s>>>(p);
-  return cudaGetLastError();
 }
+
+int spatial_twiddle_radix(int N) { return N == 2048 && r16(2048) ? 16 : 8; }
 
 cudaError_t launch_cols(int N, const ColParams& p, cudaStream_t s) {
   switch (N) {

@@ -826,18 +826,29 @@ static int temporal_impl(ddm_engine *h, const uint32_t *order, const float *mask
     const int grid = std::min(temporal_max_grid(TPAD, T, L, true, 0, tp.sparse != 0), h->nunits_full);
     CK(cudaMemsetAsync(h->d_counter, 0, sizeof(int), st));
     CKL(launch_temporal(TPAD, L, true, tp, std::max(grid, 1), st));
-    RadialFullParams rp{};
-    rp.D = h->d_fullD;
-    rp.C = h->d_fullC;
-    rp.P = h->d_fullP;
-    rp.items = h->d_items;
-    rp.offsets = h->d_offsets;
+    // the radial record from the full outputs: unit partial records, then
+    // the fused path's reduction over each bin's units in order
+    RadialFullParams fp{};
+    fp.D = h->d_fullD;
+    fp.C = h->d_fullC;
+    fp.P = h->d_fullP;
+    fp.items = h->d_items;
+    fp.units = h->d_units;
+    fp.nunits = h->nunits;
+    fp.L = L;
+    fp.partials = h->d_partials;
+    CKL(launch_radial_full(fp, st));
+    ReduceParams rp{};
+    rp.partials = h->d_partials;
+    rp.bin_units = h->d_bin_units;
+    rp.nmodes = h->d_nmodes;
+    rp.nunits = h->nunits;
     rp.NB = h->g.NB;
     rp.L = L;
-    rp.oD = h->d_radD;
-    rp.oP = h->d_radP;
-    rp.odrift = h->d_radDrift;
-    CKL(launch_radial_full(rp, st));
+    rp.D = h->d_radD;
+    rp.P = h->d_radP;
+    rp.drift = h->d_radDrift;
+    CKL(launch_reduce(rp, st));
     h->full_valid = true;
   } else {
     // the engine's work units, or those of one band of a banded analysis

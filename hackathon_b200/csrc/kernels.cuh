@@ -102,12 +102,10 @@ struct RadialFullParams {
   const float* D;          // [modes][L]
   const float2* C;         // [modes][L]
   const float* P;          // [modes]
-  const int4* items;       // bin-sorted (mode, kx, ky, bin)
-  const uint32_t* offsets; // [NB+1]
-  int NB, L;
-  double* oD;
-  double* oP;
-  double* odrift;
+  const int4* items;       // bin-sorted (mode, kx, ky, 0)
+  const int4* units;       // the fused path's units (first item, count, bin, 0)
+  int nunits, L;
+  double* partials;        // [nunits][PFIELDS][L], then [nunits] P sums (reduce_kernel's input)
 };
 
 enum { LM_PLAIN = 0, LM_SEEDED = 1, LM_SEEDED_FALLBACK = 2, LM_BROWNIAN = 3, LM_SEEDED_COST = 4 };

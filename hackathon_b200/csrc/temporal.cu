@@ -1578,12 +1578,12 @@ __global__ void reduce_kernel(ReduceParams p) {
   }
 }
 
-// Radial reduction of full per-mode outputs, one CTA per bin, one thread per
-// lag, modes of the bin in table order (ddm.wgsl:265-322 with FP64 sums). The
-// mode loop loads RF_AHEAD modes' values before it adds any of them, so that
-// many loads are in flight per thread (the sums still add in table order).
-constexpr int RF_AHEAD = 8;
-
+// Radial sums of full per-mode outputs (ddm.wgsl:265-322 with FP64 sums), in
+// the fused path's work units: block (lag block, unit u) sums the unit's modes
+// (a run of at most U modes of one bin, in table order) at its lags and
+// writes the unit's partial record; reduce_kernel then adds the units of each
+// bin in unit order -- the same reduction as the fused epilogue's, with a
+// unit's loads all issued before its sums.
 __device__ __forceinline__ void radial_full_add(double (&s)[PFIELDS], float D, float2 a, float2 c1, bool next,
                                                 int4 e) {
   s[0] += (double)D;
@@ -1606,47 +1606,40 @@ __device__ __forceinline__ void radial_full_add(double (&s)[PFIELDS], float D, f
 }
 
 __global__ void radial_full_kernel(RadialFullParams p) {
-  const int b = blockIdx.x;
+  const int u = blockIdx.y;
   const int L = p.L;
-  const uint32_t i0 = p.offsets[b], i1 = p.offsets[b + 1];
-  const double n = (double)(i1 - i0);
-  const double inv = i1 > i0 ? 1.0 / n : 0.0;
-  for (int tau = threadIdx.x; tau < L; tau += blockDim.x) {
+  const int tau = blockIdx.x * blockDim.x + threadIdx.x;
+  const int4 U = p.units[u];
+  if (tau < L) {
     double s[PFIELDS];
 #pragma unroll
     for (int c = 0; c < PFIELDS; c++) s[c] = 0.0;
     const bool next = tau + 1 < L;
-    uint32_t i = i0;
-    for (; i + RF_AHEAD <= i1; i += RF_AHEAD) {
-      int4 e[RF_AHEAD];
-      float D[RF_AHEAD];
-      float2 a[RF_AHEAD], c1[RF_AHEAD];
+    constexpr int AH = 8;
+    for (int k0 = 0; k0 < U.y; k0 += AH) {
+      int4 e[AH];
+      float D[AH];
+      float2 a[AH], c1[AH];
 #pragma unroll
-      for (int k = 0; k < RF_AHEAD; k++) e[k] = __ldg(&p.items[i + k]);
-#pragma unroll
-      for (int k = 0; k < RF_AHEAD; k++) {
+      for (int k = 0; k < AH; k++) {
+        e[k] = k0 + k < U.y ? __ldg(&p.items[U.x + k0 + k]) : make_int4(0, 0, 0, 0);
         const size_t m = (size_t)e[k].x;
-        D[k] = __ldg(&p.D[m * L + tau]);
-        a[k] = __ldg(&p.C[m * L + tau]);
-        c1[k] = next ? __ldg(&p.C[m * L + tau + 1]) : make_float2(0.f, 0.f);
+        const bool in = k0 + k < U.y;
+        D[k] = in ? __ldg(&p.D[m * L + tau]) : 0.f;
+        a[k] = in ? __ldg(&p.C[m * L + tau]) : make_float2(0.f, 0.f);
+        c1[k] = in && next ? __ldg(&p.C[m * L + tau + 1]) : make_float2(0.f, 0.f);
       }
 #pragma unroll
-      for (int k = 0; k < RF_AHEAD; k++) radial_full_add(s, D[k], a[k], c1[k], next, e[k]);
+      for (int k = 0; k < AH; k++)
+        if (k0 + k < U.y) radial_full_add(s, D[k], a[k], c1[k], next, e[k]);
     }
-    for (; i < i1; i++) {
-      const int4 e = __ldg(&p.items[i]);
-      const size_t m = (size_t)e.x;
-      radial_full_add(s, __ldg(&p.D[m * L + tau]), __ldg(&p.C[m * L + tau]),
-                      next ? __ldg(&p.C[m * L + tau + 1]) : make_float2(0.f, 0.f), next, e);
-    }
-    p.oD[(size_t)b * L + tau] = s[0] * inv;
 #pragma unroll
-    for (int c = 0; c < DRIFT; c++) p.odrift[((size_t)b * L + tau) * DRIFT + c] = s[c + 1];
+    for (int c = 0; c < PFIELDS; c++) p.partials[((size_t)u * PFIELDS + c) * L + tau] = s[c];
   }
-  if (threadIdx.x == 0) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
     double s = 0.0;
-    for (uint32_t i = i0; i < i1; i++) s += (double)p.P[p.items[i].x];
-    p.oP[b] = s * inv;
+    for (int k = 0; k < U.y; k++) s += (double)p.P[p.items[U.x + k].x];
+    p.partials[(size_t)p.nunits * PFIELDS * L + u] = s;
   }
 }
 
@@ -1862,8 +1855,9 @@ cudaError_t launch_reduce(const ReduceParams& p, cudaStream_t s) {
 }
 
 cudaError_t launch_radial_full(const RadialFullParams& p, cudaStream_t s) {
-  const int threads = p.L >= 256 ? 256 : ((p.L + 31) / 32) * 32;
-  radial_full_kernel<<<p.NB, threads, 0, s>>>(p);
+  if (p.nunits <= 0) return cudaSuccess;
+  const int threads = p.L >= 128 ? 128 : ((p.L + 31) / 32) * 32;
+  radial_full_kernel<<<dim3((p.L + threads - 1) / threads, p.nunits), threads, 0, s>>>(p);
   return cudaGetLastError();
 }
 

@@ -77,6 +77,7 @@ _SIGS = {
     "ddm_compute_temporal_async": (C.c_int, [_vp, _vp, _vp, _i32]),
     "ddm_compute_temporal_live": (C.c_int, [_vp, _vp, _vp, _i32]),
     "ddm_set_sparse": (C.c_int, [_vp, _i32]),
+    "ddm_set_blocked": (C.c_int, [_vp, _i32]),
     "ddm_last_temporal_kernel": (C.c_int, [_vp]),
     "ddm_analysis_poll": (C.c_int, [_vp, _vp]),
     "ddm_wait_analysis": (C.c_int, [_vp]),

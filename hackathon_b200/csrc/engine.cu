@@ -31,6 +31,7 @@ struct ddm_engine {
   ddm_geometry g{};
   int NH = 0, NHB = 0, modes = 0, chunk = 0, chunk_cap = 0, unit_size = 0, variant = 0;
   bool sparse_enabled = true;  // the sparse-mask temporal kernel for masks with few zeros
+  bool blocked_enabled = true;  // the blocked temporal kernel (TPAD 8192, L <= 128)
   int last_tk = -1;             // DDM_TK_* of the last temporal launch
   std::vector<float> meta_mask, meta_npairs, meta_mspec;  // temporal_meta of the last mask
   int device = 0;
@@ -805,7 +806,11 @@ static int temporal_impl(ddm_engine *h, const uint32_t *order, const float *mask
     }
     tp.sparse = h->sparse_enabled && binary && nz <= temporal_sparse_limit(TPAD, T, L, full) ? 1 : 0;
   }
-  h->last_tk = temporal_kernel_id(TPAD, full, h->variant, tp.sparse != 0);
+  if (h->blocked_enabled && temporal_blocked_ok(TPAD, T, L, full)) {  // short lags on a long series
+    tp.variant = 2;
+    tp.sparse = 0;
+  }
+  h->last_tk = temporal_kernel_id(TPAD, full, tp.variant, tp.sparse != 0);
   tp.unit_counter = h->d_counter;
   tp.err = h->d_err;
   tp.T = T;
@@ -857,7 +862,7 @@ static int temporal_impl(ddm_engine *h, const uint32_t *order, const float *mask
     tp.units = band ? band->d_units : h->d_units;
     tp.nunits = nunits;
     tp.partials = h->d_partials;
-    const int grid = std::min(temporal_max_grid(TPAD, T, L, false, h->variant, tp.sparse != 0), nunits);
+    const int grid = std::min(temporal_max_grid(TPAD, T, L, false, tp.variant, tp.sparse != 0), nunits);
     CK(cudaMemsetAsync(h->d_counter, 0, sizeof(int), st));
     if (nunits > 0) CKL(launch_temporal(TPAD, L, false, tp, std::max(grid, 1), st));
     ReduceParams rp{};
@@ -1545,6 +1550,12 @@ extern "C" int ddm_autotune(ddm_engine *h, char *report, int32_t report_len) {
 extern "C" int ddm_set_sparse(ddm_engine *h, int32_t enable) {
   if (!h) return DDM_ERR_ARG;
   h->sparse_enabled = enable != 0;
+  return DDM_OK;
+}
+
+extern "C" int ddm_set_blocked(ddm_engine *h, int32_t enable) {
+  if (!h) return DDM_ERR_ARG;
+  h->blocked_enabled = enable != 0;
   return DDM_OK;
 }
 

@@ -79,7 +79,8 @@ struct TemporalParams {
   int* err;                // error word (bounded waits that timed out)
   int T, L;                // single video; batched: the largest T and L
   const VideoDesc* videos; // nullptr: one video (the fields above); else units[u].w indexes it
-  int variant;             // 0: one-group radix-8 kernel; 1: two-group radix-16 (TPAD 1024..4096)
+  int variant;             // 0: one-group radix-8 kernel; 1: two-group radix-16 (TPAD 1024..4096);
+                           // 2: blocked kernel (TPAD 8192, L <= 128, fused radial path)
   int sparse;              // 1: single video whose mask has <= SPARSE_ZMAX zeros: A+B from
                            // prefix sums (temporal_sparse_kernel); 0: by transforms
 };
@@ -155,6 +156,8 @@ bool temporal_sparse_ok(int TPAD);
 int temporal_sparse_limit(int TPAD, int T, int L, bool full);
 // which temporal kernel launch_temporal runs for these settings (DDM_TK_*)
 int temporal_kernel_id(int TPAD, bool full, int variant, bool sparse);
+// The blocked kernel (variant 2) serves this analysis: TPAD 8192, L <= 128, fused path.
+bool temporal_blocked_ok(int TPAD, int T, int L, bool full);
 cudaError_t launch_reduce(const ReduceParams& p, cudaStream_t s);
 cudaError_t launch_radial_full(const RadialFullParams& p, cudaStream_t s);
 cudaError_t launch_lm(const LmParams& p, cudaStream_t s);

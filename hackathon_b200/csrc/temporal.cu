@@ -1643,6 +1643,304 @@ __global__ void radial_full_kernel(RadialFullParams p) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Blocked masked Wiener-Khinchin for short lag ranges (L <= 128) on long
+// series (TPAD 8192): only lags tau < L are needed, so the series is cut into
+// blocks of BL = 128 samples and every correlation is assembled from
+// 256-point transforms, one warp per mode, instead of three 8192-point
+// transforms per pair. With x~ = m x (masked series), p = m |x|^2, block
+// spectra X_b = FFT_256(x~_b zero-padded), P_b, M_b likewise (M: the mask), and
+// s_k = (-1)^k (the shift of block b + 1 by BL inside a 2 BL transform):
+//   G(tau)     = sum_t x~*(t) x~(t + tau)
+//              = IFFT[ sum_b conj(X_b) (X_b + s_k X_{b+1}) ](tau)
+//   A+B(tau)   = sum_t p(t) m(t + tau) + m(t) p(t + tau)
+//              = IFFT[ sum_b conj(P_b) (M_b + s_k M_{b+1})
+//                            + conj(M_b) (P_b + s_k P_{b+1}) ](tau)
+// exact for tau < BL (the window of block b covers blocks b and b + 1). Per
+// mode: one 256-point transform per block of x~, one per pair of blocks of p
+// (two real blocks in one complex transform), two inverse transforms; the
+// mask spectra M_b are computed once per CTA and video. D, C and P as the
+// other kernels (ddm_ref.js:275-285); the radial epilogue runs over the
+// CTA's threads (lag, quarter of the warps), FP64 sums in a fixed order.
+constexpr int BLK_L = 128, BLK_F = 256;
+#ifndef BLK_WARPS_N
+#define BLK_WARPS_N 8
+#endif
+constexpr int BLK_WARPS = BLK_WARPS_N;  // modes in flight per CTA, one per warp
+__host__ __device__ constexpr int blk_count(int T) { return (T + BLK_L - 1) / BLK_L; }
+static size_t temporal_blocked_smem(int T) {
+  return sizeof(float2) * ((size_t)(blk_count(T) + 1) * BLK_F    // mask block spectra (and a zero block)
+                           + (size_t)BLK_WARPS * 2 * BLK_F        // per-warp transform buffers
+                           + tw_size(BLK_F)) +                    // 256-point twiddles
+         sizeof(float4) * (size_t)BLK_WARPS * BLK_L +               // per-warp (A+B, G) by lag
+         sizeof(double) * (size_t)(BLK_WARPS * 32 / BLK_L) * PFIELDS * BLK_L +  // partial sums to combine
+         sizeof(float) * (BLK_L + BLK_WARPS);                       // 1/N(tau), P per warp
+}
+
+__global__ void __launch_bounds__(32 * BLK_WARPS, 1) temporal_blocked_kernel(TemporalParams p) {
+  constexpr int NTH = 32 * BLK_WARPS;
+  constexpr int QG = NTH / BLK_L;  // thread groups per lag in the epilogue
+  constexpr int WPG = BLK_WARPS / QG;  // warps (modes) per group
+  extern __shared__ __align__(16) float2 sm[];
+  __shared__ int s_next;
+  const int TS = p.T;  // the (largest) T: sizes the mask-spectrum table
+  float2* s_M = sm;                                        // [(nblk + 1)][BLK_F]
+  float2* s_buf = s_M + (size_t)(blk_count(TS) + 1) * BLK_F; // [warp][2][BLK_F]
+  float2* s_tw = s_buf + BLK_WARPS * 2 * BLK_F;
+  float4* s_E = reinterpret_cast<float4*>(s_tw + tw_size(BLK_F));  // [warp][BLK_L] (ab, g.x, g.y, -)
+  double* s_acc = reinterpret_cast<double*>(s_E + BLK_WARPS * BLK_L);  // [QG][PFIELDS][BLK_L]
+  float* s_inp = reinterpret_cast<float*>(s_acc + QG * PFIELDS * BLK_L);
+  float* s_P = s_inp + BLK_L;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  float2* b0 = s_buf + warp * 2 * BLK_F;
+  float2* b1 = b0 + BLK_F;
+  // 256-point twiddle blocks (radix 8, 8, 4), the table layout of fft_block.cuh
+  for (int i = tid; i < tw_size(BLK_F); i += NTH) {
+    const int ns = i < 7 * 8 ? 8 : 64, r = ns == 8 ? 8 : 4;
+    const int j = ns == 8 ? i : i - 7 * 8;
+    const int m = j / ns + 1, k = j % ns;
+    float s, c;
+    sincospif(-2.0f * (float)(m * k) / (float)(ns * r), &s, &c);
+    s_tw[i] = make_float2(c, s);
+  }
+  const float sk = (lane & 1) ? -1.f : 1.f;  // (-1)^k, k = lane + 32 q
+  const float inv_f = 1.f / BLK_F;
+
+  int cur_v = -1, L = 0, T = 0, nblk = 0, v_unit0 = 0, v_nunits = 0;
+  const float2* v_hist = nullptr;
+  const uint32_t* v_order = nullptr;
+  const float* v_mask = nullptr;
+  const int4* v_items = nullptr;
+  double* v_partials = nullptr;
+  float np0 = 0.f;
+  auto load_video = [&](int vi) {  // between two CTA barriers
+    const VideoDesc vd = video_of(p, vi);
+    cur_v = vi;
+    L = vd.L;
+    T = vd.T;
+    nblk = blk_count(T);
+    v_hist = vd.hist;
+    v_order = vd.order;
+    v_mask = vd.mask;
+    v_items = vd.items;
+    v_partials = vd.partials;
+    v_unit0 = vd.unit0;
+    v_nunits = vd.nunits;
+    np0 = vd.npairs[0];
+    for (int i = tid; i < BLK_L; i += NTH) {
+      const float n = i < L ? vd.npairs[i] : 0.f;
+      s_inp[i] = n > 0.5f ? 1.f / n : 0.f;
+    }
+    // mask block spectra M_b, one warp per block; block nblk (past T) is zero
+    for (int b = warp; b <= nblk; b += BLK_WARPS) {
+      float2 v[8];
+#pragma unroll
+      for (int q = 0; q < 8; q++) {
+        const int t = b * BLK_L + lane + 32 * q;
+        v[q] = make_float2(q < 4 && t < T ? __ldg(&v_mask[t]) : 0.f, 0.f);
+      }
+      const float2* Y = fft<BLK_F, false, true, SYNC_WARP>(v, lane, b0, b1, s_tw);
+#pragma unroll
+      for (int q = 0; q < 8; q++) s_M[(size_t)b * BLK_F + lane + 32 * q] = Y[pad(lane + 32 * q)];
+      __syncwarp();  // Y read before the next transform writes the buffers
+    }
+  };
+  // one block's masked samples and p = m |x|^2 at this lane's offsets lane + 32 q
+  auto load_block = [&](const float2* row, int b, float2 (&x)[4], float (&pw)[4], double& psum) {
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int t = b * BLK_L + lane + 32 * q;
+      float2 v = make_float2(0.f, 0.f);
+      float m = 0.f;
+      if (t < T) {
+        m = __ldg(&v_mask[t]);
+        v = __ldg(&row[__ldg(&v_order[t])]);
+      }
+      pw[q] = m * fmaf(v.x, v.x, v.y * v.y);
+      x[q] = make_float2(m * v.x, m * v.y);
+      psum += (double)pw[q];
+    }
+  };
+
+  if (tid == 0) s_next = atomicAdd(p.unit_counter, 1);
+  __syncthreads();
+  int u = s_next;
+  const int etau = tid % BLK_L, egrp = tid / BLK_L;  // epilogue: this thread's lag and warp group
+  double acc[PFIELDS];
+#pragma unroll
+  for (int c = 0; c < PFIELDS; c++) acc[c] = 0.0;
+  double accP = 0.0;  // thread 0
+  while (u < p.nunits) {
+    const int4 U = p.units[u];
+    const int vi = p.videos ? U.w : 0;
+    if (vi != cur_v) {
+      __syncthreads();  // the previous video's tables are no longer read
+      load_video(vi);
+      __syncthreads();
+    }
+    for (int r0 = 0; r0 < U.y; r0 += BLK_WARPS) {  // rounds of one mode per warp
+      const int k = r0 + warp;
+      if (k < U.y) {
+        const int4 e = load_item(v_items, U.x + k);
+        const float2* row = v_hist + (size_t)e.x * T;
+        float2 aG[8], aAB[8], pX[8], pP[8];
+#pragma unroll
+        for (int q = 0; q < 8; q++) aG[q] = aAB[q] = pX[q] = pP[q] = make_float2(0.f, 0.f);
+        double psum = 0.0;
+        // G: a block's spectrum X_n completes block n - 1's term
+        auto g_step = [&](const float2* Y) {
+#pragma unroll
+          for (int q = 0; q < 8; q++) {
+            const float2 xn = Y[pad(lane + 32 * q)];
+            const float2 w = make_float2(fmaf(sk, xn.x, pX[q].x), fmaf(sk, xn.y, pX[q].y));
+            aG[q].x += pX[q].x * w.x + pX[q].y * w.y;  // conj(X_{n-1}) (X_{n-1} + s_k X_n)
+            aG[q].y += pX[q].x * w.y - pX[q].y * w.x;
+            pX[q] = xn;
+          }
+          __syncwarp();
+        };
+        // A + B: block b's spectrum P_b completes block b - 1's term
+        auto ab_step = [&](int bn, const float2 (&pn)[8]) {
+#pragma unroll
+          for (int q = 0; q < 8; q++) {
+            if (bn > 0) {
+              const float2 m0 = s_M[(size_t)(bn - 1) * BLK_F + lane + 32 * q];
+              const float2 m1 = s_M[(size_t)bn * BLK_F + lane + 32 * q];
+              const float2 pb = pP[q];
+              const float re0 = pb.x * m0.x + pb.y * m0.y;        // Re conj(P_b) M_b
+              const float r1 = pb.x * m1.x + pb.y * m1.y, i1 = pb.x * m1.y - pb.y * m1.x;  // conj(P_b) M_{b+1}
+              const float r2 = m0.x * pn[q].x + m0.y * pn[q].y, i2 = m0.x * pn[q].y - m0.y * pn[q].x;  // conj(M_b) P_{b+1}
+              aAB[q].x += 2.f * re0 + sk * (r1 + r2);
+              aAB[q].y += sk * (i1 + i2);
+            }
+            pP[q] = pn[q];
+          }
+        };
+        for (int b = 0; b < nblk; b += 2) {
+          float2 xv[4];
+          float p0[4], p1[4];
+          float2 v[8];
+          load_block(row, b, xv, p0, psum);
+#pragma unroll
+          for (int q = 0; q < 8; q++) v[q] = q < 4 ? xv[q] : make_float2(0.f, 0.f);
+          g_step(fft<BLK_F, false, true, SYNC_WARP>(v, lane, b0, b1, s_tw));
+          const bool two = b + 1 < nblk;
+          if (two) {
+            load_block(row, b + 1, xv, p1, psum);
+#pragma unroll
+            for (int q = 0; q < 8; q++) v[q] = q < 4 ? xv[q] : make_float2(0.f, 0.f);
+            g_step(fft<BLK_F, false, true, SYNC_WARP>(v, lane, b0, b1, s_tw));
+          } else {
+#pragma unroll
+            for (int q = 0; q < 4; q++) p1[q] = 0.f;
+          }
+          // P_b and P_{b+1} from one transform of p_b + i p_{b+1}
+#pragma unroll
+          for (int q = 0; q < 8; q++) v[q] = q < 4 ? make_float2(p0[q], p1[q]) : make_float2(0.f, 0.f);
+          const float2* Z = fft<BLK_F, false, true, SYNC_WARP>(v, lane, b0, b1, s_tw);
+          float2 pa[8], pb[8];
+#pragma unroll
+          for (int q = 0; q < 8; q++) {
+            const int kk = lane + 32 * q;
+            const float2 zk = Z[pad(kk)], zn = Z[pad((BLK_F - kk) & (BLK_F - 1))];
+            pa[q] = make_float2(0.5f * (zk.x + zn.x), 0.5f * (zk.y - zn.y));
+            pb[q] = make_float2(0.5f * (zk.y + zn.y), 0.5f * (zn.x - zk.x));
+          }
+          __syncwarp();
+          ab_step(b, pa);
+          if (two) ab_step(b + 1, pb);
+        }
+        // the last block's terms: X_nblk = P_nblk = 0, M_nblk = 0 (the zero block)
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+          aG[q].x += pX[q].x * pX[q].x + pX[q].y * pX[q].y;
+          const float2 m0 = s_M[(size_t)(nblk - 1) * BLK_F + lane + 32 * q];
+          const float2 m1 = s_M[(size_t)nblk * BLK_F + lane + 32 * q];
+          const float2 pbq = pP[q];
+          aAB[q].x += 2.f * (pbq.x * m0.x + pbq.y * m0.y) + sk * (pbq.x * m1.x + pbq.y * m1.y);
+          aAB[q].y += sk * (pbq.x * m1.y - pbq.y * m1.x);
+        }
+        // G(tau) and (A + B)(tau), tau = lane + 32 q < BLK_L
+        float4* E = s_E + warp * BLK_L;
+        {
+          const float2* Y = fft<BLK_F, true, true, SYNC_WARP>(aG, lane, b0, b1, s_tw);
+#pragma unroll
+          for (int q = 0; q < 4; q++) {
+            const float2 g = Y[pad(lane + 32 * q)];
+            E[lane + 32 * q] = make_float4(0.f, g.x * inv_f, g.y * inv_f, 0.f);
+          }
+          __syncwarp();
+          const float2* W = fft<BLK_F, true, true, SYNC_WARP>(aAB, lane, b0, b1, s_tw);
+#pragma unroll
+          for (int q = 0; q < 4; q++) E[lane + 32 * q].x = W[pad(lane + 32 * q)].x * inv_f;
+          __syncwarp();
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) psum += __shfl_xor_sync(0xffffffffu, psum, o);
+        if (lane == 0) s_P[warp] = np0 > 0.5f ? (float)(psum / np0) : 0.f;
+      }
+      __syncthreads();  // the round's (A + B, G) complete
+      // radial epilogue: thread (lag etau, group egrp) adds the modes of warps
+      // egrp * WPG .. egrp * WPG + WPG - 1 of this round, in warp order
+      if (etau < L) {
+        const float inp = s_inp[etau];
+        const bool next = etau + 1 < L;
+        const float inp1 = next ? s_inp[etau + 1] : 0.f;
+        for (int w = egrp * WPG; w < egrp * WPG + WPG && r0 + w < U.y; w++) {
+          const int4 e = load_item(v_items, U.x + r0 + w);
+          const double kx = e.y, ky = e.z;
+          const float4 E0 = s_E[w * BLK_L + etau];
+          acc[0] += (double)((E0.x - 2.f * E0.y) * inp);
+          if (next) {
+            const float4 E1 = s_E[w * BLK_L + etau + 1];
+            const float cx = E0.y * inp, cy = E0.z * inp;
+            const float c1x = E1.y * inp1, c1y = E1.z * inp1;
+            const float zr = fmaf(c1x, cx, c1y * cy);  // C(tau+1) conj C(tau)
+            const float zi = fmaf(c1y, cx, -c1x * cy);
+            const float wgt = sqrtf(fmaf(zr, zr, zi * zi));
+            if (wgt > 0.f) {
+              const double wd = wgt, ph = atan2f(zi, zr);
+              acc[1] += wd;
+              acc[2] += wd * kx * kx;
+              acc[3] += wd * kx * ky;
+              acc[4] += wd * ky * ky;
+              acc[5] += wd * kx * ph;
+              acc[6] += wd * ky * ph;
+              acc[7] += wd * ph * ph;
+              acc[8] += 1.0;
+            }
+          }
+        }
+      }
+      if (tid == 0)
+        for (int w = 0; w < BLK_WARPS && r0 + w < U.y; w++) accP += (double)s_P[w];
+      __syncthreads();  // s_E and s_P are rewritten by the next round
+    }
+    // the unit's partial record: the warp groups' sums added in group order
+    const int ul = u - v_unit0;
+    if (egrp > 0 && etau < L)
+#pragma unroll
+      for (int c = 0; c < PFIELDS; c++) s_acc[((egrp - 1) * PFIELDS + c) * BLK_L + etau] = acc[c];
+    __syncthreads();
+    if (egrp == 0 && etau < L)
+#pragma unroll
+      for (int c = 0; c < PFIELDS; c++) {
+        double t = acc[c];
+        for (int g = 1; g < QG; g++) t += s_acc[((g - 1) * PFIELDS + c) * BLK_L + etau];
+        v_partials[((size_t)ul * PFIELDS + c) * L + etau] = t;
+      }
+#pragma unroll
+    for (int c = 0; c < PFIELDS; c++) acc[c] = 0.0;
+    if (tid == 0) {
+      v_partials[(size_t)v_nunits * PFIELDS * L + ul] = accP;
+      accP = 0.0;
+      s_next = atomicAdd(p.unit_counter, 1);
+    }
+    __syncthreads();  // s_acc read; the next unit index published
+    u = s_next;
+  }
+}
+
 // ------------------------------------------------------------------ launchers
 
 template <int NP>
@@ -1701,6 +1999,14 @@ static size_t temporal_sparse_smem(int T, int L, int LPT) {
 template <int NP, int LPT, bool FULL>
 static cudaError_t launch_k(const TemporalParams& p, int grid, cudaStream_t s) {
   if constexpr (use_big(NP)) {
+    if constexpr (!FULL) {
+      if (p.variant == 2) {
+        const size_t sm = temporal_blocked_smem(p.T);
+        cudaFuncSetAttribute(temporal_blocked_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        temporal_blocked_kernel<<<grid, 32 * BLK_WARPS, sm, s>>>(p);
+        return cudaGetLastError();
+      }
+    }
     if (p.sparse) {
       auto k = temporal_sparse_big_kernel<NP, LPT, FULL>;
       const size_t sm = temporal_sparse_big_smem<NP>(p.T, p.L, LPT);
@@ -1753,6 +2059,7 @@ static int occupancy_grid(K k, int threads, size_t smem) {
 template <int NP, int LPT, bool FULL>
 static int grid_of(int T, int L, int variant, bool sparse) {
   if constexpr (use_big(NP)) {
+    if (variant == 2 && !FULL) return occupancy_grid(temporal_blocked_kernel, 32 * BLK_WARPS, temporal_blocked_smem(T));
     if (sparse)
       return occupancy_grid(temporal_sparse_big_kernel<NP, LPT, FULL>, NP / 16,
                             temporal_sparse_big_smem<NP>(T, L, LPT));
@@ -1841,7 +2148,12 @@ int temporal_sparse_limit(int TPAD, int T, int L, bool full) {
   return SPARSE_ZMAX_BIG / lpt;
 }
 
+bool temporal_blocked_ok(int TPAD, int T, int L, bool full) {
+  return TPAD == 8192 && !full && L <= BLK_L && temporal_blocked_smem(T) <= 227 * 1024;
+}
+
 int temporal_kernel_id(int TPAD, bool full, int variant, bool sparse) {
+  if (use_big(TPAD) && !full && variant == 2) return DDM_TK_BLOCKED;
   if (use_big(TPAD)) return sparse ? DDM_TK_SPARSE_BIG : DDM_TK_BIG;
   if (sparse && sparse_ok(TPAD)) return DDM_TK_SPARSE;
   if (use16(TPAD, full) && variant == 1) return DDM_TK_RADIX16;

@@ -325,8 +325,14 @@ class DdmEngine:
         self._alive()
         self._check(self._lib.ddm_set_sparse(self._h, 1 if enable else 0))
 
+    def set_blocked(self, enable=True):
+        """Extension: the blocked temporal kernel for L <= 128 at TPAD 8192
+        (ddm_set_blocked); False keeps the TPAD 8192 transform kernels."""
+        self._alive()
+        self._check(self._lib.ddm_set_blocked(self._h, 1 if enable else 0))
+
     TEMPORAL_KERNELS = {0: "temporal_kernel", 1: "temporal16_kernel", 2: "temporal_sparse_kernel",
-                        3: "temporal_big_kernel", 4: "temporal_sparse_big_kernel"}
+                        3: "temporal_big_kernel", 4: "temporal_sparse_big_kernel", 5: "temporal_blocked_kernel"}
 
     @property
     def last_temporal_kernel(self):

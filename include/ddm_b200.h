@@ -212,12 +212,19 @@ int ddm_autotune(ddm_engine *h, char *report, int32_t report_len);
  * when every video qualifies and its first engine has it enabled. enable = 0
  * keeps the transform path for every mask. Default 1. */
 int ddm_set_sparse(ddm_engine *h, int32_t enable);
+/* Short lag ranges on long series (no counterpart in the reference): at TPAD
+ * 8192 with L <= 128 the fused path assembles every correlation from
+ * 128-sample blocks with 256-point transforms (DDM_TK_BLOCKED) instead of
+ * 8192-point ones. enable = 0 keeps the TPAD 8192 kernels. Default 1. */
+int ddm_set_blocked(ddm_engine *h, int32_t enable);
 /* The temporal kernel of the engine's last computeTemporal: DDM_TK_RADIX8
  * (one-group radix-8 transforms), DDM_TK_RADIX16 (two-group radix-16),
  * DDM_TK_SPARSE (sparse-mask kernel), DDM_TK_BIG (TPAD 8192),
- * DDM_TK_SPARSE_BIG (sparse-mask kernel at TPAD 8192); -1 before the first
+ * DDM_TK_SPARSE_BIG (sparse-mask kernel at TPAD 8192), DDM_TK_BLOCKED (TPAD
+ * 8192 with L <= 128: correlations from 128-sample blocks); -1 before the first
  * analysis (instrumentation). */
-enum { DDM_TK_RADIX8 = 0, DDM_TK_RADIX16 = 1, DDM_TK_SPARSE = 2, DDM_TK_BIG = 3, DDM_TK_SPARSE_BIG = 4 };
+enum { DDM_TK_RADIX8 = 0, DDM_TK_RADIX16 = 1, DDM_TK_SPARSE = 2, DDM_TK_BIG = 3, DDM_TK_SPARSE_BIG = 4,
+       DDM_TK_BLOCKED = 5 };
 int ddm_last_temporal_kernel(const ddm_engine *h);
 /* The engine's current chunk, unit size and variant; set them without
  * timing (e.g. from a cached autotune report; chunk/unit 0 and variant -1

@@ -428,6 +428,7 @@ def test_temporal_tpad8192(N, L, NB, kmax):
     frames, valid, _ = O.simulate(sim)
     idx = np.nonzero(valid)[0]
     eng = _engine(N=N, T=T, L=L, NB=NB, kmin=2, kmax=kmax)
+    eng.set_blocked(False)  # the TPAD 8192 kernels (the blocked one: test_temporal_blocked)
     eng.ingest_frames(frames[idx], idx)
     order, mask = O.linear_order(valid)
     order, mask = O.shuffle_order(order, mask, 7) if L > 2048 else (order, mask)
@@ -541,6 +542,7 @@ def test_temporal_sparse_big_256():
     eng = _engine(N=N, T=T, L=L, NB=NB, kmin=4, kmax=100)
     try:
         assert eng.TPAD == 8192
+        eng.set_blocked(False)
         eng.ingest_frames(frames[idx], idx)
         order, mask = O.linear_order(valid)
         eng.compute_temporal(order, mask)
@@ -572,3 +574,45 @@ def test_temporal_sparse_big_256():
         sc = np.abs(D2[b]).max()
         if sc > 0:
             assert np.abs(D[b] - D2[b]).max() <= 1e-5 * sc, b
+
+
+@pytest.mark.parametrize("T,L,drops,shuffle", [(4096, 128, 81, False), (4000, 100, 300, True)])
+def test_temporal_blocked(T, L, drops, shuffle):
+    """The blocked kernel (TPAD 8192, L <= 128: every correlation assembled
+    from 128-sample blocks with 256-point transforms) against the FP64
+    oracle and against the TPAD 8192 kernel on the same analysis: few dropped
+    frames and a 4096-frame series; 300 drops, a shuffled order and a series
+    that is not a whole number of blocks (4000 frames, 100 lags)."""
+    N, NB, kmax = 64, 12, 28
+    sim = dict(O.BASE, N=N, T=T, seed=29, swimmers=dict(n=6, vbar=20.0, sigma=8.0, geometry="3d"),
+               passive=dict(n=6), dropExact=drops)
+    frames, valid, _ = O.simulate(sim)
+    idx = np.nonzero(valid)[0]
+    eng = _engine(N=N, T=T, L=L, NB=NB, kmin=2, kmax=kmax)
+    try:
+        assert eng.TPAD == 8192
+        eng.ingest_frames(frames[idx], idx)
+        order, mask = O.linear_order(valid)
+        if shuffle:
+            order, mask = O.shuffle_order(order, mask, 5)
+        eng.compute_temporal(order, mask)
+        assert eng.last_temporal_kernel == "temporal_blocked_kernel"
+        rg = eng.read_radial()
+        eng.set_blocked(False)
+        eng.compute_temporal(order, mask)
+        assert eng.last_temporal_kernel in ("temporal_sparse_big_kernel", "temporal_big_kernel")
+        r2 = eng.read_radial()
+    finally:
+        eng.destroy()
+    hist = O.history_ingest(O.luma_of(frames[idx]), idx.astype(np.int32), T)
+    ro = O.analyze_radial(hist, order, mask, O.make_bins(N, NB, 2, kmax), L, TPAD=8192)  # the oracle's FFT is radix 2
+    D, D2 = rg.D2(), r2.D2()
+    for b in range(NB):
+        sc = ro["D"][b].max()
+        if sc > 0:
+            assert np.abs(D[b] - ro["D"][b]).max() <= 1e-4 * sc, b
+            assert np.abs(D[b] - D2[b]).max() <= 1e-5 * sc, b
+    assert np.allclose(rg.P, ro["P"], rtol=1e-5, atol=0)
+    # drift sums: same as the TPAD 8192 kernel's to FP32 rounding of C
+    d1, d2 = rg.drift3(), r2.drift3()
+    assert np.allclose(d1, d2, rtol=1e-3, atol=1e-4 * np.abs(d2).max())

@@ -1746,18 +1746,24 @@ __global__ void __launch_bounds__(32 * BLK_WARPS, 1) temporal_blocked_kernel(Tem
     }
   };
   // one block's masked samples and p = m |x|^2 at this lane's offsets lane + 32 q
-  auto load_block = [&](const float2* row, int b, float2 (&x)[4], float (&pw)[4], double& psum) {
+  // a block's raw samples and mask at this lane's offsets lane + 32 q (loads
+  // only: consumed a block pair later, so they are in flight meanwhile;
+  // measured on 15,676 modes x 4096 frames: 1.064 -> 1.040 ms)
+  auto fetch = [&](const float2* row, int b, float2 (&v)[4], float (&m)[4]) {
 #pragma unroll
     for (int q = 0; q < 4; q++) {
       const int t = b * BLK_L + lane + 32 * q;
-      float2 v = make_float2(0.f, 0.f);
-      float m = 0.f;
-      if (t < T) {
-        m = __ldg(&v_mask[t]);
-        v = __ldg(&row[__ldg(&v_order[t])]);
-      }
-      pw[q] = m * fmaf(v.x, v.x, v.y * v.y);
-      x[q] = make_float2(m * v.x, m * v.y);
+      const bool in = b < nblk && t < T;
+      m[q] = in ? __ldg(&v_mask[t]) : 0.f;
+      v[q] = in ? __ldg(&row[__ldg(&v_order[t])]) : make_float2(0.f, 0.f);
+    }
+  };
+  // masked samples x~ = m x and p = m |x|^2 of fetched samples
+  auto prep = [&](const float2 (&v)[4], const float (&m)[4], float2 (&x)[4], float (&pw)[4], double& psum) {
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      pw[q] = m[q] * fmaf(v[q].x, v[q].x, v[q].y * v[q].y);
+      x[q] = make_float2(m[q] * v[q].x, m[q] * v[q].y);
       psum += (double)pw[q];
     }
   };
@@ -1816,23 +1822,35 @@ __global__ void __launch_bounds__(32 * BLK_WARPS, 1) temporal_blocked_kernel(Tem
             pP[q] = pn[q];
           }
         };
+        float2 ra[4], rb[4];  // raw samples of the current block pair
+        float ma[4], mb[4];
+        fetch(row, 0, ra, ma);
+        fetch(row, 1, rb, mb);
         for (int b = 0; b < nblk; b += 2) {
+          float2 na[4], nb[4];  // the next pair's loads, in flight during this pair's transforms
+          float nma[4], nmb[4];
+          fetch(row, b + 2, na, nma);
+          fetch(row, b + 3, nb, nmb);
           float2 xv[4];
           float p0[4], p1[4];
           float2 v[8];
-          load_block(row, b, xv, p0, psum);
+          prep(ra, ma, xv, p0, psum);
 #pragma unroll
           for (int q = 0; q < 8; q++) v[q] = q < 4 ? xv[q] : make_float2(0.f, 0.f);
           g_step(fft<BLK_F, false, true, SYNC_WARP>(v, lane, b0, b1, s_tw));
           const bool two = b + 1 < nblk;
+          prep(rb, mb, xv, p1, psum);  // zeros past the last block
           if (two) {
-            load_block(row, b + 1, xv, p1, psum);
 #pragma unroll
             for (int q = 0; q < 8; q++) v[q] = q < 4 ? xv[q] : make_float2(0.f, 0.f);
             g_step(fft<BLK_F, false, true, SYNC_WARP>(v, lane, b0, b1, s_tw));
-          } else {
+          }
 #pragma unroll
-            for (int q = 0; q < 4; q++) p1[q] = 0.f;
+          for (int q = 0; q < 4; q++) {
+            ra[q] = na[q];
+            rb[q] = nb[q];
+            ma[q] = nma[q];
+            mb[q] = nmb[q];
           }
           // P_b and P_{b+1} from one transform of p_b + i p_{b+1}
 #pragma unroll
